@@ -1,0 +1,395 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries sit behind it:
+
+* ``libep_oracle.so`` -- the plain-C FP64 restatement of the voomEP
+  monodomain path (``ep_oracle.c``);
+* ``_ref/libvoomep_ref.so`` -- the reference's own cell-model sources
+  (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR}.cc) compiled
+  unmodified, used to pin the restatement and as the CPU reference arm.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this module; the product package never does.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+TUSSCHER, MAHAJAN, MAHAJAN_FAIL, LUORUDY, LUORUDYWITHGATE = 2, 3, 4, 0, 1
+NSTATE = {TUSSCHER: 19, MAHAJAN: 26, MAHAJAN_FAIL: 26, LUORUDY: 8, LUORUDYWITHGATE: 8}
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int)
+
+
+def _p(a, t=dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class _Csr(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("rowptr", ip), ("col", ip),
+                ("A", dp), ("B", dp), ("M", dp), ("K", dp), ("CL", dp)]
+
+
+class _Cells(C.Structure):
+    _fields_ = [("model", C.c_int), ("n", C.c_int), ("nstate", C.c_int), ("nconst", C.c_int),
+                ("state", dp), ("consts", dp), ("ntypes", C.c_int),
+                ("type", C.POINTER(C.c_uint8)), ("gks_scale", dp), ("alg12", dp),
+                ("lr_table", dp), ("Xi", C.c_double), ("user_Xi", C.c_double),
+                ("user_xi", C.c_int), ("newton_cap", C.c_int), ("tt_jac_true", C.c_int),
+                ("mh_abs_mode", C.c_int),
+                ("newton_total", C.c_longlong), ("newton_max", C.c_longlong),
+                ("substep_count", C.c_longlong)]
+
+
+class _Sim(C.Structure):
+    _fields_ = [("csr", C.POINTER(_Csr)), ("n", C.c_int), ("dt", C.c_double),
+                ("ionic_dt", C.c_double), ("Cm", C.c_double), ("cg_tol", C.c_double),
+                ("cg_maxit", C.c_int), ("jacobi_steps", C.c_int),
+                ("V", dp), ("istim", dp), ("dvdt", dp), ("b", dp), ("ici", dp),
+                ("ionic", C.c_void_p), ("ionic_ctx", C.c_void_p),
+                ("nsub", C.c_int), ("sub_dt", C.c_double * 64),
+                ("cg_iters_total", C.c_longlong), ("cg_fail", C.c_int), ("step", C.c_long)]
+
+
+def build():
+    """Compile the oracle (and, where the reference sources exist, _ref)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "libep_oracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.epo_cells_create.restype = C.POINTER(_Cells)
+        L.epo_cells_create.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        L.epo_cells_destroy.argtypes = [C.c_void_p]
+        L.epo_cells_compute_ion.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, dp, dp]
+        L.epo_cells_initial_voltage.argtypes = [C.c_void_p, dp]
+        L.epo_assemble.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_double, C.c_double,
+                                   C.c_double, C.POINTER(_Csr)]
+        L.epo_csr_free.argtypes = [C.POINTER(_Csr)]
+        L.epo_spmv.argtypes = [C.POINTER(_Csr), dp, dp, dp]
+        L.epo_pcg.argtypes = [C.POINTER(_Csr), dp, dp, dp, C.c_double, C.c_int, C.c_int, dp]
+        L.epo_ecg_elementwise.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_int, dp, dp, dp]
+        L.epo_ecg_weights.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_int, dp, dp]
+        L.epo_sim_init.argtypes = [C.POINTER(_Sim), C.POINTER(_Csr), C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_void_p]
+        L.epo_sim_free.argtypes = [C.POINTER(_Sim)]
+        L.epo_sim_step.argtypes = [C.POINTER(_Sim)]
+        L.epo_stim_schedule.argtypes = [C.c_int, dp, dp, C.c_double, C.c_long,
+                                        C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.epo_num_steps.restype = C.c_long
+        L.epo_num_steps.argtypes = [C.c_double, C.c_double]
+        L.epo_set_threads.argtypes = [C.c_int]
+        L.epo_get_threads.restype = C.c_int
+        L.epo_tt_constants.argtypes = [dp]
+        L.epo_mh_constants.argtypes = [dp, C.c_int, C.c_int]
+        L.epo_tt_initial_state.argtypes = [dp]
+        L.epo_mh_initial_state.argtypes = [dp, C.c_int]
+        L.epo_lr_initial_state.argtypes = [dp]
+        _LIB = L
+    return _LIB
+
+
+def ref_lib():
+    """The reference cell models compiled unmodified (None if not built)."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libvoomep_ref.so")
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_cells_create.restype = C.c_void_p
+        L.ref_cells_create.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        L.ref_cells_destroy.argtypes = [C.c_void_p]
+        L.ref_cells_nstate.argtypes = [C.c_void_p]
+        L.ref_cells_compute_ion.argtypes = [C.c_void_p, C.c_double, C.c_double, dp, dp, dp]
+        L.ref_cells_get_states.argtypes = [C.c_void_p, dp]
+        L.ref_cells_set_states.argtypes = [C.c_void_p, dp]
+        L.ref_cells_get_voltage.argtypes = [C.c_void_p, dp]
+        L.ref_cells_set_user_xi.argtypes = [C.c_void_p, C.c_double]
+        L.epo_assemble.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_double, C.c_double,
+                                   C.c_double, C.POINTER(_Csr)]
+        L.epo_csr_free.argtypes = [C.POINTER(_Csr)]
+        L.epo_sim_init.argtypes = [C.POINTER(_Sim), C.POINTER(_Csr), C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_void_p]
+        L.epo_sim_step.argtypes = [C.POINTER(_Sim)]
+        L.epo_sim_free.argtypes = [C.POINTER(_Sim)]
+        L.epo_set_threads.argtypes = [C.c_int]
+        _REF = L
+    return _REF
+
+
+def set_threads(n):
+    lib().epo_set_threads(int(n))
+    r = ref_lib()
+    if r is not None:
+        r.epo_set_threads(int(n))
+
+
+def tt_constants():
+    c = np.zeros(54)
+    lib().epo_tt_constants(_p(c))
+    return c
+
+
+def mh_constants(pos, failing=False):
+    c = np.zeros(35)
+    lib().epo_mh_constants(_p(c), int(pos), int(bool(failing)))
+    return c
+
+
+def initial_state(model, pos=0):
+    L = lib()
+    if model == TUSSCHER:
+        s = np.zeros(19); L.epo_tt_initial_state(_p(s))
+    elif model in (MAHAJAN, MAHAJAN_FAIL):
+        s = np.zeros(26); L.epo_mh_initial_state(_p(s), int(pos))
+    else:
+        s = np.zeros(8); L.epo_lr_initial_state(_p(s))
+    return s
+
+
+class Cells:
+    """Oracle population: one state row per node (node-major, FP64)."""
+
+    def __init__(self, model, n, types=None, type_consts=None, gks_scale=None,
+                 newton_cap=0, mh_abs_mode=0, user_xi=None, tt_jac_true=0):
+        L = lib()
+        self.model, self.n = model, n
+        self._types = None if types is None else np.ascontiguousarray(types, dtype=np.uint8)
+        self._tc = None
+        ntypes = 0
+        if type_consts is not None:
+            self._tc = np.ascontiguousarray(type_consts, dtype=np.float64)
+            ntypes = self._tc.shape[0]
+        elif self._types is not None:
+            ntypes = int(self._types.max()) + 1 if n else 1
+            if model == TUSSCHER:
+                ntypes = 1
+        self.h = L.epo_cells_create(model, n, _p(self._types, C.c_void_p) if self._types is not None else None,
+                                    ntypes, _p(self._tc, C.c_void_p) if self._tc is not None else None)
+        c = self.h.contents
+        c.newton_cap = int(newton_cap)
+        c.tt_jac_true = int(tt_jac_true)
+        c.mh_abs_mode = int(mh_abs_mode)
+        if user_xi is not None:
+            c.user_Xi = float(user_xi); c.user_xi = 1
+        self.nstate = c.nstate
+        if gks_scale is not None:
+            # malloc'd by libc so that epo_cells_destroy can free it
+            libc = C.CDLL(None)
+            libc.malloc.restype = C.c_void_p
+            buf = libc.malloc(C.c_size_t(8 * n))
+            arr = np.ctypeslib.as_array(C.cast(buf, dp), shape=(n,))
+            arr[:] = gks_scale
+            c.gks_scale = C.cast(buf, dp)
+
+    @property
+    def state(self):
+        c = self.h.contents
+        return np.ctypeslib.as_array(c.state, shape=(self.n, self.nstate))
+
+    @property
+    def newton_stats(self):
+        c = self.h.contents
+        return c.newton_total, c.newton_max
+
+    def compute_ion(self, V, istim, dt, Cm=1.0):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        istim = np.ascontiguousarray(istim, dtype=np.float64)
+        out = np.empty(self.n)
+        lib().epo_cells_compute_ion(self.h, Cm, dt, _p(V), _p(istim), _p(out))
+        return out
+
+    def initial_voltage(self):
+        V = np.empty(self.n)
+        lib().epo_cells_initial_voltage(self.h, _p(V))
+        return V
+
+    def __del__(self):
+        try:
+            lib().epo_cells_destroy(self.h)
+        except Exception:
+            pass
+
+
+class RefCells:
+    """The reference's unmodified cell objects (one heap object per node)."""
+
+    def __init__(self, model, n, types=None):
+        L = ref_lib()
+        if L is None:
+            raise RuntimeError("oracle/_ref/libvoomep_ref.so is not built")
+        self._types = None if types is None else np.ascontiguousarray(types, dtype=np.uint8)
+        self.h = L.ref_cells_create(model, n, _p(self._types, C.c_void_p) if self._types is not None else None)
+        self.n, self.model = n, model
+        self.nstate = L.ref_cells_nstate(self.h)
+
+    def compute_ion(self, V, istim, dt, Cm=1.0):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        istim = np.ascontiguousarray(istim, dtype=np.float64)
+        out = np.empty(self.n)
+        ref_lib().ref_cells_compute_ion(self.h, Cm, dt, _p(V), _p(istim), _p(out))
+        return out
+
+    @property
+    def state(self):
+        out = np.empty((self.n, self.nstate))
+        ref_lib().ref_cells_get_states(self.h, _p(out))
+        return out
+
+    @state.setter
+    def state(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        ref_lib().ref_cells_set_states(self.h, _p(s))
+
+    def get_voltage(self):
+        out = np.empty(self.n)
+        ref_lib().ref_cells_get_voltage(self.h, _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            ref_lib().ref_cells_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Csr:
+    """Assembled CN system (oracle)."""
+
+    def __init__(self, xyz, tets, fibers=None, D=(1e-3, 1e-3, 1e-3), Cm=1.0, dt=0.02,
+                 smoothing_alpha=0.0, L=None):
+        self._L = L or lib()
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self.tets = np.ascontiguousarray(tets, dtype=np.int32)
+        self.fibers = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
+        self.D = np.ascontiguousarray(D, dtype=np.float64)
+        self.c = _Csr()
+        rc = self._L.epo_assemble(len(self.xyz), _p(self.xyz), len(self.tets), _p(self.tets, ip),
+                                  _p(self.fibers), _p(self.D), Cm, dt, smoothing_alpha,
+                                  C.byref(self.c))
+        self.degenerate = rc != 0
+        self.n, self.nnz = self.c.n, self.c.nnz
+
+    def arr(self, name):
+        size = self.n + 1 if name == "rowptr" else (self.n if name == "CL" else self.nnz)
+        return np.ctypeslib.as_array(getattr(self.c, name), shape=(size,)).copy()
+
+    def scipy(self, name):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.arr(name), self.arr("col"), self.arr("rowptr")),
+                             shape=(self.n, self.n))
+
+    def pcg(self, b, x0, tol=1e-7, maxit=1000, jacobi_steps=3):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x0, dtype=np.float64)
+        rr = C.c_double(0)
+        it = lib().epo_pcg(C.byref(self.c), self.c.A, _p(b), _p(x), tol, maxit, jacobi_steps,
+                           C.byref(rr))
+        return x, it, rr.value
+
+    def __del__(self):
+        try:
+            self._L.epo_csr_free(C.byref(self.c))
+        except Exception:
+            pass
+
+
+def ecg_elementwise(xyz, tets, fibers, D, electrodes, V):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    fib = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    el = np.ascontiguousarray(electrodes, dtype=np.float64)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    out = np.zeros(len(el))
+    lib().epo_ecg_elementwise(len(xyz), _p(xyz), len(tets), _p(tets, ip), _p(fib), _p(D),
+                              len(el), _p(el), _p(V), _p(out))
+    return out
+
+
+def ecg_weights(xyz, tets, fibers, D, electrodes):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    fib = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    el = np.ascontiguousarray(electrodes, dtype=np.float64)
+    W = np.zeros((len(el), len(xyz)))
+    lib().epo_ecg_weights(len(xyz), _p(xyz), len(tets), _p(tets, ip), _p(fib), _p(D),
+                          len(el), _p(el), _p(W))
+    return W
+
+
+def stim_schedule(t_start, t_stop, dt, nsteps):
+    t0 = np.ascontiguousarray(t_start, dtype=np.float64)
+    t1 = np.ascontiguousarray(t_stop, dtype=np.float64)
+    s0 = (C.c_long * len(t0))()
+    s1 = (C.c_long * len(t0))()
+    lib().epo_stim_schedule(len(t0), _p(t0), _p(t1), dt, nsteps, s0, s1)
+    return np.array(list(s0)), np.array(list(s1))
+
+
+def num_steps(dt, T):
+    return lib().epo_num_steps(dt, T)
+
+
+class Sim:
+    """The split time step (EP_CrankNicholson::Solve) on the oracle.
+
+    ``cells`` is a :class:`Cells` (restatement) or :class:`RefCells` (the
+    reference objects); the FEM/PCG part is the C restatement either way.
+    """
+
+    def __init__(self, csr, cells, dt, ionic_dt, Cm=1.0, cg_tol=1e-7, cg_maxit=1000,
+                 jacobi_steps=3):
+        self.csr, self.cells = csr, cells
+        self.s = _Sim()
+        if isinstance(cells, RefCells):
+            L = ref_lib()
+            fn = C.cast(L.ref_cells_ionic_cb, C.c_void_p)
+            ctx = C.c_void_p(cells.h)
+            self._L = L
+        else:
+            L = lib()
+            fn = C.cast(L.epo_cells_ionic_cb, C.c_void_p)
+            ctx = C.cast(cells.h, C.c_void_p)
+            self._L = L
+        self._L.epo_sim_init(C.byref(self.s), C.byref(csr.c), dt, ionic_dt, Cm, cg_tol,
+                             cg_maxit, jacobi_steps, fn, ctx)
+        self.n = csr.n
+
+    @property
+    def V(self):
+        return np.ctypeslib.as_array(self.s.V, shape=(self.n,))
+
+    @property
+    def istim(self):
+        return np.ctypeslib.as_array(self.s.istim, shape=(self.n,))
+
+    @property
+    def sub_dt(self):
+        return [self.s.sub_dt[i] for i in range(self.s.nsub)]
+
+    def step(self, k=1):
+        for _ in range(k):
+            self._L.epo_sim_step(C.byref(self.s))
+
+    def __del__(self):
+        try:
+            self._L.epo_sim_free(C.byref(self.s))
+        except Exception:
+            pass
