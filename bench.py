@@ -1,0 +1,304 @@
+"""Benchmark: node-steps/s of the monodomain split step on the ~2M-node shell.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain_fp32|fp64]
+                    [--impl ours|reference]
+
+One step = one global dt (0.1 ms) of EP_CrankNicholson::Solve over the whole
+shell: half diffusion step (SpMV + Jacobi-PCG to 1e-7), 5 ionic sub-steps
+(ten Tusscher, endo/M/epi, PMJ stimuli), half diffusion step, and the
+pseudo-ECG every 10 steps.  Inputs (the operators and all cell states) are
+resident in HBM; they total > 126 MB, so no L2 flush is needed between
+steps.  Multi-GPU: independent replicas (the path does not shard), weak
+scaling, timing = max over ranks of the device (CUDA-event) time.
+
+--impl reference times the reference's own CPU implementation on the host
+cores: the reference cell-model sources compiled unmodified (oracle/_ref)
+inside the C restatement of the CN/PCG split step, on a bounded sample of the
+same workload (a coarser shell), all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s at 2M-node shell: surrogate vs plain FP32, act-time err ≤0.5 ms"
+UNIT = "node-steps/s"
+
+
+def _env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.lines = []
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        import statistics
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_every=10):
+    """Bytes one launch must move at minimum.
+
+    cg (one half diffusion step, SELL values + int32 columns):
+      prologue  nnz*(A + B + col) + n*(x + dinv + r_write + p_write)
+      iteration nnz*(A + col) + n*(r, dinv, p_old read + p_new, q write)   [phase A]
+                + n*(p_new, x, r, q, dinv read + x, r write)                [phase B]
+    ionic: the V + stored states read and written once, the activation
+      record read (16 B), node type (1 B), G_Ks scale and stimulus head (4 B each).
+    ecg: V and the ne weight rows read once per sample.
+    """
+    if kernel == "cg":
+        pro = nnz * (2 * rbytes + 4) + n * 4 * rbytes
+        it = nnz * (rbytes + 4) + n * 5 * rbytes + n * 7 * rbytes
+        return pro + cg_iters_per_solve * it
+    if kernel == "ionic":
+        return n * (2 * nstate * rbytes + 16 + 1 + rbytes + 4)
+    if kernel == "ecg":
+        return n * (1 + ne) * rbytes
+    raise ValueError(kernel)
+
+
+def cpu_sample(kind, h, steps, threads):
+    """Time the CPU path on a coarser shell (same model, dt, stimuli).
+    kind 'reference': the reference cell objects (oracle/_ref) in the C
+    restatement of the CN split step with AztecOO's 3-step Jacobi;
+    kind 'port': the C restatement throughout."""
+    from oracle import oracle as O
+    from ucla_cmg_b200 import workloads as W
+    O.set_threads(threads)
+    wl = W.shell_c2(h=h)
+    m = wl.mesh
+    csr = O.Csr(m.xyz, m.tets, m.fibers, wl.D, 1.0, wl.dt)
+    if kind == "reference" and O.ref_lib() is not None:
+        cells = O.RefCells(O.TUSSCHER, m.n)        # the reference has the epicardial set only
+    else:
+        kind = "port"
+        cells = O.Cells(O.TUSSCHER, m.n, types=wl.node_type, type_consts=wl.type_consts,
+                        gks_scale=wl.gks_scale, tt_jac_true=1, newton_cap=100)
+    sim = O.Sim(csr, cells, wl.dt, wl.ionic_dt, cg_tol=1e-7, cg_maxit=1000, jacobi_steps=3)
+    sim.V[:] = wl.V0
+    on = (wl.stim_on / wl.dt).astype(int)
+    off = (wl.stim_off / wl.dt).astype(int)
+    times = []
+    for k in range(steps):
+        sim.istim[:] = 0.0
+        act = (on <= k) & (k < off)
+        sim.istim[wl.stim_ids[act]] = wl.stim_amp[act]
+        t0 = time.perf_counter()
+        sim.step()
+        times.append(time.perf_counter() - t0)
+    return m.n, times, kind
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    h = float(os.environ.get("EP_REF_SAMPLE_H", "0.2"))
+    n, times, kind = cpu_sample("reference", h, args.warmup + args.steps, threads)
+    timed = times[args.warmup:]
+    tot = sum(timed)
+    v = n * len(timed) / tot
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(timed), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"shell_c2 sample: truncated ellipsoid shell h={h} cm ({n} nodes), "
+                                   "ten Tusscher, dt 0.1 / ionic 0.02 ms, 200 PMJ stimuli",
+                       "form": "reference CPU (FP64)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{len(timed)} steps of a {n}-node shell (h={h} cm) from t=0"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    from ucla_cmg_b200 import capi, workloads as W
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    prec = capi.FP64 if args.form == "fp64" else capi.FP32
+    wl = W.shell_c2()
+    g = wl.create(prec, device=local)
+    g.set_profiling(True)
+    n = wl.mesh.n
+    g.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(local)
+    clk.start()
+    st = g.step(args.steps)
+    clocks = clk.stop()
+    torch.cuda.synchronize()
+    ms = st["device_ms"]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = n * args.steps * world / (ms * 1e-3)
+    # ---- end to end through the public API with host buffers ----
+    states = g.states()
+    V = g.voltage()
+    k_e2e = max(3, min(args.steps, 20))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.set_states(states)
+    g.set_voltage(V)
+    for _ in range(k_e2e):
+        g.step(1)
+        V = g.voltage()
+    e2e_s = time.perf_counter() - t0
+    rb = 8 if prec == capi.FP64 else 4
+    e2e = {"value": n * k_e2e / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int((states.nbytes + V.nbytes) / k_e2e),
+           "d2h_bytes_per_step": int(V.nbytes)}
+    # ---- roofline of the dominant kernel ----
+    nnz = int(wl.mesh.n + 2 * _edge_count(wl.mesh))
+    cg_per_solve = st["cg_iters"] / max(1, 2 * args.steps)
+    kms = {"cg": st["cg_ms"], "ionic": st["ionic_ms"], "ecg": st["ecg_ms"]}
+    launches = {"cg": 2 * args.steps, "ionic": args.steps, "ecg": args.steps // 10}
+    dom = max(kms, key=kms.get)
+    per_launch_ms = kms[dom] / max(1, launches[dom])
+    alg = algorithmic_bytes(dom, n, nnz, cg_per_solve, rb)
+    peak, peak_kind = _peaks()
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom),
+            "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
+            "kernel_ms": kms}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32",
+            "data": "synthetic",
+            "config": {"workload": f"shell_c2: truncated prolate-ellipsoid shell, {n} nodes, "
+                                   f"{wl.mesh.m} tets, ten Tusscher endo/M/epi 40/30/30, G_Ks 0.8->1.2 "
+                                   "apex->base, 200 PMJ stimuli t~U(0,30) ms, 10 electrodes",
+                       "form": args.form, "dt_ms": wl.dt, "ionic_dt_ms": wl.ionic_dt,
+                       "t_window_ms": [0.0, round((args.warmup + args.steps) * wl.dt, 3)],
+                       "l2": "inputs > L2 (operators + states ~ 0.5 GB), no flush",
+                       "cg_iters_per_solve": cg_per_solve, "newton_iters": st["newton_iters"],
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": int(st["launches"]),
+            "clocks": clocks, "roofline": roof, "e2e": e2e}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        h = float(os.environ.get("EP_CPU_SAMPLE_H", "0.12"))
+        ncpu, times, kind = cpu_sample("reference", h, 6, threads)
+        v = ncpu * 5 / sum(times[1:])
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"5 steps (after 1 untimed) of a {ncpu}-node shell "
+                                          f"(h={h} cm) from t=0, same model, dt and stimuli"}
+    g.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def _edge_count(m):
+    import numpy as np
+    e = np.concatenate([m.tets[:, [a, b]] for a in range(4) for b in range(a + 1, 4)])
+    e.sort(axis=1)
+    key = e[:, 0].astype(np.int64) * m.n + e[:, 1]
+    return len(np.unique(key))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="plain_fp32", choices=["plain_fp32", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * ep_gpu.h -- C ABI of the B200-native voomEP monodomain time step.
+ *
+ * One handle = one tissue instance resident on one GPU (device memory owned
+ * by the handle, one CUDA stream per handle, not thread-safe per handle).
+ * The caller owns every host buffer.  Every entry point returns EP_OK (0)
+ * or a negative EP_ERR_* code; nothing calls exit().  ep_last_error()
+ * returns a thread-local message for the last failure.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * wsklug/UCLA_CMG, voomEP/src/...).
+ */
+#ifndef EP_GPU_H
+#define EP_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EP_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define EP_OK               0
+#define EP_ERR_ARG         -1   /* bad argument / size */
+#define EP_ERR_CUDA        -2   /* CUDA runtime error */
+#define EP_ERR_NOMEM       -3
+#define EP_ERR_MESH        -4   /* degenerate or inverted element */
+#define EP_ERR_CG          -5   /* a CG solve reached cg_maxit */
+#define EP_ERR_NEWTON      -6   /* a Newton solve reached its cap */
+#define EP_ERR_NAN         -7   /* non-finite voltage detected */
+#define EP_ERR_TIMEOUT     -8   /* an in-kernel wait gave up */
+#define EP_ERR_UNSUPPORTED -9
+#define EP_ERR_IO          -10
+
+/* ---- cell models: the reference enum CellModelType
+ *      (Body/CardiacBody.h:57) ---- */
+#define EP_LUORUDY          0
+#define EP_LUORUDYWITHGATE  1
+#define EP_TUSSCHER         2
+#define EP_MAHAJAN          3
+#define EP_MAHAJAN_FAIL     4
+
+/* ---- arithmetic of the ionic update and the SpMV ---- */
+#define EP_FP64       0   /* everything FP64 */
+#define EP_FP32       1   /* ionic + SpMV FP32; CG dots, residual, ECG sums FP64 */
+#define EP_SURROGATE  2   /* EP_FP32 with the learned ionic step (ep_set_surrogate) */
+
+/* ---- ten Tusscher Newton Jacobian layout ---- */
+#define EP_TT_JAC_REFERENCE 0  /* the reference hands J[j*6+i]=df_j/dx_i to the
+                                  column-major dgesv_ (Tusscher.cc:173,181) and so
+                                  solves with J^T; kept for parity */
+#define EP_TT_JAC_TRUE      1  /* Newton with J itself */
+
+typedef struct ep_handle ep_handle;
+
+/* Geometry: Mesh::New + TetMesh::Compute (Mesh/Mesh.cc:142-483,
+ * Mesh/TetMesh.cc:9-71) and CardiacBody::setDiffusion / setNodalCapacitance
+ * (Body/CardiacBody.h:252-260). */
+typedef struct ep_mesh_desc {
+    int32_t n_nodes;
+    const double *xyz;          /* 3 * n_nodes, cm */
+    int32_t n_tets;
+    const int32_t *tets;        /* 4 * n_tets */
+    int32_t one_based;          /* 1: ids as in the reference .ele files */
+    const double *fibers;       /* 9 * n_tets (f, s, n) or NULL: isotropic D[0] */
+    double D[3];                /* cm^2/ms along f, s, n */
+    double Cm;                  /* uF/cm^2 (the reference uses 1.0) */
+} ep_mesh_desc;
+
+/* Cell models: CardiacBody::New + SetUp*Parameters
+ * (Body/CardiacBody.cc:975-1101, IonicModel/SetUpIonicConstants.h). */
+typedef struct ep_model_desc {
+    int32_t model;              /* EP_TUSSCHER, ... */
+    int32_t n_types;            /* parameter sets (<= 16) */
+    const double *type_consts;  /* n_types * ep_model_nconst(model), or NULL:
+                                   the reference constants for type 0..n_types-1 */
+    const uint8_t *node_type;   /* n_nodes or NULL (all type 0) */
+    const double *node_gks_scale; /* n_nodes or NULL: G_Ks multiplier (TT) */
+    double user_xi;             /* > 0: CardiacBody user Xi; else the model's own */
+    int32_t newton_cap;         /* TT Newton cap (0: 100) */
+    int32_t tt_jacobian;        /* EP_TT_JAC_* */
+    int32_t mh_abs_mode;        /* Mahajan sub-step trigger: 0 int |dV/dt| (as
+                                   compiled), 1 double fabs (Mahajan.cc:611) */
+    const double *initial_states; /* n_nodes * nstate node-major, or NULL */
+} ep_model_desc;
+
+/* Time stepping: EPSolver::New/setSolveTime/setIonicTimeStep
+ * (Solvers/EPSolver.h:190-223) and EP_CrankNicholson (Solvers/
+ * EP_CrankNicholson.cc:5-156). */
+typedef struct ep_solver_desc {
+    double dt;                  /* global step (ms) */
+    double ionic_dt;            /* ionic sub-step (ms) */
+    double cg_tol;              /* relative to ||r0|| (reference 1e-7) */
+    int32_t cg_maxit;           /* reference 1000 */
+    double smoothing_alpha;     /* SMOOTHING key, 0 = off */
+    int32_t precision;          /* EP_FP64 / EP_FP32 / EP_SURROGATE */
+    double newton_tol;          /* TT, 0: 1e-6 (the reference's absolute
+                                   tolerance; FP32 scales it by max(|x|,1)) */
+    int32_t ecg_every;          /* steps between pseudo-ECG samples (0 off) */
+    double act_threshold;       /* mV; activation = upward crossing (0: -40) */
+} ep_solver_desc;
+
+typedef struct ep_step_stats {
+    int64_t steps;              /* steps done by this call */
+    int64_t cg_iters;           /* CG iterations, both half-steps, all steps */
+    int32_t cg_max_iters;       /* most iterations one solve took */
+    int32_t cg_failures;        /* solves that hit cg_maxit */
+    int64_t newton_iters;       /* TT Newton iterations, all nodes and sub-steps */
+    int32_t newton_cap_hits;
+    int32_t nonfinite;          /* nodes with a non-finite V after the call */
+    int64_t fallback_nodes;     /* surrogate: node-steps run on the plain model */
+    double device_ms;           /* CUDA-event time of the call's GPU work */
+    int32_t timeouts;
+    /* per-kernel CUDA-event times, filled when profiling is on */
+    double cg_ms;               /* both CN half diffusion steps */
+    double ionic_ms;            /* ionic phase */
+    double ecg_ms;              /* pseudo-ECG samples */
+    int64_t launches;           /* kernels launched by the call */
+} ep_step_stats;
+
+/* ---- life cycle ---- */
+int  ep_version(void);
+const char *ep_last_error(void);
+/* stored-state count of a model (the reference getInternalParameters nData:
+ * TT 19, Mahajan 26, LR 8) and its constant count */
+int  ep_model_nstate(int model);
+int  ep_model_nconst(int model);
+/* reference default constants of parameter set `type` (SetUp*Parameters) */
+int  ep_model_default_consts(int model, int type, double *out);
+
+/* EPSolver::New(..., CRANKNICKOLSON) with CardiacBody::New and Compute()
+ * (Solvers/EPSolver.cc:339-362, Body/CardiacBody.cc:78-187,975-1101):
+ * assembles K, M and C_L in FP64 on the host, uploads the CN operators. */
+int  ep_create(const ep_mesh_desc *mesh, const ep_model_desc *model,
+               const ep_solver_desc *solver, int device, ep_handle **out);
+void ep_destroy(ep_handle *h);
+int  ep_num_nodes(const ep_handle *h);
+int  ep_num_states(const ep_handle *h);
+
+/* EPSolver::InitializeVoltage (Solvers/EPSolver.h:214-223) */
+int  ep_set_voltage(ep_handle *h, const double *V);
+/* the voltage field EPSolver::WriteOutput writes (Solvers/EPSolver.cc:116-152) */
+int  ep_get_voltage(ep_handle *h, double *V);
+/* CardiacBody::getStateVariables / setStateVariables
+ * (Body/CardiacBody.cc:438-463): n_nodes * nstate, node-major */
+int  ep_get_states(ep_handle *h, double *out);
+int  ep_set_states(ep_handle *h, const double *in);
+/* the resting voltage the cell models report (CardiacBody::getInitialVoltage,
+ * Body/CardiacBody.h:299-307): Mahajan State[0]; TT and LR report 0 there
+ * (IonicModel.h:42), which is what this returns for them too. */
+int  ep_get_model_voltage(ep_handle *h, double *V);
+
+/* Nodal stimuli: CardiacBody::setStimulusCurrent(nodeSet, istim) switched
+ * on/off by the EPSimulator schedule (Body/CardiacBody.cc:315-324,
+ * EPSimulator.cc:483-570).  Entry k stimulates node_ids[k] with amp[k]
+ * [uA/cm^3] for steps long(t_on/dt) <= step < long(t_off/dt).  Replaces
+ * the previous table.  A node may appear in several entries; at a given
+ * step the entry whose window covers the step and starts latest wins. */
+int  ep_set_stimulus(ep_handle *h, int32_t n, const int32_t *node_ids,
+                     const double *t_on, const double *t_off, const double *amp);
+
+/* Pseudo-ECG electrodes (ComputeECG.h:30-189 with the D of the run, or
+ * D_ecg[3] when non-NULL -- the reference post-processor hard-codes
+ * {1e-3, 5e-4, 2.5e-4}, ComputeECG.cc:88). */
+int  ep_set_electrodes(ep_handle *h, int32_t n, const double *xyz, const double *D_ecg);
+/* samples taken so far: out[s * n_electrodes + k], s < *n_samples */
+int  ep_get_ecg(ep_handle *h, double *out, int32_t max_samples, int32_t *n_samples,
+                double *t_samples);
+/* ECG of the current voltage field, computed now */
+int  ep_compute_ecg(ep_handle *h, double *out);
+
+/* Advance n_steps global steps: EP_CrankNicholson::Solve per step
+ * (half diffusion step, ionic sub-steps, half diffusion step), stimulus
+ * windows, ECG sampling and activation tracking on the device. */
+int  ep_step(ep_handle *h, int32_t n_steps, ep_step_stats *stats);
+/* Record CUDA events around every kernel of ep_step (per-kernel times in
+ * ep_step_stats); adds a few microseconds per step.  No reference
+ * counterpart (the reference has no timers). */
+int  ep_set_profiling(ep_handle *h, int on);
+/* One Crank-Nicolson half diffusion step on the current voltage, nothing
+ * else: V <- A^-1 (B V) (EP_CrankNicholson.cc:99-104).  *iters receives the
+ * CG iteration count, *relres the final ||r||/||r0||. */
+int  ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres);
+/* simulated time (ms) and step count */
+int  ep_get_time(ep_handle *h, double *t, int64_t *step);
+
+/* Activation time (first upward crossing of act_threshold, ms, -1 if none)
+ * and APD90 (ms, -1 if not repolarised) per node. */
+int  ep_get_activation(ep_handle *h, double *t_act, double *apd90);
+
+/* Reference output formats (Solvers/EPSolver.cc:116-211), rank 00:
+ * Voltage_time_%08.2f.00 (raw FP64 V) and InterVariables_time_%08.2f.00
+ * (per node int nVar + nVar FP64). */
+int  ep_write_output(ep_handle *h, double t, const char *dir);
+int  ep_write_restart(ep_handle *h, double t, const char *dir);
+int  ep_read_restart(ep_handle *h, double t, const char *dir);
+
+/* Plugin-level entry: IonicModel::Compute_Ion for a batch of independent
+ * cells (IonicModel/IonicModel.h:34-35, Body/CardiacBody.cc:405-435).
+ * states: n * nstate node-major, updated in place; dvdt[i] receives the
+ * return value.  Host buffers; runs on the current CUDA device. */
+int  ep_ionic_step(const ep_model_desc *model, int32_t precision, int32_t n,
+                   double dt, double Cm, const double *V, const double *istim,
+                   double *states, double *dvdt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

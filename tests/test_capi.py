@@ -1,0 +1,56 @@
+"""The C ABI library loads and exports every entry point include/ep_gpu.h
+declares (no compute calls: runs without a GPU)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from ucla_cmg_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_header_symbols_exported():
+    syms = capi.exported_symbols()
+    assert len(syms) >= 20
+    missing = [n for n, ok in syms if not ok]
+    assert not missing, missing
+
+
+def test_every_header_function_bound():
+    hdr = open(os.path.join(ROOT, "include", "ep_gpu.h")).read()
+    names = set(re.findall(r"\b(ep_[a-z0-9_]+)\s*\(", hdr))
+    L = capi.lib()
+    for n in names:
+        assert hasattr(L, n)
+
+
+def test_host_only_entry_points():
+    L = capi.lib()
+    assert L.ep_version() == 1
+    assert L.ep_model_nstate(capi.TUSSCHER) == 19
+    assert L.ep_model_nstate(capi.MAHAJAN) == 26
+    assert L.ep_model_nstate(capi.LUORUDY) == 8
+    assert L.ep_model_nstate(99) < 0
+    c = capi.default_consts(capi.TUSSCHER)
+    assert c[15] == 0.392 and c[20] == 0.294 and c[18] == 0.0000398 and c[53] == 0.0
+    m0 = capi.default_consts(capi.MAHAJAN, 0)
+    assert np.isclose(m0[10], 1.9 * 0.32) and np.isclose(m0[24], 96.485 / (8.314 * 308.0))
+    mf = capi.default_consts(capi.MAHAJAN_FAIL, 8)
+    assert np.isclose(mf[7], 0.12 * 0.77 * 0.67) and np.isclose(mf[10], 0.9 * 0.1386 * 0.6)
+
+
+def test_constants_match_oracle():
+    from oracle import oracle as O
+    assert np.array_equal(capi.default_consts(capi.TUSSCHER), O.tt_constants())
+    for t in range(9):
+        assert np.array_equal(capi.default_consts(capi.MAHAJAN, t), O.mh_constants(t))
+        assert np.array_equal(capi.default_consts(capi.MAHAJAN_FAIL, t), O.mh_constants(t, True))
+
+
+def test_bad_arguments_return_codes():
+    L = capi.lib()
+    h = C.c_void_p()
+    rc = L.ep_create(None, None, None, 0, C.byref(h))
+    assert rc == -1 and b"null" in L.ep_last_error()

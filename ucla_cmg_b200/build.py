@@ -1,0 +1,74 @@
+"""Build the sm_100a shared library ``libepgpu.so`` in-tree with nvcc.
+
+``python -m ucla_cmg_b200.build`` (or ``__graft_entry__.build()``) compiles
+every ``csrc/*.cu`` / ``csrc/*.cpp`` with
+``-gencode arch=compute_100a,code=sm_100a`` and links them into
+``ucla_cmg_b200/libepgpu.so``.  Objects are cached in ``_build/`` and only
+recompiled when a source or header is newer.
+"""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(ROOT, "_build")
+LIB = os.path.join(HERE, "libepgpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
+          "-I" + os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
+
+
+def _newest_header():
+    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return max((os.path.getmtime(h) for h in hs), default=0.0)
+
+
+def build(verbose=False, ptxas_info=False, jobs=8):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    hdr_t = _newest_header()
+    objs, cmds = [], []
+    for s in srcs:
+        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        objs.append(o)
+        if os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(s), hdr_t):
+            continue
+        cmd = [NVCC] + ARCH + COMMON + ["-c", s, "-o", o]
+        if ptxas_info and s.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"]
+        cmds.append(cmd)
+    procs = []
+    for cmd in cmds:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        if len(procs) >= jobs:
+            _drain(procs, verbose or ptxas_info)
+    _drain(procs, verbose or ptxas_info)
+    if cmds or not os.path.exists(LIB):
+        link = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"]
+        if verbose:
+            print(" ".join(link), flush=True)
+        subprocess.run(link, check=True)
+    return LIB
+
+
+def _drain(procs, show):
+    while procs:
+        cmd, p = procs.pop(0)
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out.decode(errors="replace"))
+            raise RuntimeError("nvcc failed: " + " ".join(cmd))
+        if show and out:
+            sys.stdout.write(out.decode(errors="replace"))
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

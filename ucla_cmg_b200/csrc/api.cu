@@ -1,0 +1,866 @@
+// api.cu -- the C ABI (include/ep_gpu.h): handle life cycle, the split
+// time-step driver, I/O in the reference formats.
+#include <cstdarg>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <string>
+#include <memory>
+
+#include "kernels.cuh"
+#include "host_fem.h"
+#include "model_defaults.h"
+
+namespace ep {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+const char *last_error() { return g_err; }
+
+// owning device buffer
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { if (p) cudaFree(p); }
+    int alloc(size_t b) {
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (b == 0) return EP_OK;
+        if (cudaMalloc(&p, b) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(%zu) failed", b);
+            return EP_ERR_NOMEM;
+        }
+        bytes = b;
+        return EP_OK;
+    }
+    template <typename T> T *as() const { return (T *)p; }
+};
+
+}  // namespace ep
+
+using namespace ep;
+
+struct ep_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int n = 0, pitch = 0, model = 0, precision = 0, nstate = 0, ns = 0, ntypes = 1;
+    size_t rsize = 8;                    // bytes per real
+    double dt = 0.1, ionic_dt = 0.1, Cm = 1.0, Xi = 0.0;
+    int nsub = 1;
+    double sub_dt[kMaxSub];
+    double cg_tol = 1e-7;
+    int cg_maxit = 1000;
+    int cg_grid = 0, cg_block = 256;
+    int ecg_every = 0;
+    double act_thr = -40.0;
+    TTOpts tt{};
+    int mh_abs = 0;
+    long long step = 0;
+    int nslices = 0;
+    // device memory
+    DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, consts, gks, lr_table, type, slice_ptr, col;
+    DBuf partial, bar, status, cg_stats, cg_last, d_step, track;
+    DBuf stim_head, stim_next, stim_on, stim_off, stim_amp;
+    int nstim = 0;
+    DBuf W, ecg_buf, ecg_partial, ecg_counter;
+    int ne = 0, ecg_cap = 0, ecg_count = 0, ecg_grid = 0;
+    std::vector<double> ecg_t;
+    std::vector<double> model_V0;        // IonicModel::getVoltage() per node
+    // mesh kept for the ECG weights
+    std::vector<double> xyz, fibers;
+    std::vector<int> tets;
+    double D[3] = {0, 0, 0};
+    // per-kernel timing
+    int profile = 0;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pkind;              // kernel class started at each event
+    long long launches = 0;
+};
+
+namespace {
+
+template <typename R>
+int upload(DBuf &b, const std::vector<double> &h, size_t count = 0) {
+    const size_t n = count ? count : h.size();
+    int rc = b.alloc(n * sizeof(R));
+    if (rc) return rc;
+    std::vector<R> tmp(n, R(0));
+    for (size_t i = 0; i < std::min(n, h.size()); i++) tmp[i] = (R)h[i];
+    EP_CUDA(cudaMemcpy(b.p, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice));
+    return EP_OK;
+}
+
+template <typename T>
+int upload_raw(DBuf &b, const T *h, size_t n) {
+    int rc = b.alloc(n * sizeof(T));
+    if (rc) return rc;
+    if (n) EP_CUDA(cudaMemcpy(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return EP_OK;
+}
+
+template <typename R>
+int download(const DBuf &b, std::vector<double> &h, size_t n, cudaStream_t s) {
+    std::vector<R> tmp(n);
+    EP_CUDA(cudaMemcpyAsync(tmp.data(), b.p, n * sizeof(R), cudaMemcpyDeviceToHost, s));
+    EP_CUDA(cudaStreamSynchronize(s));
+    h.resize(n);
+    for (size_t i = 0; i < n; i++) h[i] = (double)tmp[i];
+    return EP_OK;
+}
+
+bool is_mh(int m) { return m == EP_MAHAJAN || m == EP_MAHAJAN_FAIL; }
+bool is_lr(int m) { return m == EP_LUORUDY || m == EP_LUORUDYWITHGATE; }
+
+// sub-step sequence of one ionic phase (EP_CrankNicholson.cc:114-143),
+// computed with the reference's own double arithmetic
+int substeps(double dt, double idt, double *out) {
+    double total = 0.0, h = (idt < dt) ? idt : dt;
+    int k = 0;
+    while (total < dt) {
+        if (k >= kMaxSub) return -1;
+        out[k++] = h;
+        total += h;
+        h = (total + h < dt) ? h : dt - total;
+    }
+    return k;
+}
+
+template <typename R>
+void fill_ionic_args(ep_handle *h, IonicArgs<R> &a) {
+    std::memset(&a, 0, sizeof a);
+    a.n = h->n; a.pitch = h->pitch;
+    a.V = h->V.as<R>(); a.S = h->S.as<R>();
+    a.type = h->type.as<uint8_t>();
+    a.gks = h->gks.as<R>();
+    a.stim_head = h->nstim ? h->stim_head.as<int>() : nullptr;
+    a.stim_next = h->stim_next.as<int>();
+    a.stim_on = h->stim_on.as<long long>();
+    a.stim_off = h->stim_off.as<long long>();
+    a.stim_amp = h->stim_amp.as<R>();
+    a.step_ptr = h->d_step.as<long long>();
+    a.t_per_step = h->dt;
+    a.Cm = (R)h->Cm; a.Xi = (R)h->Xi;
+    a.nsub = h->nsub;
+    for (int k = 0; k < h->nsub; k++) a.sub_dt[k] = (R)h->sub_dt[k];
+    a.act_thr = (R)h->act_thr;
+    a.track = h->track.as<Track>();
+    a.status = h->status.as<DevStatus>();
+    a.consts = h->consts.as<R>();
+    a.nconst = ep_model_nconst(h->model);
+    a.dvdt_out = nullptr;
+    a.tt = h->tt;
+    a.mh_abs = h->mh_abs;
+    a.lr_table = h->lr_table.as<R>();
+}
+
+template <typename R>
+void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
+    a.n = h->n; a.nslices = h->nslices;
+    a.slice_ptr = h->slice_ptr.as<int>(); a.col = h->col.as<int>();
+    a.Aval = h->Aval.as<R>(); a.Bval = h->Bval.as<R>(); a.dinv = h->dinv.as<R>();
+    a.x = h->V.as<R>(); a.r = h->r.as<R>(); a.q = h->q.as<R>();
+    a.p0 = h->p0.as<R>(); a.p1 = h->p1.as<R>();
+    a.partial = h->partial.as<double>();
+    a.bar = h->bar.as<GridBarrier>();
+    a.tol = h->cg_tol; a.maxit = h->cg_maxit;
+    a.floor_rel = sizeof(R) == 4 ? 1.2e-7 : 2.2e-16;   // unit roundoff of R
+    unsigned long long *st = h->cg_stats.as<unsigned long long>();
+    a.iters_total = st;
+    a.iters_max = (unsigned int *)(st + 1);
+    a.fails = (unsigned int *)(st + 1) + 1;
+    a.last = h->cg_last.as<double>();
+}
+
+template <typename R>
+int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &states_nm,
+                 const std::vector<double> &consts, const ep_model_desc *md) {
+    const int n = h->n;
+    int rc;
+    // operators
+    Sell sell;
+    pack_sell(csr, {&csr.A, &csr.B}, sell);
+    h->nslices = sell.nslices;
+    if ((rc = upload_raw(h->slice_ptr, sell.slice_ptr.data(), sell.slice_ptr.size()))) return rc;
+    if ((rc = upload_raw(h->col, sell.col.data(), sell.col.size()))) return rc;
+    if ((rc = upload<R>(h->Aval, sell.vals[0]))) return rc;
+    if ((rc = upload<R>(h->Bval, sell.vals[1]))) return rc;
+    std::vector<double> dinv(h->pitch, 1.0);
+    for (int i = 0; i < n; i++) {
+        double d = 0.0;
+        for (int k = csr.rowptr[i]; k < csr.rowptr[i + 1]; k++) if (csr.col[k] == i) d = csr.A[k];
+        dinv[i] = 1.0 / d;
+    }
+    if ((rc = upload<R>(h->dinv, dinv))) return rc;
+    const size_t vb = (size_t)h->pitch * sizeof(R);
+    if ((rc = h->r.alloc(vb)) || (rc = h->q.alloc(vb)) || (rc = h->p0.alloc(vb)) || (rc = h->p1.alloc(vb)))
+        return rc;
+    EP_CUDA(cudaMemset(h->r.p, 0, vb)); EP_CUDA(cudaMemset(h->q.p, 0, vb));
+    EP_CUDA(cudaMemset(h->p0.p, 0, vb)); EP_CUDA(cudaMemset(h->p1.p, 0, vb));
+    // cell states (SoA) and voltage
+    std::vector<double> V(h->pitch, 0.0), S((size_t)h->ns * h->pitch, 0.0);
+    const int off = is_lr(h->model) ? 0 : 1;       // LR keeps V in slot 7
+    for (int i = 0; i < n; i++) {
+        const double *s = &states_nm[(size_t)i * h->nstate];
+        if (is_lr(h->model)) {
+            V[i] = s[7];
+            for (int k = 0; k < 7; k++) S[(size_t)k * h->pitch + i] = s[k];
+        } else {
+            V[i] = s[0];
+            for (int k = 0; k < h->ns; k++) S[(size_t)k * h->pitch + i] = s[k + off];
+        }
+    }
+    if ((rc = upload<R>(h->V, V))) return rc;
+    if ((rc = upload<R>(h->S, S))) return rc;
+    if ((rc = upload<R>(h->consts, consts))) return rc;
+    if (md->node_gks_scale) {
+        std::vector<double> g(md->node_gks_scale, md->node_gks_scale + n);
+        if ((rc = upload<R>(h->gks, g))) return rc;
+    }
+    if (h->model == EP_LUORUDYWITHGATE) {
+        std::vector<double> tab;
+        lr_gate_table(tab);
+        if ((rc = upload<R>(h->lr_table, tab))) return rc;
+    }
+    rc = cg_grid_size<R>(h->cg_block, &h->cg_grid);
+    return rc;
+}
+
+}  // namespace
+
+static int ensure_ecg_cap(ep_handle *h, int need) {
+    if (need <= h->ecg_cap) return EP_OK;
+    int cap = std::max(need, std::max(64, 2 * h->ecg_cap));
+    DBuf nb;
+    int rc = nb.alloc(sizeof(double) * (size_t)cap * std::max(1, h->ne));
+    if (rc) return rc;
+    if (h->ecg_count)
+        EP_CUDA(cudaMemcpyAsync(nb.p, h->ecg_buf.p, sizeof(double) * (size_t)h->ecg_count * h->ne,
+                                cudaMemcpyDeviceToDevice, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    std::swap(h->ecg_buf.p, nb.p);
+    std::swap(h->ecg_buf.bytes, nb.bytes);
+    h->ecg_cap = cap;
+    return EP_OK;
+}
+
+enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
+
+// event before each kernel when profiling (the class of the kernel it starts)
+static int mark(ep_handle *h, size_t &ne, int kind) {
+    if (!h->profile) return EP_OK;
+    if (ne == h->pev.size()) {
+        cudaEvent_t e;
+        EP_CUDA(cudaEventCreate(&e));
+        h->pev.push_back(e);
+        h->pkind.push_back(kind);
+    }
+    h->pkind[ne] = kind;
+    EP_CUDA(cudaEventRecord(h->pev[ne], h->stream));
+    ne++;
+    return EP_OK;
+}
+
+template <typename R>
+static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
+    IonicArgs<R> ia;
+    fill_ionic_args<R>(h, ia);
+    CGArgs<R> ca;
+    fill_cg_args<R>(h, ca);
+    int rc;
+    for (int s = 0; s < nsteps; s++) {
+        if ((rc = mark(h, ne, K_CG))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
+        if ((rc = mark(h, ne, K_IONIC))) return rc;
+        if ((rc = launch_ionic<R>(h->model, ia, h->stream))) return rc;
+        if ((rc = mark(h, ne, K_CG))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
+        if ((rc = mark(h, ne, K_OTHER))) return rc;
+        launch_step_inc(h->d_step.as<long long>(), h->stream);
+        h->launches += 4;
+        h->step++;
+        if (h->ecg_every && h->ne > 0 && h->step % h->ecg_every == 0) {
+            if ((rc = mark(h, ne, K_ECG))) return rc;
+            rc = launch_ecg<R>(h->n, h->ne, h->W.as<R>(), h->pitch, h->V.as<R>(), h->ecg_partial.as<double>(),
+                               h->ecg_counter.as<unsigned int>(),
+                               h->ecg_buf.as<double>() + (size_t)h->ecg_count * h->ne, h->ecg_grid, h->stream);
+            if (rc) return rc;
+            h->launches += 1;
+            h->ecg_count++;
+            h->ecg_t.push_back((double)h->step * h->dt);
+        }
+    }
+    return mark(h, ne, K_OTHER);
+}
+
+
+static std::string out_name(const char *dir, const char *stem, double t) {
+    char buf[1024];
+    snprintf(buf, sizeof buf, "%s/%s_time_%08.2f.%02.0f", dir, stem, t, 0.0);
+    return buf;
+}
+
+
+extern "C" {
+
+int ep_version(void) { return EP_ABI_VERSION; }
+const char *ep_last_error(void) { return ep::last_error(); }
+
+int ep_model_nstate(int model) {
+    switch (model) {
+    case EP_TUSSCHER: return 19;
+    case EP_MAHAJAN: case EP_MAHAJAN_FAIL: return 26;
+    case EP_LUORUDY: case EP_LUORUDYWITHGATE: return 8;
+    default: return EP_ERR_ARG;
+    }
+}
+
+int ep_model_nconst(int model) {
+    switch (model) {
+    case EP_TUSSCHER: return TT_NC;
+    case EP_MAHAJAN: case EP_MAHAJAN_FAIL: return MH_NC;
+    case EP_LUORUDY: case EP_LUORUDYWITHGATE: return 1;
+    default: return EP_ERR_ARG;
+    }
+}
+
+int ep_model_default_consts(int model, int type, double *out) {
+    EP_CHECK_ARG(out != nullptr, "null output");
+    return default_consts(model, type, out);
+}
+
+void ep_destroy(ep_handle *h) {
+    if (!h) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    cudaSetDevice(cur);
+}
+
+int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver_desc *sd,
+              int device, ep_handle **out) {
+    EP_CHECK_ARG(mesh && md && sd && out, "null descriptor");
+    *out = nullptr;
+    EP_CHECK_ARG(mesh->n_nodes > 0 && mesh->n_tets > 0 && mesh->xyz && mesh->tets, "empty mesh");
+    const int nst = ep_model_nstate(md->model);
+    EP_CHECK_ARG(nst > 0, "unknown cell model");
+    EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32, "unsupported precision");
+    EP_CHECK_ARG(sd->dt > 0 && sd->ionic_dt > 0, "dt and ionic_dt must be positive");
+    const int ntypes = md->n_types > 0 ? md->n_types : 1;
+    EP_CHECK_ARG(ntypes <= kMaxTypes, "too many parameter sets");
+    std::unique_ptr<ep_handle> h(new ep_handle());
+    h->device = device;
+    EP_CUDA(cudaSetDevice(device));
+    const int n = mesh->n_nodes, m = mesh->n_tets;
+    h->n = n;
+    h->pitch = (n + 31) / 32 * 32;
+    h->model = md->model;
+    h->precision = sd->precision;
+    h->rsize = sd->precision == EP_FP64 ? 8 : 4;
+    h->nstate = nst;
+    h->ns = is_lr(md->model) ? 7 : nst - 1;
+    h->ntypes = ntypes;
+    h->dt = sd->dt; h->ionic_dt = sd->ionic_dt;
+    h->nsub = substeps(sd->dt, sd->ionic_dt, h->sub_dt);
+    EP_CHECK_ARG(h->nsub > 0, "more than 64 ionic sub-steps per step");
+    h->Cm = mesh->Cm > 0 ? mesh->Cm : 1.0;
+    h->cg_tol = sd->cg_tol > 0 ? sd->cg_tol : 1e-7;
+    h->cg_maxit = sd->cg_maxit > 0 ? sd->cg_maxit : 1000;
+    h->ecg_every = sd->ecg_every > 0 ? sd->ecg_every : 0;
+    h->act_thr = sd->act_threshold != 0.0 ? sd->act_threshold : -40.0;
+    h->Xi = md->user_xi > 0 ? md->user_xi : model_xi(md->model);
+    h->tt.newton_cap = md->newton_cap > 0 ? md->newton_cap : 100;
+    h->tt.jac_true = md->tt_jacobian == EP_TT_JAC_TRUE ? 1 : 0;
+    h->tt.fp32_scaled_tol = sd->precision == EP_FP64 ? 0 : 1;
+    h->tt.newton_tol = sd->newton_tol > 0 ? sd->newton_tol : 1e-6;
+    h->mh_abs = md->mh_abs_mode ? 1 : 0;
+    for (int k = 0; k < 3; k++) h->D[k] = mesh->D[k];
+    // mesh (zero-based)
+    h->xyz.assign(mesh->xyz, mesh->xyz + 3 * (size_t)n);
+    h->tets.resize((size_t)m * 4);
+    for (size_t k = 0; k < (size_t)m * 4; k++) {
+        const int v = mesh->tets[k] - (mesh->one_based ? 1 : 0);
+        EP_CHECK_ARG(v >= 0 && v < n, "tet node id out of range");
+        h->tets[k] = v;
+    }
+    if (mesh->fibers) h->fibers.assign(mesh->fibers, mesh->fibers + 9 * (size_t)m);
+    // FEM operators in FP64
+    HostCSR csr;
+    if (assemble_cn(n, h->xyz.data(), m, h->tets.data(), mesh->fibers ? h->fibers.data() : nullptr,
+                    mesh->D, h->Cm, h->dt, sd->smoothing_alpha, csr) != 0) {
+        set_error("mesh has an element with non-positive volume");
+        return EP_ERR_MESH;
+    }
+    // parameter sets
+    const int nc = ep_model_nconst(md->model);
+    std::vector<double> consts((size_t)ntypes * nc);
+    for (int t = 0; t < ntypes; t++) {
+        if (md->type_consts) std::memcpy(&consts[(size_t)t * nc], md->type_consts + (size_t)t * nc, sizeof(double) * nc);
+        else default_consts(md->model, t, &consts[(size_t)t * nc]);
+    }
+    // initial states, node-major like InterVariables
+    std::vector<double> st((size_t)n * nst);
+    for (int i = 0; i < n; i++) {
+        const int t = md->node_type ? md->node_type[i] : 0;
+        if (md->node_type) EP_CHECK_ARG(t < ntypes, "node type beyond n_types");
+        if (md->initial_states) std::memcpy(&st[(size_t)i * nst], md->initial_states + (size_t)i * nst, sizeof(double) * nst);
+        else default_state(md->model, t, &st[(size_t)i * nst]);
+    }
+    h->model_V0.assign(n, 0.0);
+    if (is_mh(md->model))
+        for (int i = 0; i < n; i++) h->model_V0[i] = st[(size_t)i * nst];
+    int rc = EP_OK;
+    EP_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    EP_CUDA(cudaEventCreate(&h->ev0));
+    EP_CUDA(cudaEventCreate(&h->ev1));
+    if (md->node_type) {
+        if ((rc = upload_raw(h->type, md->node_type, (size_t)n))) return rc;
+    }
+    if (h->precision == EP_FP64) rc = create_typed<double>(h.get(), csr, st, consts, md);
+    else rc = create_typed<float>(h.get(), csr, st, consts, md);
+    if (rc) return rc;
+    // solver scratch and status
+    if ((rc = h->partial.alloc(sizeof(double) * 4 * (size_t)h->cg_grid))) return rc;
+    if ((rc = h->bar.alloc(sizeof(GridBarrier)))) return rc;
+    if ((rc = h->status.alloc(sizeof(DevStatus)))) return rc;
+    if ((rc = h->cg_stats.alloc(32))) return rc;
+    if ((rc = h->cg_last.alloc(2 * sizeof(double)))) return rc;
+    if ((rc = h->d_step.alloc(sizeof(long long)))) return rc;
+    EP_CUDA(cudaMemset(h->bar.p, 0, sizeof(GridBarrier)));
+    EP_CUDA(cudaMemset(h->status.p, 0, sizeof(DevStatus)));
+    EP_CUDA(cudaMemset(h->cg_stats.p, 0, 32));
+    EP_CUDA(cudaMemset(h->d_step.p, 0, sizeof(long long)));
+    std::vector<Track> tr(n, Track{-1.f, -1.f, -1.f, 1e30f});
+    if ((rc = upload_raw(h->track, tr.data(), tr.size()))) return rc;
+    EP_CUDA(cudaDeviceSynchronize());
+    *out = h.release();
+    return EP_OK;
+}
+
+int ep_num_nodes(const ep_handle *h) { return h ? h->n : EP_ERR_ARG; }
+int ep_num_states(const ep_handle *h) { return h ? h->nstate : EP_ERR_ARG; }
+
+int ep_set_voltage(ep_handle *h, const double *V) {
+    EP_CHECK_ARG(h && V, "null argument");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<double> v(V, V + h->n);
+    int rc = h->precision == EP_FP64 ? upload<double>(h->V, v, h->pitch) : upload<float>(h->V, v, h->pitch);
+    return rc;
+}
+
+int ep_get_voltage(ep_handle *h, double *V) {
+    EP_CHECK_ARG(h && V, "null argument");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<double> v;
+    int rc = h->precision == EP_FP64 ? download<double>(h->V, v, h->n, h->stream)
+                                     : download<float>(h->V, v, h->n, h->stream);
+    if (rc) return rc;
+    std::memcpy(V, v.data(), sizeof(double) * h->n);
+    return EP_OK;
+}
+
+int ep_get_model_voltage(ep_handle *h, double *V) {
+    EP_CHECK_ARG(h && V, "null argument");
+    std::memcpy(V, h->model_V0.data(), sizeof(double) * h->n);
+    return EP_OK;
+}
+
+int ep_get_states(ep_handle *h, double *out) {
+    EP_CHECK_ARG(h && out, "null argument");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<double> S, V;
+    const size_t tot = (size_t)h->ns * h->pitch;
+    int rc = h->precision == EP_FP64 ? download<double>(h->S, S, tot, h->stream)
+                                     : download<float>(h->S, S, tot, h->stream);
+    if (rc) return rc;
+    std::vector<double> v(h->n);
+    if ((rc = ep_get_voltage(h, v.data()))) return rc;
+    for (int i = 0; i < h->n; i++) {
+        double *o = out + (size_t)i * h->nstate;
+        if (is_lr(h->model)) {
+            for (int k = 0; k < 7; k++) o[k] = S[(size_t)k * h->pitch + i];
+            o[7] = v[i];
+        } else {
+            o[0] = v[i];
+            for (int k = 0; k < h->ns; k++) o[k + 1] = S[(size_t)k * h->pitch + i];
+        }
+    }
+    return EP_OK;
+}
+
+int ep_set_states(ep_handle *h, const double *in) {
+    EP_CHECK_ARG(h && in, "null argument");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<double> S((size_t)h->ns * h->pitch, 0.0);
+    for (int i = 0; i < h->n; i++) {
+        const double *s = in + (size_t)i * h->nstate;
+        if (is_lr(h->model)) for (int k = 0; k < 7; k++) S[(size_t)k * h->pitch + i] = s[k];
+        else for (int k = 0; k < h->ns; k++) S[(size_t)k * h->pitch + i] = s[k + 1];
+    }
+    return h->precision == EP_FP64 ? upload<double>(h->S, S) : upload<float>(h->S, S);
+}
+
+int ep_set_stimulus(ep_handle *h, int32_t n, const int32_t *ids, const double *t_on,
+                    const double *t_off, const double *amp) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CHECK_ARG(n >= 0 && (n == 0 || (ids && t_on && t_off && amp)), "bad stimulus table");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<int> head(h->n, -1), next(n, -1);
+    std::vector<long long> on(n), off(n);
+    std::vector<double> a(n);
+    for (int k = 0; k < n; k++) {
+        EP_CHECK_ARG(ids[k] >= 0 && ids[k] < h->n, "stimulus node id out of range");
+        next[k] = head[ids[k]];
+        head[ids[k]] = k;
+        on[k] = (long long)(t_on[k] / h->dt);      // long(t/dt) as EPSimulator.cc:487-488
+        off[k] = (long long)(t_off[k] / h->dt);
+        a[k] = amp[k];
+    }
+    int rc;
+    if ((rc = upload_raw(h->stim_head, head.data(), head.size()))) return rc;
+    if ((rc = upload_raw(h->stim_next, next.data(), next.size()))) return rc;
+    if ((rc = upload_raw(h->stim_on, on.data(), on.size()))) return rc;
+    if ((rc = upload_raw(h->stim_off, off.data(), off.size()))) return rc;
+    rc = h->precision == EP_FP64 ? upload<double>(h->stim_amp, a) : upload<float>(h->stim_amp, a);
+    h->nstim = n;
+    return rc;
+}
+
+int ep_set_electrodes(ep_handle *h, int32_t ne, const double *xyz, const double *D_ecg) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CHECK_ARG(ne >= 0 && ne <= 16 && (ne == 0 || xyz), "1..16 electrodes");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    const double *D = D_ecg ? D_ecg : h->D;
+    std::vector<double> W;
+    ecg_weights(h->n, h->xyz.data(), (int)(h->tets.size() / 4), h->tets.data(),
+                h->fibers.empty() ? nullptr : h->fibers.data(), D, ne, xyz, W);
+    // pad each electrode row to the pitch
+    std::vector<double> Wp((size_t)ne * h->pitch, 0.0);
+    for (int k = 0; k < ne; k++)
+        std::memcpy(&Wp[(size_t)k * h->pitch], &W[(size_t)k * h->n], sizeof(double) * h->n);
+    int rc = h->precision == EP_FP64 ? upload<double>(h->W, Wp) : upload<float>(h->W, Wp);
+    if (rc) return rc;
+    h->ne = ne;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    h->ecg_grid = std::max(1, std::min(nsm * 4, div_up(h->n, 256)));
+    if ((rc = h->ecg_partial.alloc(sizeof(double) * 16 * (size_t)h->ecg_grid))) return rc;
+    if ((rc = h->ecg_counter.alloc(sizeof(unsigned int)))) return rc;
+    EP_CUDA(cudaMemset(h->ecg_counter.p, 0, sizeof(unsigned int)));
+    h->ecg_cap = 0; h->ecg_count = 0; h->ecg_t.clear();
+    h->ecg_buf.alloc(0);
+    return EP_OK;
+}
+
+int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
+    EP_CHECK_ARG(h && nsteps >= 0, "bad arguments");
+    EP_CUDA(cudaSetDevice(h->device));
+    if (h->ecg_every && h->ne > 0) {
+        int rc = ensure_ecg_cap(h, h->ecg_count + nsteps / h->ecg_every + 1);
+        if (rc) return rc;
+    }
+    EP_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(DevStatus), h->stream));
+    EP_CUDA(cudaMemsetAsync(h->cg_stats.p, 0, 32, h->stream));
+    EP_CUDA(cudaEventRecord(h->ev0, h->stream));
+    size_t ne = 0;
+    h->launches = 0;
+    int rc = h->precision == EP_FP64 ? step_typed<double>(h, nsteps, ne) : step_typed<float>(h, nsteps, ne);
+    if (rc) return rc;
+    EP_CUDA(cudaEventRecord(h->ev1, h->stream));
+    EP_CUDA(cudaEventSynchronize(h->ev1));
+    double kms[4] = {0, 0, 0, 0};
+    for (size_t k = 0; k + 1 < ne; k++) {
+        float e = 0.f;
+        EP_CUDA(cudaEventElapsedTime(&e, h->pev[k], h->pev[k + 1]));
+        kms[h->pkind[k]] += e;
+    }
+    DevStatus st;
+    unsigned long long cgs[4];
+    GridBarrier bar;
+    EP_CUDA(cudaMemcpy(&st, h->status.p, sizeof st, cudaMemcpyDeviceToHost));
+    EP_CUDA(cudaMemcpy(cgs, h->cg_stats.p, 32, cudaMemcpyDeviceToHost));
+    EP_CUDA(cudaMemcpy(&bar, h->bar.p, sizeof bar, cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    EP_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->steps = nsteps;
+        stats->cg_iters = (int64_t)cgs[0];
+        stats->cg_max_iters = (int32_t)((unsigned int *)(cgs + 1))[0];
+        stats->cg_failures = (int32_t)((unsigned int *)(cgs + 1))[1];
+        stats->newton_iters = (int64_t)st.newton_iters;
+        stats->newton_cap_hits = (int32_t)st.newton_cap_hits;
+        stats->nonfinite = (int32_t)st.nonfinite;
+        stats->fallback_nodes = (int64_t)st.fallback;
+        stats->device_ms = ms;
+        stats->timeouts = (int32_t)bar.err;
+        stats->cg_ms = kms[K_CG];
+        stats->ionic_ms = kms[K_IONIC];
+        stats->ecg_ms = kms[K_ECG];
+        stats->launches = h->launches;
+    }
+    if (bar.err) {
+        set_error("a grid barrier wait gave up");
+        return EP_ERR_TIMEOUT;
+    }
+    return EP_OK;
+}
+
+int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CUDA(cudaSetDevice(h->device));
+    int rc;
+    if (h->precision == EP_FP64) {
+        CGArgs<double> ca;
+        fill_cg_args<double>(h, ca);
+        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream);
+    } else {
+        CGArgs<float> ca;
+        fill_cg_args<float>(h, ca);
+        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream);
+    }
+    if (rc) return rc;
+    double last[2];
+    EP_CUDA(cudaMemcpyAsync(last, h->cg_last.p, sizeof last, cudaMemcpyDeviceToHost, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    GridBarrier bar;
+    EP_CUDA(cudaMemcpy(&bar, h->bar.p, sizeof bar, cudaMemcpyDeviceToHost));
+    if (iters) *iters = (int32_t)last[0];
+    if (relres) *relres = last[1];
+    if (bar.err) { set_error("a grid barrier wait gave up"); return EP_ERR_TIMEOUT; }
+    return EP_OK;
+}
+
+int ep_set_profiling(ep_handle *h, int on) {
+    EP_CHECK_ARG(h, "null handle");
+    h->profile = on ? 1 : 0;
+    return EP_OK;
+}
+
+int ep_get_time(ep_handle *h, double *t, int64_t *step) {
+    EP_CHECK_ARG(h, "null handle");
+    if (t) *t = (double)h->step * h->dt;
+    if (step) *step = h->step;
+    return EP_OK;
+}
+
+int ep_get_ecg(ep_handle *h, double *out, int32_t max_samples, int32_t *n_samples, double *t_samples) {
+    EP_CHECK_ARG(h && n_samples, "null argument");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    const int cnt = std::min(h->ecg_count, std::max(0, max_samples));
+    *n_samples = h->ecg_count;
+    if (out && cnt > 0 && h->ne > 0)
+        EP_CUDA(cudaMemcpy(out, h->ecg_buf.p, sizeof(double) * (size_t)cnt * h->ne, cudaMemcpyDeviceToHost));
+    if (t_samples) for (int s = 0; s < cnt; s++) t_samples[s] = h->ecg_t[s];
+    return EP_OK;
+}
+
+int ep_compute_ecg(ep_handle *h, double *out) {
+    EP_CHECK_ARG(h && out, "null argument");
+    EP_CHECK_ARG(h->ne > 0, "no electrodes set");
+    EP_CUDA(cudaSetDevice(h->device));
+    DBuf tmp;
+    int rc = tmp.alloc(sizeof(double) * h->ne);
+    if (rc) return rc;
+    if (h->precision == EP_FP64)
+        rc = launch_ecg<double>(h->n, h->ne, h->W.as<double>(), h->pitch, h->V.as<double>(),
+                                h->ecg_partial.as<double>(), h->ecg_counter.as<unsigned int>(),
+                                tmp.as<double>(), h->ecg_grid, h->stream);
+    else
+        rc = launch_ecg<float>(h->n, h->ne, h->W.as<float>(), h->pitch, h->V.as<float>(),
+                               h->ecg_partial.as<double>(), h->ecg_counter.as<unsigned int>(),
+                               tmp.as<double>(), h->ecg_grid, h->stream);
+    if (rc) return rc;
+    EP_CUDA(cudaMemcpyAsync(out, tmp.p, sizeof(double) * h->ne, cudaMemcpyDeviceToHost, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    return EP_OK;
+}
+
+int ep_get_activation(ep_handle *h, double *t_act, double *apd90) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<Track> tr(h->n);
+    EP_CUDA(cudaMemcpy(tr.data(), h->track.p, sizeof(Track) * h->n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < h->n; i++) {
+        if (t_act) t_act[i] = tr[i].t_act;
+        if (apd90) apd90[i] = (tr[i].t_act >= 0.f && tr[i].t_rep >= 0.f) ? (double)tr[i].t_rep - tr[i].t_act : -1.0;
+    }
+    return EP_OK;
+}
+
+int ep_write_output(ep_handle *h, double t, const char *dir) {
+    EP_CHECK_ARG(h && dir, "null argument");
+    std::vector<double> v(h->n);
+    int rc = ep_get_voltage(h, v.data());
+    if (rc) return rc;
+    const std::string name = out_name(dir, "Voltage", t);
+    FILE *f = fopen(name.c_str(), "wb");
+    if (!f) { set_error("cannot create %s", name.c_str()); return EP_ERR_IO; }
+    const size_t w = fwrite(v.data(), sizeof(double), v.size(), f);
+    fclose(f);
+    if (w != v.size()) { set_error("short write %s", name.c_str()); return EP_ERR_IO; }
+    return EP_OK;
+}
+
+int ep_write_restart(ep_handle *h, double t, const char *dir) {
+    EP_CHECK_ARG(h && dir, "null argument");
+    std::vector<double> s((size_t)h->n * h->nstate);
+    int rc = ep_get_states(h, s.data());
+    if (rc) return rc;
+    const std::string name = out_name(dir, "InterVariables", t);
+    FILE *f = fopen(name.c_str(), "wb");
+    if (!f) { set_error("cannot create %s", name.c_str()); return EP_ERR_IO; }
+    const int nv = h->nstate;
+    bool ok = true;
+    for (int i = 0; i < h->n && ok; i++) {
+        ok = fwrite(&nv, sizeof(int), 1, f) == 1 &&
+             fwrite(&s[(size_t)i * nv], sizeof(double), nv, f) == (size_t)nv;
+    }
+    fclose(f);
+    if (!ok) { set_error("short write %s", name.c_str()); return EP_ERR_IO; }
+    return EP_OK;
+}
+
+int ep_read_restart(ep_handle *h, double t, const char *dir) {
+    EP_CHECK_ARG(h && dir, "null argument");
+    const std::string vn = out_name(dir, "Voltage", t), sn = out_name(dir, "InterVariables", t);
+    FILE *fv = fopen(vn.c_str(), "rb");
+    if (!fv) { set_error("cannot open %s", vn.c_str()); return EP_ERR_IO; }
+    std::vector<double> v(h->n);
+    const size_t got = fread(v.data(), sizeof(double), h->n, fv);
+    fclose(fv);
+    if (got != (size_t)h->n) { set_error("truncated %s", vn.c_str()); return EP_ERR_IO; }
+    FILE *fs = fopen(sn.c_str(), "rb");
+    if (!fs) { set_error("cannot open %s", sn.c_str()); return EP_ERR_IO; }
+    std::vector<double> s((size_t)h->n * h->nstate);
+    for (int i = 0; i < h->n; i++) {
+        int nv = 0;
+        if (fread(&nv, sizeof(int), 1, fs) != 1 || nv != h->nstate ||
+            fread(&s[(size_t)i * nv], sizeof(double), nv, fs) != (size_t)nv) {
+            fclose(fs);
+            set_error("truncated or mismatched %s at node %d", sn.c_str(), i);
+            return EP_ERR_IO;
+        }
+    }
+    fclose(fs);
+    int rc = ep_set_states(h, s.data());
+    if (rc) return rc;
+    rc = ep_set_voltage(h, v.data());
+    if (rc) return rc;
+    h->step = (long long)(t / h->dt);   // count = long(simtime/dt), EPSimulator.cc:499
+    EP_CUDA(cudaMemcpy(h->d_step.p, &h->step, sizeof(long long), cudaMemcpyHostToDevice));
+    return EP_OK;
+}
+
+int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double dt, double Cm,
+                  const double *V, const double *istim, double *states, double *dvdt) {
+    EP_CHECK_ARG(md && V && states && dvdt && n > 0, "bad arguments");
+    EP_CHECK_ARG(precision == EP_FP64 || precision == EP_FP32, "unsupported precision");
+    const int nst = ep_model_nstate(md->model);
+    EP_CHECK_ARG(nst > 0, "unknown model");
+    const int ntypes = md->n_types > 0 ? md->n_types : 1;
+    EP_CHECK_ARG(ntypes <= kMaxTypes, "too many parameter sets");
+    ep_handle h;
+    cudaGetDevice(&h.device);
+    h.n = n; h.pitch = (n + 31) / 32 * 32; h.model = md->model; h.precision = precision;
+    h.nstate = nst; h.ns = is_lr(md->model) ? 7 : nst - 1; h.ntypes = ntypes;
+    h.dt = dt; h.nsub = 1; h.sub_dt[0] = dt; h.Cm = Cm;
+    h.Xi = md->user_xi > 0 ? md->user_xi : model_xi(md->model);
+    h.tt.newton_cap = md->newton_cap > 0 ? md->newton_cap : 100;
+    h.tt.jac_true = md->tt_jacobian == EP_TT_JAC_TRUE ? 1 : 0;
+    h.tt.fp32_scaled_tol = precision == EP_FP64 ? 0 : 1;
+    h.tt.newton_tol = 1e-6;
+    h.mh_abs = md->mh_abs_mode ? 1 : 0;
+    const int nc = ep_model_nconst(md->model);
+    std::vector<double> consts((size_t)ntypes * nc);
+    for (int t = 0; t < ntypes; t++) {
+        if (md->type_consts) std::memcpy(&consts[(size_t)t * nc], md->type_consts + (size_t)t * nc, sizeof(double) * nc);
+        else default_consts(md->model, t, &consts[(size_t)t * nc]);
+    }
+    std::vector<double> S((size_t)h.ns * h.pitch, 0.0), Vv(h.pitch, 0.0), ist(h.pitch, 0.0);
+    for (int i = 0; i < n; i++) {
+        const double *s = states + (size_t)i * nst;
+        if (is_lr(md->model)) for (int k = 0; k < 7; k++) S[(size_t)k * h.pitch + i] = s[k];
+        else for (int k = 0; k < h.ns; k++) S[(size_t)k * h.pitch + i] = s[k + 1];
+        Vv[i] = V[i];
+        ist[i] = istim ? istim[i] : 0.0;
+    }
+    // the stimulus enters as one window per node covering step 0
+    std::vector<int> head(n), next(n, -1);
+    std::vector<long long> on(n, 0), off(n, 1);
+    for (int i = 0; i < n; i++) head[i] = i;
+    DBuf dvd;
+    int rc;
+    EP_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    auto run = [&](auto tag) -> int {
+        using R = decltype(tag);
+        int r2;
+        if ((r2 = upload<R>(h.S, S)) || (r2 = upload<R>(h.V, Vv)) || (r2 = upload<R>(h.consts, consts)) ||
+            (r2 = upload<R>(h.stim_amp, ist)))
+            return r2;
+        if ((r2 = upload_raw(h.stim_head, head.data(), n)) || (r2 = upload_raw(h.stim_next, next.data(), n)) ||
+            (r2 = upload_raw(h.stim_on, on.data(), n)) || (r2 = upload_raw(h.stim_off, off.data(), n)))
+            return r2;
+        h.nstim = n;
+        if (md->node_type && (r2 = upload_raw(h.type, md->node_type, (size_t)n))) return r2;
+        if (md->node_gks_scale) {
+            std::vector<double> g(md->node_gks_scale, md->node_gks_scale + n);
+            if ((r2 = upload<R>(h.gks, g))) return r2;
+        }
+        if (md->model == EP_LUORUDYWITHGATE) {
+            std::vector<double> tab;
+            lr_gate_table(tab);
+            if ((r2 = upload<R>(h.lr_table, tab))) return r2;
+        }
+        if ((r2 = h.status.alloc(sizeof(DevStatus))) || (r2 = h.d_step.alloc(sizeof(long long))) ||
+            (r2 = dvd.alloc(sizeof(R) * h.pitch)))
+            return r2;
+        EP_CUDA(cudaMemset(h.status.p, 0, sizeof(DevStatus)));
+        EP_CUDA(cudaMemset(h.d_step.p, 0, sizeof(long long)));
+        IonicArgs<R> a;
+        fill_ionic_args<R>(&h, a);
+        a.track = nullptr;
+        a.dvdt_out = dvd.as<R>();
+        if ((r2 = launch_ionic<R>(h.model, a, h.stream))) return r2;
+        EP_CUDA(cudaStreamSynchronize(h.stream));
+        std::vector<double> o, so;
+        if ((r2 = download<R>(dvd, o, n, h.stream))) return r2;
+        if ((r2 = download<R>(h.S, so, (size_t)h.ns * h.pitch, h.stream))) return r2;
+        for (int i = 0; i < n; i++) {
+            dvdt[i] = o[i];
+            double *s = states + (size_t)i * nst;
+            if (is_lr(md->model)) for (int k = 0; k < 7; k++) s[k] = so[(size_t)k * h.pitch + i];
+            else {
+                s[0] = V[i];
+                for (int k = 0; k < h.ns; k++) s[k + 1] = so[(size_t)k * h.pitch + i];
+            }
+        }
+        return EP_OK;
+    };
+    rc = precision == EP_FP64 ? run(double(0)) : run(float(0));
+    cudaStreamDestroy(h.stream);
+    h.stream = nullptr;
+    return rc;
+}
+
+}  // extern "C"

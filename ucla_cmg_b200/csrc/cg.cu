@@ -1,0 +1,295 @@
+// cg.cu -- one Crank-Nicolson half diffusion step as a single persistent
+// cooperative launch.
+//
+// Reference: EP_CrankNicholson::Solve (Solvers/EP_CrankNicholson.cc:99-104,
+// 146-150): b = B V (B = C_m M - dt/4 K), then AztecOO CG with a Jacobi
+// preconditioner on A = C_m M + dt/4 K from x0 = V, stopped when
+// ||r_k||_2 <= tol ||r_0||_2.
+//
+// Layout: SELL-32 (slices of 32 consecutive rows, column-major inside the
+// slice, one warp per slice, one lane per row) so every value/column load is
+// a coalesced 128-byte transaction.  A and B share the column array.
+//
+// Per iteration two grid barriers:
+//   phase A  p' = z + beta p (recomputed on the fly for each column, z =
+//            dinv r), q = A p', partial p'.q          -> barrier
+//   phase B  x += alpha p', r -= alpha q, partial r.z, r.r -> barrier
+// The same thread owns a row in every phase, so x, r, q need no cross-block
+// visibility; only r and p are read across blocks (through L2, ld.cg).
+// Dot products accumulate in FP64 whatever the vector type.  Reductions
+// sum the per-block partials in block order, so results are deterministic.
+#include "kernels.cuh"
+
+namespace ep {
+
+__device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
+
+// p' = z + beta p with z = dinv r, written as one explicit fma so the owner
+// row and every neighbour that recomputes it round identically
+template <typename R>
+__device__ __forceinline__ R pdir(R dinv, R r, R beta, R p) { return fma(beta, p, dinv * r); }
+
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double *out, int stride) {
+    __shared__ double sh[NV][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[k][warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = lane < nw ? sh[k][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) out[k * stride + blockIdx.x] = t;
+        }
+    }
+    __syncthreads();
+}
+
+// every block sums the grid's partials in the same order
+template <int NV>
+__device__ __forceinline__ void grid_total(const double *partial, int stride, int nblk, double (&tot)[NV]) {
+    __shared__ double sh[NV];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = 0.0;
+            for (int b = lane; b < nblk; b += 32) t += __ldcg(partial + k * stride + b);
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) sh[k] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) tot[k] = sh[k];
+    __syncthreads();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const unsigned int nblk = gridDim.x;
+    const int G = gridDim.x;
+
+    // ---- prologue: r = B x - A x, z = dinv r, p = 0 ----
+    {
+        double v[3] = {0.0, 0.0, 0.0};
+        for (int s = gwarp; s < a.nslices; s += nwarps) {
+            const int row = s * kSlice + lane;
+            const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+            R ax = R(0), bx = R(0);
+            for (int k = 0; k < w; k++) {
+                const int idx = beg + k * kSlice + lane;
+                const int c = __ldg(a.col + idx);
+                const R xv = a.x[c];
+                ax += __ldg(a.Aval + idx) * xv;
+                bx += __ldg(a.Bval + idx) * xv;
+            }
+            if (row < a.n) {
+                const R r = bx - ax;
+                const R z = __ldg(a.dinv + row) * r;
+                a.r[row] = r;
+                a.p0[row] = R(0);
+                v[0] += (double)r * (double)z;
+                v[1] += (double)r * (double)r;
+                v[2] += (double)bx * (double)bx;
+            }
+        }
+        block_reduce_store<3>(v, a.partial, G);
+    }
+    if (!grid_sync(a.bar, nblk)) return;
+    double rz, rr0, bb;
+    {
+        double t[3];
+        grid_total<3>(a.partial, G, G, t);
+        rz = t[0]; rr0 = t[1]; bb = t[2];
+    }
+    // ||r|| <= tol ||r0||, or the residual is at the resolution of b in the
+    // vector type (FP32 cannot resolve a 1e-7 reduction of an r0 that is
+    // itself rounding noise of B x - A x; in FP64 the floor is ~1e-16 ||b||)
+    const double floor2 = a.floor_rel * a.floor_rel * bb;
+    const double stop2 = fmax(a.tol * a.tol * rr0, floor2);
+    double beta = 0.0;
+    int it = 0;
+    bool converged = (rr0 <= stop2);
+    double rr_last = rr0;
+    R *pc = a.p0, *pn = a.p1;
+    while (!converged && it < a.maxit) {
+        // ---- phase A: p' = z + beta p; q = A p' ----
+        {
+            double v[1] = {0.0};
+            const R bR = (R)beta;
+            for (int s = gwarp; s < a.nslices; s += nwarps) {
+                const int row = s * kSlice + lane;
+                const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+                R q = R(0);
+                for (int k = 0; k < w; k++) {
+                    const int idx = beg + k * kSlice + lane;
+                    const int c = __ldg(a.col + idx);
+                    const R pj = pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pc + c));
+                    q += __ldg(a.Aval + idx) * pj;
+                }
+                if (row < a.n) {
+                    const R pi = pdir(__ldg(a.dinv + row), a.r[row], bR, ldcg(pc + row));
+                    pn[row] = pi;
+                    a.q[row] = q;
+                    v[0] += (double)pi * (double)q;
+                }
+            }
+            block_reduce_store<1>(v, a.partial + 3 * G, G);   // disjoint from the neighbours' slots
+        }
+        if (!grid_sync(a.bar, nblk)) return;
+        double pq;
+        {
+            double t[1];
+            grid_total<1>(a.partial + 3 * G, G, G, t);
+            pq = t[0];
+        }
+        const double alpha = rz / pq;
+        // ---- phase B: x += alpha p', r -= alpha q ----
+        {
+            double v[2] = {0.0, 0.0};
+            const R aR = (R)alpha;
+            for (int s = gwarp; s < a.nslices; s += nwarps) {
+                const int row = s * kSlice + lane;
+                if (row < a.n) {
+                    const R pi = pn[row];
+                    a.x[row] += aR * pi;
+                    const R r = a.r[row] - aR * a.q[row];
+                    a.r[row] = r;
+                    const R z = __ldg(a.dinv + row) * r;
+                    v[0] += (double)r * (double)z;
+                    v[1] += (double)r * (double)r;
+                }
+            }
+            block_reduce_store<2>(v, a.partial, G);
+        }
+        if (!grid_sync(a.bar, nblk)) return;
+        double t[2];
+        grid_total<2>(a.partial, G, G, t);
+        it++;
+        rr_last = t[1];
+        converged = (t[1] <= stop2);
+        beta = t[0] / rz;
+        rz = t[0];
+        R *tmp = pc; pc = pn; pn = tmp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(a.iters_total, (unsigned long long)it);
+        atomicMax(a.iters_max, (unsigned int)it);
+        if (!converged) atomicAdd(a.fails, 1u);
+        if (a.last) {
+            a.last[0] = (double)it;
+            a.last[1] = rr0 > 0.0 ? sqrt(rr_last / rr0) : 0.0;
+        }
+    }
+}
+
+template <typename R>
+int cg_grid_size(int block, int *grid) {
+    int dev = 0, nsm = 0, per = 0;
+    EP_CUDA(cudaGetDevice(&dev));
+    EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cn_half<R>, block, 0));
+    if (per < 1) { set_error("CG kernel cannot be resident"); return EP_ERR_CUDA; }
+    *grid = nsm * per;
+    return EP_OK;
+}
+
+template <typename R>
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R>, a));
+    return EP_OK;
+}
+
+template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t);
+template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t);
+template int cg_grid_size<float>(int, int *);
+template int cg_grid_size<double>(int, int *);
+
+// ---------------------------------------------------------------------------
+// pseudo-ECG: out[k] = sum_i W[k * wpitch + i] V[i], FP64 accumulation.
+// Block partials, then the last block to finish sums them in block order.
+template <typename R>
+__global__ void __launch_bounds__(256) k_ecg(int n, int ne, const R *__restrict__ W, int wpitch,
+                                             const R *__restrict__ V, double *partial,
+                                             unsigned int *counter, double *out) {
+    constexpr int MAXE = 16;
+    double acc[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; k++) acc[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = (double)V[i];
+#pragma unroll
+        for (int k = 0; k < MAXE; k++)
+            if (k < ne) acc[k] += (double)__ldg(W + (size_t)k * wpitch + i) * v;
+    }
+    __shared__ double sh[MAXE][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < MAXE; k++) {
+        double t = acc[k];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) sh[k][warp] = t;
+    }
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x < ne) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[threadIdx.x][w];
+        partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        if (threadIdx.x < ne) {
+            double t = 0.0;
+            for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(partial + (size_t)threadIdx.x * gridDim.x + b);
+            out[threadIdx.x] = t;
+        }
+        if (threadIdx.x == 0) *counter = 0;
+    }
+}
+
+template <typename R>
+int launch_ecg(int n, int ne, const R *W, int wpitch, const R *V, double *partial,
+               unsigned int *counter, double *out, int grid, cudaStream_t s) {
+    if (ne <= 0) return EP_OK;
+    if (ne > 16) { set_error("at most 16 electrodes"); return EP_ERR_ARG; }
+    k_ecg<R><<<grid, 256, 0, s>>>(n, ne, W, wpitch, V, partial, counter, out);
+    EP_CUDA(cudaGetLastError());
+    return EP_OK;
+}
+
+template int launch_ecg<float>(int, int, const float *, int, const float *, double *, unsigned int *,
+                               double *, int, cudaStream_t);
+template int launch_ecg<double>(int, int, const double *, int, const double *, double *,
+                                unsigned int *, double *, int, cudaStream_t);
+
+__global__ void k_step_inc(long long *step) { *step += 1; }
+void launch_step_inc(long long *step, cudaStream_t s) { k_step_inc<<<1, 1, 0, s>>>(step); }
+
+}  // namespace ep

@@ -1,0 +1,165 @@
+// ionic.cu -- the ionic phase of one split step, one thread per node.
+//
+// Each thread loads its node's state once (SoA, coalesced), runs all ionic
+// sub-steps of the global step in registers -- Compute_Ion followed by the
+// lumped-capacitance update V <- V + h dV/dt of EP_CrankNicholson.cc:124-133
+// -- applies its stimulus window, tracks activation/repolarisation, and
+// writes the state back once.
+#include "kernels.cuh"
+
+namespace ep {
+
+template <typename R>
+__device__ __forceinline__ R node_istim(const IonicArgs<R> &a, int i, long long step) {
+    if (a.stim_head == nullptr) return R(0);
+    int k = a.stim_head[i];
+    long long best_on = -1;
+    R amp = R(0);
+    while (k >= 0) {
+        const long long on = a.stim_on[k], off = a.stim_off[k];
+        if (step >= on && step < off && on > best_on) { best_on = on; amp = a.stim_amp[k]; }
+        k = a.stim_next[k];
+    }
+    return amp;
+}
+
+template <typename R>
+__device__ __forceinline__ void track_update(Track &tr, bool &dirty, R v0, R v1, double t0, R h, R thr) {
+    if (tr.t_act < 0.f) {
+        if ((float)v0 < tr.v_rest) { tr.v_rest = (float)v0; dirty = true; }
+        if (v0 < thr && v1 >= thr) {
+            const R frac = (thr - v0) / (v1 - v0);
+            tr.t_act = (float)(t0 + (double)(frac * h));
+            tr.v_peak = (float)v1;
+            dirty = true;
+        }
+    } else if (tr.t_rep < 0.f) {
+        if ((float)v1 > tr.v_peak) { tr.v_peak = (float)v1; dirty = true; }
+        const R v90 = R(tr.v_peak) - R(0.9) * (R(tr.v_peak) - R(tr.v_rest));
+        if ((float)t0 > tr.t_act + 5.f && v0 >= v90 && v1 < v90) {
+            const R frac = (v0 - v90) / (v0 - v1);
+            tr.t_rep = (float)(t0 + (double)(frac * h));
+            dirty = true;
+        }
+    }
+}
+
+template <typename R, int MODEL, int NS>
+__global__ void __launch_bounds__(128) k_ionic(const IonicArgs<R> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ unsigned long long s_newton;
+    __shared__ unsigned int s_caps, s_bad;
+    if (threadIdx.x == 0) { s_newton = 0; s_caps = 0; s_bad = 0; }
+    __syncthreads();
+    unsigned int my_newton = 0, my_caps = 0, my_bad = 0;
+    if (i < a.n) {
+        const long long step = *a.step_ptr;
+        const double t_start = (double)step * a.t_per_step;
+        R V = a.V[i];
+        R s[NS + 1];
+#pragma unroll
+        for (int k = 0; k < NS; k++) s[k + 1] = a.S[(size_t)k * a.pitch + i];
+        const int ty = a.type ? a.type[i] : 0;
+        const R istim = node_istim(a, i, step);
+        Track tr = {-1.f, -1.f, -1.f, 1e30f};
+        bool dirty = false;
+        if (a.track) tr = a.track[i];
+        const bool do_track = a.track != nullptr && tr.t_rep < 0.f;
+        double tsub = t_start;
+        R last = R(0);
+        if constexpr (MODEL == EP_TUSSCHER) {
+            const R *__restrict__ c = a.consts + (size_t)ty * a.nconst;
+            const R gks = a.gks ? a.gks[i] : R(1);
+            const R ist = -istim / (a.Cm * a.Xi);
+            for (int k = 0; k < a.nsub; k++) {
+                const R h = a.sub_dt[k];
+                int it = 0;
+                const R dvdt = tt_compute_ion<R>(s + 1, V, ist, h, c, gks, a.tt, it);
+                my_newton += it;
+                if (it >= a.tt.newton_cap) my_caps++;
+                last = dvdt;
+                const R v1 = V + h * dvdt;
+                if (do_track) track_update(tr, dirty, V, v1, tsub, h, a.act_thr);
+                V = v1;
+                tsub += (double)h;
+            }
+        } else if constexpr (MODEL == EP_MAHAJAN || MODEL == EP_MAHAJAN_FAIL) {
+            const R *__restrict__ c = a.consts + (size_t)ty * a.nconst;
+            const R ist = istim / (a.Cm * a.Xi);
+            for (int k = 0; k < a.nsub; k++) {
+                const R h = a.sub_dt[k];
+                int sub = 0;
+                const R dvdt = mh_compute_ion<R>(s, V, ist, h, c, a.mh_abs, sub);
+                my_newton += sub;
+                last = dvdt;
+                const R v1 = V + h * dvdt;
+                if (do_track) track_update(tr, dirty, V, v1, tsub, h, a.act_thr);
+                V = v1;
+                tsub += (double)h;
+            }
+        } else {
+            for (int k = 0; k < a.nsub; k++) {
+                const R h = a.sub_dt[k];
+                const R dvdt = lr_compute_ion<R>(s + 1, V, istim, a.Cm, h, a.lr_table);
+                last = dvdt;
+                const R v1 = V + h * dvdt;
+                if (do_track) track_update(tr, dirty, V, v1, tsub, h, a.act_thr);
+                V = v1;
+                tsub += (double)h;
+            }
+        }
+        if (!isfinite((double)V)) my_bad = 1;
+        if (a.dvdt_out) a.dvdt_out[i] = last;
+        else a.V[i] = V;
+#pragma unroll
+        for (int k = 0; k < NS; k++) a.S[(size_t)k * a.pitch + i] = s[k + 1];
+        if (dirty) a.track[i] = tr;
+    }
+    // block-level status reduction, one atomic per block
+    for (int o = 16; o > 0; o >>= 1) {
+        my_newton += __shfl_xor_sync(0xffffffffu, my_newton, o);
+        my_caps += __shfl_xor_sync(0xffffffffu, my_caps, o);
+        my_bad += __shfl_xor_sync(0xffffffffu, my_bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (my_newton) atomicAdd(&s_newton, (unsigned long long)my_newton);
+        if (my_caps) atomicAdd(&s_caps, my_caps);
+        if (my_bad) atomicAdd(&s_bad, my_bad);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_newton) atomicAdd(&a.status->newton_iters, s_newton);
+        if (s_caps) atomicAdd(&a.status->newton_cap_hits, s_caps);
+        if (s_bad) atomicAdd(&a.status->nonfinite, s_bad);
+    }
+}
+
+template <typename R>
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st) {
+    const int block = 128;
+    const int grid = div_up(a.n, block);
+    if (a.n == 0) return EP_OK;
+    switch (model) {
+    case EP_TUSSCHER:
+        k_ionic<R, EP_TUSSCHER, TT_NS><<<grid, block, 0, st>>>(a);
+        break;
+    case EP_MAHAJAN:
+    case EP_MAHAJAN_FAIL:
+        k_ionic<R, EP_MAHAJAN, MH_NS><<<grid, block, 0, st>>>(a);
+        break;
+    case EP_LUORUDY:
+    case EP_LUORUDYWITHGATE:
+        k_ionic<R, EP_LUORUDY, LR_NS><<<grid, block, 0, st>>>(a);
+        break;
+    default:
+        set_error("unknown model %d", model);
+        return EP_ERR_ARG;
+    }
+    EP_CUDA(cudaGetLastError());
+    return EP_OK;
+}
+
+template int launch_ionic<float>(int, const IonicArgs<float> &, cudaStream_t);
+template int launch_ionic<double>(int, const IonicArgs<double> &, cudaStream_t);
+
+}  // namespace ep

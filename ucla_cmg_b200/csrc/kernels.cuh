@@ -1,0 +1,78 @@
+// kernels.cuh -- launch interfaces of the device kernels (host side).
+#pragma once
+#include "common.cuh"
+#include "tt.cuh"
+#include "mahajan.cuh"
+#include "lr.cuh"
+
+namespace ep {
+
+// Per-node activation record {t_act, t_rep, v_peak, v_rest}; -1 = not yet.
+struct Track { float t_act, t_rep, v_peak, v_rest; };
+
+// Ionic phase of one global step for all nodes: the reference loop of
+// EP_CrankNicholson::Solve (Solvers/EP_CrankNicholson.cc:114-143) with
+// CardiacBody::getIonicCurrent (Body/CardiacBody.cc:405-435) inside.
+template <typename R> struct IonicArgs {
+    int n, pitch;
+    R *V;                        // in/out
+    R *S;                        // SoA states: S[k * pitch + i]
+    const uint8_t *type;         // nullable
+    const R *gks;                // nullable (TT)
+    // stimulus windows, chained per node (head[i] = -1: none)
+    const int *stim_head, *stim_next;
+    const long long *stim_on, *stim_off;
+    const R *stim_amp;
+    const long long *step_ptr;   // device step counter (read)
+    double t_per_step;           // dt
+    R Cm, Xi;                    // Xi: the model's or the user's
+    int nsub;
+    R sub_dt[kMaxSub];
+    R act_thr;
+    Track *track;                // nullable
+    DevStatus *status;
+    const R *consts;             // ntypes * nconst, device memory
+    int nconst;
+    R *dvdt_out;                 // non-null: plugin mode -- write the returned
+                                 // dV/dt, leave V unchanged (one sub-step)
+    // model options
+    TTOpts tt;
+    int mh_abs;
+    const R *lr_table;           // nullable
+};
+
+template <typename R>
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t s);
+
+// Crank-Nicolson half diffusion step: x <- A^-1 (B x) by Jacobi-PCG in one
+// persistent cooperative launch (Solvers/EP_CrankNicholson.cc:99-104).
+template <typename R> struct CGArgs {
+    int n, nslices;
+    const int *slice_ptr;        // nslices + 1
+    const int *col;
+    const R *Aval, *Bval, *dinv;
+    R *x, *r, *q, *p0, *p1;
+    double *partial;             // 4 * grid: consecutive phases use disjoint slots
+    GridBarrier *bar;
+    double tol;
+    double floor_rel;            // stop also when ||r|| <= floor_rel ||B x||
+    int maxit;
+    unsigned long long *iters_total;
+    unsigned int *iters_max, *fails;
+    double *last;                // [0] iterations, [1] ||r||/||r0|| of this solve
+};
+
+template <typename R>
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s);
+template <typename R>
+int cg_grid_size(int block, int *grid);
+
+// ECG_k = sum_i W[k n + i] V[i] (ComputeECG.h:172-189 in per-node form),
+// deterministic two-level reduction, written to out[k].
+template <typename R>
+int launch_ecg(int n, int ne, const R *W, int wpitch, const R *V, double *partial,
+               unsigned int *counter, double *out, int grid, cudaStream_t s);
+
+void launch_step_inc(long long *step, cudaStream_t s);
+
+}  // namespace ep

@@ -7,8 +7,8 @@ The reference reads its geometry from ``.node/.ele/.fibers/.cell`` files
   tetrahedra along its main diagonal (Kuhn split, conforming), with the fibre
   angle rotating linearly through the thickness;
 * :func:`shell` -- a truncated prolate-ellipsoid shell (a ventricle-like
-  wall) built from a structured (phi, theta, rho) grid whose apex column is
-  collapsed onto one node per transmural layer.
+  wall): a ring-by-ring surface triangulation of near-uniform spacing,
+  extruded through the wall into prisms of 3 tets each.
 
 Element fibres use the reference's 9-number layout per element (f, s, n;
 voomEP/src/Body/CardiacBody.cc:158-167).  Node ids are zero-based here; the
@@ -105,83 +105,127 @@ def slab(nx, ny, nz, Lx, Ly, Lz, fiber_deg=(-60.0, 60.0), origin=(0.0, 0.0, 0.0)
     return TetMesh(xyz, tets, fib, meta)
 
 
-def shell(n_phi=480, n_theta=200, n_rho=20, a_in=2.5, c_in=5.0, wall=1.0, z_base=2.0,
+def _zip_rings(ring_a, ang_a, ring_b, ang_b):
+    """Triangulate the band between two closed rings of nodes (angles
+    increasing in [0, 2pi)), advancing along whichever ring is behind."""
+    na, nb = len(ring_a), len(ring_b)
+    tris = []
+    i = j = 0
+    while i < na or j < nb:
+        a0, b0 = ring_a[i % na], ring_b[j % nb]
+        ta = ang_a[i + 1] if i + 1 <= na else np.inf
+        tb = ang_b[j + 1] if j + 1 <= nb else np.inf
+        if j >= nb or (i < na and ta <= tb):
+            tris.append((a0, ring_a[(i + 1) % na], b0))
+            i += 1
+        else:
+            tris.append((a0, ring_b[(j + 1) % nb], b0))
+            j += 1
+    return tris
+
+
+def shell(h=0.0365, n_rho=20, a_in=2.5, c_in=5.0, wall=1.0, z_base=2.0,
           helix_deg=(60.0, -60.0)):
-    """Truncated prolate-ellipsoid shell.
+    """Truncated prolate-ellipsoid shell with near-uniform element size.
 
     Inner surface x^2/a^2 + y^2/a^2 + z^2/c^2 = 1 with (a, c) = (a_in, c_in),
-    outer surface with (a_in + wall, c_in + wall); apex at z = -c, cut by the
-    base plane z = ``z_base``.  Grid: ``n_phi`` nodes around, ``n_theta``
-    intervals apex->base, ``n_rho`` intervals endo->epi; the apex column
-    (theta = 0) is one node per layer and the degenerate tets there are
-    dropped.  Fibres: helix angle rotating linearly endo->epi in the plane of
-    the circumferential and longitudinal directions.
+    outer surface (a_in + wall, c_in + wall); apex at z = -c, cut by the base
+    plane z = ``z_base``.  A surface mesh of rings (ring j has as many nodes
+    as its mid-wall circumference holds at spacing ``h``; one apex node) is
+    zipped into triangles and extruded through ``n_rho`` transmural layers;
+    each prism is split into 3 tets.  Defaults give ~2.0M nodes / ~11.5M
+    tets.  Fibres: helix angle rotating linearly endo->epi.
     meta["rho"] (per node, 0 endo .. 1 epi) and meta["height"] (0 apex .. 1
     base) feed the transmural and apicobasal parameter maps.
     """
     rho = np.linspace(0.0, 1.0, n_rho + 1)
     a = a_in + wall * rho
     c = c_in + wall * rho
-    tmax = np.arccos(-z_base / c)                     # per layer
-    u = np.linspace(0.0, 1.0, n_theta + 1)            # fraction apex->base
-    phi = np.linspace(0.0, 2.0 * np.pi, n_phi, endpoint=False)
-    # node numbering: apex node of layer k = k; ring nodes afterwards
-    n_apex = n_rho + 1
-    def nid(ip, jt, kr):
-        ip = np.asarray(ip) % n_phi
-        return np.where(jt == 0, kr, n_apex + ((kr * n_theta + (jt - 1)) * n_phi + ip))
-    # coordinates
-    xyz = np.zeros((n_apex + (n_rho + 1) * n_theta * n_phi, 3))
-    xyz[:n_apex, 2] = -c
-    K, J, I = np.meshgrid(np.arange(n_rho + 1), np.arange(1, n_theta + 1), np.arange(n_phi), indexing="ij")
-    th = u[J] * tmax[K]
-    ids = n_apex + (K * n_theta + (J - 1)) * n_phi + I
-    xyz[ids.ravel(), 0] = (a[K] * np.sin(th) * np.cos(phi[I])).ravel()
-    xyz[ids.ravel(), 1] = (a[K] * np.sin(th) * np.sin(phi[I])).ravel()
-    xyz[ids.ravel(), 2] = (-c[K] * np.cos(th)).ravel()
-    # hex cells (phi, theta, rho) -> Kuhn tets, collapsing theta=0
-    ip, jt, kr = np.meshgrid(np.arange(n_phi), np.arange(n_theta), np.arange(n_rho), indexing="ij")
-    ip, jt, kr = ip.ravel(), jt.ravel(), kr.ravel()
-    tets = []
-    for path in _kuhn_local():
-        tets.append(np.stack([nid(ip + cc[0], jt + cc[1], kr + cc[2]) for cc in path], axis=1))
-    tets = np.concatenate(tets, axis=0).astype(np.int64)
-    # drop tets with repeated vertices (apex collapse)
-    srt = np.sort(tets, axis=1)
-    keep = np.all(srt[:, 1:] != srt[:, :-1], axis=1)
-    tets = tets[keep].astype(np.int32)
-    tets, vol = _orient(xyz, tets)
-    good = vol > 1e-14
-    tets = tets[good]
-    # per-node transmural depth and height
-    rho_n = np.zeros(len(xyz)); rho_n[:n_apex] = rho
-    rho_n[ids.ravel()] = rho[K].ravel()
+    tmax = np.arccos(-z_base / c)
+    # mid-wall meridian arc length -> number of rings
+    am, cm = a_in + 0.5 * wall, c_in + 0.5 * wall
+    tm = np.arccos(-z_base / cm)
+    tt = np.linspace(0.0, tm, 4001)
+    seg = np.hypot(np.diff(am * np.sin(tt)), np.diff(cm * np.cos(tt)))
+    arc = np.concatenate([[0.0], np.cumsum(seg)])
+    n_theta = max(2, int(round(arc[-1] / h)))
+    u = np.interp(np.linspace(0.0, arc[-1], n_theta + 1), arc, tt) / tm   # fraction of tmax
+    ring_n = [1] + [max(6, int(round(2 * np.pi * am * np.sin(u[j] * tm) / h))) for j in range(1, n_theta + 1)]
+    offs = np.concatenate([[0], np.cumsum(ring_n)])
+    n_surf = int(offs[-1])
+    # surface triangulation (same for every layer)
+    tris = [(0, offs[1] + k, offs[1] + (k + 1) % ring_n[1]) for k in range(ring_n[1])]
+    for j in range(1, n_theta):
+        na, nb = ring_n[j], ring_n[j + 1]
+        ang_a = np.concatenate([2 * np.pi * np.arange(na) / na, [2 * np.pi]])
+        ang_b = np.concatenate([2 * np.pi * np.arange(nb) / nb, [2 * np.pi]])
+        tris += _zip_rings(offs[j] + np.arange(na), ang_a, offs[j + 1] + np.arange(nb), ang_b)
+    tris = np.array(tris, dtype=np.int64)
+    # node coordinates, node id = layer * n_surf + surface id
+    jj = np.zeros(n_surf, dtype=np.int64)
+    phi = np.zeros(n_surf)
+    for j in range(1, n_theta + 1):
+        jj[offs[j]:offs[j + 1]] = j
+        phi[offs[j]:offs[j + 1]] = 2 * np.pi * np.arange(ring_n[j]) / ring_n[j]
+    xyz = np.zeros(((n_rho + 1) * n_surf, 3))
+    for k in range(n_rho + 1):
+        th = u[jj] * tmax[k]
+        sl = slice(k * n_surf, (k + 1) * n_surf)
+        xyz[sl, 0] = a[k] * np.sin(th) * np.cos(phi)
+        xyz[sl, 1] = a[k] * np.sin(th) * np.sin(phi)
+        xyz[sl, 2] = -c[k] * np.cos(th)
+    # prisms -> tets
+    bot = np.concatenate([tris + k * n_surf for k in range(n_rho)])
+    tets = _split_prisms(bot, bot + n_surf)
+    tets, vol = _orient(xyz, tets.astype(np.int32))
+    rho_n = np.repeat(rho, n_surf)
     zmin = -c[0]
     height = np.clip((xyz[:, 2] - zmin) / (z_base - zmin), 0.0, 1.0)
-    fib = None
-    if helix_deg is not None:
-        cen = xyz[tets].mean(axis=1)
-        rc = rho_n[tets].mean(axis=1)
-        # circumferential direction (about z) and the local outward normal of
-        # the ellipsoid family through the centroid
-        r_xy = np.hypot(cen[:, 0], cen[:, 1])
-        ec = np.stack([-cen[:, 1], cen[:, 0], np.zeros(len(cen))], axis=1)
-        near_axis = r_xy < 1e-9
-        ec[near_axis] = np.array([1.0, 0.0, 0.0])
-        ec /= np.linalg.norm(ec, axis=1, keepdims=True)
-        ae = a_in + wall * rc
-        ce = c_in + wall * rc
-        nrm = np.stack([cen[:, 0] / ae ** 2, cen[:, 1] / ae ** 2, cen[:, 2] / ce ** 2], axis=1)
-        nrm -= np.einsum("ij,ij->i", nrm, ec)[:, None] * ec
-        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
-        el = np.cross(nrm, ec)                          # longitudinal (tangent)
-        al = np.deg2rad(helix_deg[0] + (helix_deg[1] - helix_deg[0]) * rc)
-        f = np.cos(al)[:, None] * ec + np.sin(al)[:, None] * el
-        s = -np.sin(al)[:, None] * ec + np.cos(al)[:, None] * el
-        fib = np.concatenate([f, s, nrm], axis=1)
-    meta = dict(kind="shell", rho=rho_n, height=height, n_phi=n_phi, n_theta=n_theta,
-                n_rho=n_rho, endo_nodes=np.where(rho_n == 0.0)[0], z_base=z_base)
+    fib = _helix_fibers(xyz, tets, rho_n, a_in, c_in, wall, helix_deg)
+    meta = dict(kind="shell", rho=rho_n, height=height, n_theta=n_theta, n_rho=n_rho,
+                endo_nodes=np.arange(n_surf), z_base=z_base, h=h, ring_n=np.array(ring_n))
     return TetMesh(xyz, tets, fib, meta)
+
+
+def _split_prisms(bot, top):
+    """Conforming 3-tet split of prisms (bottom tri, top tri): every quad
+    face is cut along the diagonal through its smallest global node id
+    (the face diagonals then never form a cycle, so 3 tets always fit)."""
+    P = np.concatenate([bot, top], axis=1)
+    m = np.argmin(P, axis=1)
+    flip = m >= 3
+    P[flip] = np.concatenate([P[flip, 3:], P[flip, :3]], axis=1)
+    m = np.where(flip, m - 3, m)
+    r = np.arange(len(P))
+    i0, i1, i2 = m, (m + 1) % 3, (m + 2) % 3
+    v0, v1, v2 = P[r, i0], P[r, i1], P[r, i2]
+    v3, v4, v5 = P[r, 3 + i0], P[r, 3 + i1], P[r, 3 + i2]
+    d15 = np.minimum(v1, v5) < np.minimum(v2, v4)
+    t1 = np.where(d15[:, None], np.stack([v0, v1, v2, v5], 1), np.stack([v0, v1, v2, v4], 1))
+    t2 = np.where(d15[:, None], np.stack([v0, v1, v5, v4], 1), np.stack([v0, v4, v2, v5], 1))
+    t3 = np.stack([v0, v4, v5, v3], 1)
+    return np.concatenate([t1, t2, t3], axis=0)
+
+
+def _helix_fibers(xyz, tets, rho_n, a_in, c_in, wall, helix_deg):
+    if helix_deg is None:
+        return None
+    cen = xyz[tets].mean(axis=1)
+    rc = rho_n[tets].mean(axis=1)
+    r_xy = np.hypot(cen[:, 0], cen[:, 1])
+    ec = np.stack([-cen[:, 1], cen[:, 0], np.zeros(len(cen))], axis=1)
+    ec[r_xy < 1e-9] = np.array([1.0, 0.0, 0.0])
+    ec /= np.linalg.norm(ec, axis=1, keepdims=True)
+    ae = a_in + wall * rc
+    ce = c_in + wall * rc
+    nrm = np.stack([cen[:, 0] / ae ** 2, cen[:, 1] / ae ** 2, cen[:, 2] / ce ** 2], axis=1)
+    nrm -= np.einsum("ij,ij->i", nrm, ec)[:, None] * ec
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    el = np.cross(nrm, ec)
+    al = np.deg2rad(helix_deg[0] + (helix_deg[1] - helix_deg[0]) * rc)
+    f = np.cos(al)[:, None] * ec + np.sin(al)[:, None] * el
+    s = -np.sin(al)[:, None] * ec + np.cos(al)[:, None] * el
+    return np.concatenate([f, s, nrm], axis=1)
 
 
 def lumped_volume(mesh):
@@ -210,10 +254,10 @@ def pmj_sites(mesh, count=200, seed=0, radius=0.1):
     w = lumped_volume(mesh)[endo]
     w = w / w.sum()
     sites = rng.choice(endo, size=count, replace=False, p=w)
-    balls = []
-    for s in sites:
-        d = np.linalg.norm(mesh.xyz - mesh.xyz[s], axis=1)
-        balls.append(np.where(d <= radius)[0].astype(np.int32))
+    from scipy.spatial import cKDTree
+    tree = cKDTree(mesh.xyz)
+    balls = [np.sort(np.asarray(b, dtype=np.int32))
+             for b in tree.query_ball_point(mesh.xyz[sites], r=radius)]
     return sites.astype(np.int32), balls
 
 

@@ -1,0 +1,243 @@
+"""Host-side mirror of the reference's EP solver interface over the C ABI.
+
+Reference interface (paths inside wsklug/UCLA_CMG, voomEP/src/...):
+
+* ``CardiacBody`` (Body/CardiacBody.h) -- cell model per node, diffusion
+  tensor, stimulus currents;
+* ``EPSolver`` / ``EP_CrankNicholson`` (Solvers/EPSolver.h,
+  EP_CrankNicholson.cc) -- ``InitializeVoltage``, ``setIonicTimeStep``,
+  ``setSolveTime``, ``Solve``, ``WriteOutput``, ``writeRestart``,
+  ``readRestart``;
+* ``EPSimulator`` main loop (Applications/CardiacEP/EPSimulator.cc:483-596).
+
+:class:`Monodomain` owns one device-resident tissue instance
+(``ep_create``); the method names of the reference are kept as aliases.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import check, ptr
+
+
+class Monodomain:
+    """One tissue instance on one GPU (FP64 or FP32 arithmetic).
+
+    mesh: :class:`ucla_cmg_b200.mesh.TetMesh` (zero-based tets)
+    model: capi.TUSSCHER / MAHAJAN / MAHAJAN_FAIL / LUORUDY / LUORUDYWITHGATE
+    D: (D_f, D_s, D_n) in cm^2/ms; Cm in uF/cm^2
+    """
+
+    def __init__(self, mesh, model=capi.TUSSCHER, precision=capi.FP64, dt=0.02, ionic_dt=0.02,
+                 D=(1e-3, 5e-4, 2.5e-4), Cm=1.0, cg_tol=1e-7, cg_maxit=1000, node_type=None,
+                 type_consts=None, n_types=None, gks_scale=None, user_xi=0.0, newton_cap=0,
+                 tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0, initial_states=None,
+                 smoothing_alpha=0.0, newton_tol=0.0, ecg_every=0, act_threshold=-40.0, device=0):
+        L = capi.lib()
+        self.mesh = mesh
+        self.model = model
+        self.precision = precision
+        self.dt = float(dt)
+        self.n = mesh.n
+        self._xyz = np.ascontiguousarray(mesh.xyz, dtype=np.float64)
+        self._tets = np.ascontiguousarray(mesh.tets, dtype=np.int32)
+        self._fib = None if mesh.fibers is None else np.ascontiguousarray(mesh.fibers, dtype=np.float64)
+        md = capi.MeshDesc()
+        md.n_nodes = mesh.n
+        md.xyz = ptr(self._xyz)
+        md.n_tets = mesh.m
+        md.tets = ptr(self._tets, C.POINTER(C.c_int32))
+        md.one_based = 0
+        md.fibers = ptr(self._fib)
+        for k in range(3):
+            md.D[k] = float(D[k])
+        md.Cm = float(Cm)
+        mo = capi.ModelDesc()
+        mo.model = model
+        self._types = None if node_type is None else np.ascontiguousarray(node_type, dtype=np.uint8)
+        self._tc = None if type_consts is None else np.ascontiguousarray(type_consts, dtype=np.float64)
+        if n_types is None:
+            if self._tc is not None:
+                n_types = self._tc.shape[0]
+            elif self._types is not None and len(self._types):
+                n_types = int(self._types.max()) + 1
+            else:
+                n_types = 1
+        mo.n_types = int(n_types)
+        mo.type_consts = ptr(self._tc)
+        mo.node_type = ptr(self._types, C.POINTER(C.c_uint8))
+        self._gks = None if gks_scale is None else np.ascontiguousarray(gks_scale, dtype=np.float64)
+        mo.node_gks_scale = ptr(self._gks)
+        mo.user_xi = float(user_xi)
+        mo.newton_cap = int(newton_cap)
+        mo.tt_jacobian = int(tt_jacobian)
+        mo.mh_abs_mode = int(mh_abs_mode)
+        self._init = None if initial_states is None else np.ascontiguousarray(initial_states, dtype=np.float64)
+        mo.initial_states = ptr(self._init)
+        sd = capi.SolverDesc()
+        sd.dt, sd.ionic_dt = float(dt), float(ionic_dt)
+        sd.cg_tol, sd.cg_maxit = float(cg_tol), int(cg_maxit)
+        sd.smoothing_alpha = float(smoothing_alpha)
+        sd.precision = int(precision)
+        sd.newton_tol = float(newton_tol)
+        sd.ecg_every = int(ecg_every)
+        sd.act_threshold = float(act_threshold)
+        h = C.c_void_p()
+        check(L.ep_create(C.byref(md), C.byref(mo), C.byref(sd), int(device), C.byref(h)))
+        self._h = h
+        self.nstate = L.ep_num_states(h)
+        self.last_stats = None
+
+    # ---- life cycle ----
+    def close(self):
+        if getattr(self, "_h", None):
+            capi.lib().ep_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state ----
+    def set_voltage(self, V):
+        V = np.ascontiguousarray(np.broadcast_to(np.asarray(V, dtype=np.float64), (self.n,)))
+        check(capi.lib().ep_set_voltage(self._h, ptr(V)))
+
+    InitializeVoltage = set_voltage
+
+    def voltage(self):
+        out = np.empty(self.n)
+        check(capi.lib().ep_get_voltage(self._h, ptr(out)))
+        return out
+
+    def model_voltage(self):
+        out = np.empty(self.n)
+        check(capi.lib().ep_get_model_voltage(self._h, ptr(out)))
+        return out
+
+    def states(self):
+        out = np.empty((self.n, self.nstate))
+        check(capi.lib().ep_get_states(self._h, ptr(out)))
+        return out
+
+    def set_states(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(self.n, self.nstate)
+        check(capi.lib().ep_set_states(self._h, ptr(s)))
+
+    # ---- stimulus, electrodes ----
+    def set_stimulus(self, node_ids, t_on, t_off, amp):
+        """Per-entry nodal windows [t_on, t_off) in ms, amplitude uA/cm^3."""
+        ids = np.ascontiguousarray(node_ids, dtype=np.int32)
+        k = len(ids)
+        t0 = np.ascontiguousarray(np.broadcast_to(np.asarray(t_on, dtype=np.float64), (k,)))
+        t1 = np.ascontiguousarray(np.broadcast_to(np.asarray(t_off, dtype=np.float64), (k,)))
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(amp, dtype=np.float64), (k,)))
+        check(capi.lib().ep_set_stimulus(self._h, k, ptr(ids, C.POINTER(C.c_int32)), ptr(t0),
+                                         ptr(t1), ptr(a)))
+
+    def set_electrodes(self, xyz, D_ecg=None):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self._ne = len(xyz)
+        D = None if D_ecg is None else np.ascontiguousarray(D_ecg, dtype=np.float64)
+        check(capi.lib().ep_set_electrodes(self._h, len(xyz), ptr(xyz), ptr(D)))
+
+    def compute_ecg(self):
+        out = np.empty(self._ne)
+        check(capi.lib().ep_compute_ecg(self._h, ptr(out)))
+        return out
+
+    def ecg(self):
+        n = C.c_int32(0)
+        check(capi.lib().ep_get_ecg(self._h, None, 0, C.byref(n), None))
+        out = np.empty((n.value, self._ne))
+        t = np.empty(n.value)
+        if n.value:
+            check(capi.lib().ep_get_ecg(self._h, ptr(out), n.value, C.byref(n), ptr(t)))
+        return t, out
+
+    # ---- time stepping ----
+    def step(self, n_steps=1):
+        st = capi.StepStats()
+        check(capi.lib().ep_step(self._h, int(n_steps), C.byref(st)))
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def diffusion_half_step(self):
+        """One CN half diffusion step on the current V; returns (CG
+        iterations, final ||r||/||r0||)."""
+        it = C.c_int32(0)
+        rr = C.c_double(0)
+        check(capi.lib().ep_diffusion_half_step(self._h, C.byref(it), C.byref(rr)))
+        return it.value, rr.value
+
+    def set_profiling(self, on=True):
+        check(capi.lib().ep_set_profiling(self._h, int(bool(on))))
+
+    def Solve(self):
+        """EP_CrankNicholson::Solve: one global step."""
+        return self.step(1)
+
+    def time(self):
+        t = C.c_double(0)
+        s = C.c_int64(0)
+        check(capi.lib().ep_get_time(self._h, C.byref(t), C.byref(s)))
+        return t.value, s.value
+
+    def activation(self):
+        ta = np.empty(self.n)
+        apd = np.empty(self.n)
+        check(capi.lib().ep_get_activation(self._h, ptr(ta), ptr(apd)))
+        return ta, apd
+
+    # ---- reference file formats ----
+    def write_output(self, t, directory):
+        check(capi.lib().ep_write_output(self._h, float(t), str(directory).encode()))
+
+    WriteOutput = write_output
+
+    def write_restart(self, t, directory):
+        check(capi.lib().ep_write_restart(self._h, float(t), str(directory).encode()))
+
+    writeRestart = write_restart
+
+    def read_restart(self, t, directory):
+        check(capi.lib().ep_read_restart(self._h, float(t), str(directory).encode()))
+
+    readRestart = read_restart
+
+
+def ionic_step(model, V, istim, states, dt, Cm=1.0, precision=capi.FP64, node_type=None,
+               type_consts=None, gks_scale=None, user_xi=0.0, newton_cap=0,
+               tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0):
+    """Batched IonicModel::Compute_Ion: returns dV/dt, updates ``states``
+    (n x nstate, node-major, FP64) in place."""
+    n = len(V)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    istim = np.ascontiguousarray(np.broadcast_to(np.asarray(istim, dtype=np.float64), (n,)))
+    assert states.dtype == np.float64 and states.flags.c_contiguous
+    mo = capi.ModelDesc()
+    mo.model = model
+    types = None if node_type is None else np.ascontiguousarray(node_type, dtype=np.uint8)
+    tc = None if type_consts is None else np.ascontiguousarray(type_consts, dtype=np.float64)
+    mo.n_types = tc.shape[0] if tc is not None else (int(types.max()) + 1 if types is not None else 1)
+    mo.type_consts = ptr(tc)
+    mo.node_type = ptr(types, C.POINTER(C.c_uint8))
+    g = None if gks_scale is None else np.ascontiguousarray(gks_scale, dtype=np.float64)
+    mo.node_gks_scale = ptr(g)
+    mo.user_xi = float(user_xi)
+    mo.newton_cap = int(newton_cap)
+    mo.tt_jacobian = int(tt_jacobian)
+    mo.mh_abs_mode = int(mh_abs_mode)
+    out = np.empty(n)
+    check(capi.lib().ep_ionic_step(C.byref(mo), int(precision), n, float(dt), float(Cm), ptr(V),
+                                   ptr(istim), ptr(states), ptr(out)))
+    return out
