@@ -182,6 +182,25 @@ int  ep_set_profiling(ep_handle *h, int on);
  * else: V <- A^-1 (B V) (EP_CrankNicholson.cc:99-104).  *iters receives the
  * CG iteration count, *relres the final ||r||/||r0||. */
 int  ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres);
+/* Allocation-free Crank-Nicolson half diffusion step.  No counterpart in
+ * the reference: it exists for callers that own all device memory and may
+ * not allocate any (solvers embedded in another code's memory pool, time
+ * loops that must not call cudaMalloc after start-up, C/Fortran hosts that
+ * pass only their own buffers).  The caller passes, in device memory, the
+ * SELL-32 operators (slice_ptr: nslices+1 element offsets, col, Aval = A,
+ * Bval = B, dinv = 1/diag(A); values FP64 or FP32 per `precision`) and x,
+ * which holds V on entry and A^-1 B V on return; stream may be NULL.  The
+ * working vectors live in one static device array of this library sized for
+ * at most 262144 rows (about 8.2 MB, held by every GPU that loads the
+ * library until exit); larger n returns EP_ERR_ARG.  Every call shares that
+ * array, so calls that overlap on the GPU race: serialise them.  The first
+ * call on a device looks up the array's address on that device; make it
+ * before any stream capture. */
+int  ep_cn_half_step_noalloc(int32_t precision, int32_t n, int32_t nslices,
+                             const int32_t *slice_ptr, const int32_t *col,
+                             const void *Aval, const void *Bval, const void *dinv,
+                             void *x, double cg_tol, int32_t cg_maxit, void *stream,
+                             int32_t *iters, double *relres);
 /* simulated time (ms) and step count */
 int  ep_get_time(ep_handle *h, double *t, int64_t *step);
 

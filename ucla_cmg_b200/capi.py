@@ -98,6 +98,9 @@ def lib():
         "ep_get_time": ([H, dp, C.POINTER(C.c_int64)], C.c_int),
         "ep_set_profiling": ([H, C.c_int], C.c_int),
         "ep_diffusion_half_step": ([H, C.POINTER(C.c_int32), dp], C.c_int),
+        "ep_cn_half_step_noalloc": ([C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                     C.c_int32, C.c_void_p, C.POINTER(C.c_int32), dp], C.c_int),
         "ep_get_activation": ([H, dp, dp], C.c_int),
         "ep_write_output": ([H, C.c_double, C.c_char_p], C.c_int),
         "ep_write_restart": ([H, C.c_double, C.c_char_p], C.c_int),
