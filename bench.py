@@ -196,9 +196,12 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    prec = capi.FP64 if args.form == "fp64" else capi.FP32
+    prec = {"fp64": capi.FP64, "plain_fp32": capi.FP32, "surrogate": capi.SURROGATE}[args.form]
     wl = W.shell_c2()
     g = wl.create(prec, device=local)
+    if prec == capi.SURROGATE:
+        from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
+        Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(g)
     g.set_profiling(True)
     n = wl.mesh.n
     g.step(args.warmup)
@@ -249,7 +252,7 @@ def run_ours(args, rank, world, local):
             "kernel_ms": kms}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else ("bf16+f32" if prec == capi.SURROGATE else "f32"),
             "data": "synthetic",
             "config": {"workload": f"shell_c2: truncated prolate-ellipsoid shell, {n} nodes, "
                                    f"{wl.mesh.m} tets, ten Tusscher endo/M/epi 40/30/30, G_Ks 0.8->1.2 "
@@ -258,6 +261,7 @@ def run_ours(args, rank, world, local):
                        "t_window_ms": [0.0, round((args.warmup + args.steps) * wl.dt, 3)],
                        "l2": "inputs > L2 (operators + states ~ 0.5 GB), no flush",
                        "cg_iters_per_solve": cg_per_solve, "newton_iters": st["newton_iters"],
+                       "fallback_fraction": st["fallback_nodes"] / float(n * args.steps),
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": int(st["launches"]),
             "clocks": clocks, "roofline": roof, "e2e": e2e}
@@ -290,7 +294,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain_fp32", choices=["plain_fp32", "fp64"])
+    ap.add_argument("--form", default="plain_fp32", choices=["plain_fp32", "fp64", "surrogate"])
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     rank, world, local = _env()

@@ -83,6 +83,8 @@ typedef struct ep_model_desc {
     int32_t mh_abs_mode;        /* Mahajan sub-step trigger: 0 int |dV/dt| (as
                                    compiled), 1 double fabs (Mahajan.cc:611) */
     const double *initial_states; /* n_nodes * nstate node-major, or NULL */
+    double newton_tol;          /* TT, batch entry points only (0: 1e-6, the
+                                   reference's); handles take it from the solver */
 } ep_model_desc;
 
 /* Time stepping: EPSolver::New/setSolveTime/setIonicTimeStep
@@ -222,6 +224,62 @@ int  ep_read_restart(ep_handle *h, double t, const char *dir);
 int  ep_ionic_step(const ep_model_desc *model, int32_t precision, int32_t n,
                    double dt, double Cm, const double *V, const double *istim,
                    double *states, double *dvdt);
+
+/* The ionic phase of one global step for independent cells: the sub-step
+ * loop of EP_CrankNicholson::Solve (Solvers/EP_CrankNicholson.cc:114-143)
+ * with Compute_Ion and V += h dV/dt per sub-step, no diffusion.  V and
+ * states (node-major) are advanced in place.  This is the map the learned
+ * ionic step replaces; it also produces its training targets. */
+int  ep_ionic_phase(const ep_model_desc *model, int32_t precision, int32_t n, double dt,
+                    double ionic_dt, double Cm, double *V, const double *istim, double *states);
+
+/* ---------------- learned ionic step (no reference counterpart) ----------
+ * A tanh MLP trained on the plain model's ionic phase.  Training runs on
+ * the GPU through ep_mlp_* (FP32 master weights, the project's own forward,
+ * backward and Adam kernels); deployment (ep_set_surrogate) converts the
+ * weights to BF16 for the tcgen05 tensor-core inference kernel. */
+typedef struct ep_mlp ep_mlp;
+/* dims[0..n_layers]: input, hidden..., output widths; hidden layers use tanh */
+int  ep_mlp_create(int32_t n_layers, const int32_t *dims, uint64_t seed, int device, ep_mlp **out);
+void ep_mlp_destroy(ep_mlp *m);
+int  ep_mlp_num_params(const ep_mlp *m);
+/* parameters flattened as W1 (dims[1] x dims[0], row-major), b1, W2, b2, ... */
+int  ep_mlp_get_params(ep_mlp *m, float *out);
+int  ep_mlp_set_params(ep_mlp *m, const float *in);
+/* device pointers, row-major FP32: X [batch x dims[0]], Y [batch x dims[L]] */
+int  ep_mlp_forward(ep_mlp *m, const float *X, float *Y, int32_t batch, void *stream);
+/* loss = mean_i sum_j w_j (f(X_i)_j - Y_ij)^2 (w = 1 when NULL); gradients
+ * are accumulated into the trainer and optionally copied to grad_host */
+int  ep_mlp_loss_grad(ep_mlp *m, const float *X, const float *Y, const float *w_out_host,
+                      int32_t batch, double *loss, float *grad_host, void *stream);
+int  ep_mlp_adam_step(ep_mlp *m, float lr, float beta1, float beta2, float eps);
+
+/* Deployment of a trained network as the ionic phase of EP_SURROGATE
+ * handles (ten Tusscher only).  Inputs per node, in this order: V, the 18
+ * stored states, I_stim [uA/uF], G_Ks (with the node scale), G_to, the
+ * s-gate variant; outputs: the changes of V and the 18 states over one
+ * global step.  A node whose inputs leave the box [env_lo, env_hi], whose
+ * fast sodium gate product m^3 h exceeds nah_max, or which is being
+ * stimulated, runs the plain FP32 model for that step instead. */
+typedef struct ep_surrogate_desc {
+    int32_t n_in, n_hidden, n_hidden_layers, n_out;
+    const float *params;         /* ep_mlp flattening (FP32; converted to BF16) */
+    const float *in_mean, *in_std, *out_mean, *out_std;
+    const float *env_lo, *env_hi;   /* box in the transformed feature space */
+    float nah_max;
+    uint32_t log_mask;              /* bit k: feature k enters as log(x); for the
+                                       states (k < 19) the output is then the
+                                       change of log(x) and x' = x exp(out) */
+    int32_t v_update;               /* 0: V' = V + dV from the network;
+                                       1: V' = V + dt dV/dt(V + dV/2, (s + s')/2),
+                                       the cell model's own current balance at
+                                       the step midpoint */
+} ep_surrogate_desc;
+int  ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d);
+/* The deployed network alone on host buffers (tests): X [n x 32] already
+ * normalised inputs (23 used), Y [n x 32] raw outputs before
+ * de-normalisation (19 used); runs the same tensor-core kernel. */
+int  ep_surrogate_forward(const ep_surrogate_desc *d, int32_t n, const float *X, float *Y);
 
 #ifdef __cplusplus
 }

@@ -40,7 +40,7 @@ class ModelDesc(C.Structure):
     _fields_ = [("model", C.c_int32), ("n_types", C.c_int32), ("type_consts", dp),
                 ("node_type", C.POINTER(C.c_uint8)), ("node_gks_scale", dp),
                 ("user_xi", C.c_double), ("newton_cap", C.c_int32), ("tt_jacobian", C.c_int32),
-                ("mh_abs_mode", C.c_int32), ("initial_states", dp)]
+                ("mh_abs_mode", C.c_int32), ("initial_states", dp), ("newton_tol", C.c_double)]
 
 
 class SolverDesc(C.Structure):
@@ -150,3 +150,46 @@ def default_consts(model, ctype=0):
     out = np.zeros(nc)
     check(lib().ep_model_default_consts(model, ctype, ptr(out)))
     return out
+
+
+class SurrogateDesc(C.Structure):
+    _fields_ = [("n_in", C.c_int32), ("n_hidden", C.c_int32), ("n_hidden_layers", C.c_int32),
+                ("n_out", C.c_int32), ("params", C.POINTER(C.c_float)),
+                ("in_mean", C.POINTER(C.c_float)), ("in_std", C.POINTER(C.c_float)),
+                ("out_mean", C.POINTER(C.c_float)), ("out_std", C.POINTER(C.c_float)),
+                ("env_lo", C.POINTER(C.c_float)), ("env_hi", C.POINTER(C.c_float)),
+                ("nah_max", C.c_float), ("log_mask", C.c_uint32), ("v_update", C.c_int32)]
+
+
+def _bind_learned(L):
+    fp = C.POINTER(C.c_float)
+    H = C.c_void_p
+    sig = {
+        "ep_ionic_phase": ([C.POINTER(ModelDesc), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                            C.c_double, dp, dp, dp], C.c_int),
+        "ep_mlp_create": ([C.c_int32, C.POINTER(C.c_int32), C.c_uint64, C.c_int, C.POINTER(H)], C.c_int),
+        "ep_mlp_destroy": ([H], None),
+        "ep_mlp_num_params": ([H], C.c_int),
+        "ep_mlp_get_params": ([H, fp], C.c_int),
+        "ep_mlp_set_params": ([H, fp], C.c_int),
+        "ep_mlp_forward": ([H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+        "ep_mlp_loss_grad": ([H, C.c_void_p, C.c_void_p, fp, C.c_int32, dp, fp, C.c_void_p], C.c_int),
+        "ep_mlp_adam_step": ([H, C.c_float, C.c_float, C.c_float, C.c_float], C.c_int),
+        "ep_set_surrogate": ([H, C.POINTER(SurrogateDesc)], C.c_int),
+        "ep_surrogate_forward": ([C.POINTER(SurrogateDesc), C.c_int32, fp, fp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+
+
+_lib_plain = lib
+
+
+def lib():  # noqa: F811  (extends the binding with the learned-step entry points)
+    L = _lib_plain()
+    if not getattr(L, "_learned_bound", False):
+        _bind_learned(L)
+        L._learned_bound = True
+    return L

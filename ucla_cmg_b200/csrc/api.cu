@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "host_fem.h"
 #include "model_defaults.h"
+#include "surrogate.cuh"
 
 namespace ep {
 
@@ -85,6 +86,9 @@ struct ep_handle {
     std::vector<cudaEvent_t> pev;
     std::vector<int> pkind;              // kernel class started at each event
     long long launches = 0;
+    // learned ionic step (EP_SURROGATE)
+    DBuf sg_wimg, sg_aux, sg_list, sg_count, sg_err;
+    int has_surrogate = 0;
 };
 
 namespace {
@@ -253,6 +257,42 @@ static int ensure_ecg_cap(ep_handle *h, int need) {
     return EP_OK;
 }
 
+static void fill_surrogate_args(ep_handle *h, const IonicArgs<float> &ia, SurrogateArgs &sa) {
+    std::memset(&sa, 0, sizeof sa);
+    sa.n = h->n; sa.pitch = h->pitch;
+    sa.V = ia.V; sa.S = ia.S; sa.type = ia.type; sa.gks = ia.gks;
+    sa.consts = ia.consts; sa.nconst = ia.nconst;
+    sa.stim_head = ia.stim_head; sa.stim_next = ia.stim_next;
+    sa.stim_on = ia.stim_on; sa.stim_off = ia.stim_off; sa.stim_amp = ia.stim_amp;
+    sa.step_ptr = ia.step_ptr; sa.t_per_step = h->dt;
+    sa.Cm = ia.Cm; sa.Xi = ia.Xi; sa.act_thr = ia.act_thr;
+    sa.track = ia.track;
+    sa.wimg = h->sg_wimg.as<unsigned short>();
+    sa.aux = h->sg_aux.as<SurrogateAux>();
+    sa.fallback_list = h->sg_list.as<int>();
+    sa.fallback_count = h->sg_count.as<int>();
+    sa.status = h->status.as<DevStatus>();
+    sa.err = h->sg_err.as<unsigned int>();
+}
+
+// the learned ionic phase: tensor-core MLP for the nodes inside the training
+// envelope, then the plain FP32 kernel over the compacted fallback list
+static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
+    if (!h->has_surrogate) {
+        set_error("EP_SURROGATE handle stepped before ep_set_surrogate");
+        return EP_ERR_ARG;
+    }
+    EP_CUDA(cudaMemsetAsync(h->sg_count.p, 0, sizeof(int), h->stream));
+    SurrogateArgs sa;
+    fill_surrogate_args(h, ia, sa);
+    int rc = launch_surrogate(sa, h->stream);
+    if (rc) return rc;
+    IonicArgs<float> fb = ia;
+    fb.node_list = h->sg_list.as<int>();
+    fb.list_count = h->sg_count.as<int>();
+    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream);
+}
+
 enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
 
 // event before each kernel when profiling (the class of the kernel it starts)
@@ -281,7 +321,16 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
         if ((rc = mark(h, ne, K_CG))) return rc;
         if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
         if ((rc = mark(h, ne, K_IONIC))) return rc;
-        if ((rc = launch_ionic<R>(h->model, ia, h->stream))) return rc;
+        if constexpr (sizeof(R) == 4) {
+            if (h->precision == EP_SURROGATE) {
+                if ((rc = launch_learned_phase(h, ia))) return rc;
+                h->launches += 2;
+            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream))) {
+                return rc;
+            }
+        } else {
+            if ((rc = launch_ionic<R>(h->model, ia, h->stream))) return rc;
+        }
         if ((rc = mark(h, ne, K_CG))) return rc;
         if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
         if ((rc = mark(h, ne, K_OTHER))) return rc;
@@ -359,7 +408,9 @@ int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver
     EP_CHECK_ARG(mesh->n_nodes > 0 && mesh->n_tets > 0 && mesh->xyz && mesh->tets, "empty mesh");
     const int nst = ep_model_nstate(md->model);
     EP_CHECK_ARG(nst > 0, "unknown cell model");
-    EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32, "unsupported precision");
+    EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32 ||
+                     (sd->precision == EP_SURROGATE && md->model == EP_TUSSCHER),
+                 "unsupported precision (EP_SURROGATE needs the ten Tusscher model)");
     EP_CHECK_ARG(sd->dt > 0 && sd->ionic_dt > 0, "dt and ionic_dt must be positive");
     const int ntypes = md->n_types > 0 ? md->n_types : 1;
     EP_CHECK_ARG(ntypes <= kMaxTypes, "too many parameter sets");
@@ -617,8 +668,11 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
         stats->ecg_ms = kms[K_ECG];
         stats->launches = h->launches;
     }
-    if (bar.err) {
-        set_error("a grid barrier wait gave up");
+    unsigned int sg_err = 0;
+    if (h->has_surrogate) EP_CUDA(cudaMemcpy(&sg_err, h->sg_err.p, sizeof sg_err, cudaMemcpyDeviceToHost));
+    if (stats) stats->timeouts += (int32_t)sg_err;
+    if (bar.err || sg_err) {
+        set_error(bar.err ? "a grid barrier wait gave up" : "a tensor-core completion wait gave up");
         return EP_ERR_TIMEOUT;
     }
     return EP_OK;
@@ -646,6 +700,112 @@ int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
     if (iters) *iters = (int32_t)last[0];
     if (relres) *relres = last[1];
     if (bar.err) { set_error("a grid barrier wait gave up"); return EP_ERR_TIMEOUT; }
+    return EP_OK;
+}
+
+// IEEE float -> bfloat16, round to nearest even (NaN kept quiet)
+static unsigned short to_bf16(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (unsigned short)((u >> 16) | 0x40u);
+    const uint32_t r = 0x7fffu + ((u >> 16) & 1u);
+    return (unsigned short)((u + r) >> 16);
+}
+
+// BF16 weight images + FP32 side block for the tensor-core kernel
+static int pack_surrogate(const ep_surrogate_desc *d, std::vector<unsigned short> &img, SurrogateAux &aux) {
+    EP_CHECK_ARG(d && d->params, "null surrogate descriptor");
+    if (d->n_in != SG_NF || d->n_hidden != SG_H || d->n_hidden_layers != 3 || d->n_out != SG_NY) {
+        set_error("surrogate shape %d-%dx%d-%d unsupported (the kernel is %d-%dx3-%d)", d->n_in, d->n_hidden,
+                  d->n_hidden_layers, d->n_out, SG_NF, SG_H, SG_NY);
+        return EP_ERR_UNSUPPORTED;
+    }
+    EP_CHECK_ARG(d->in_mean && d->in_std && d->out_mean && d->out_std && d->env_lo && d->env_hi,
+                 "normalisation and envelope arrays are required");
+    img.assign(SG_WTOT, 0);
+    std::memset(&aux, 0, sizeof aux);
+    const float *p = d->params;
+    const int dims[5] = {SG_NF, SG_H, SG_H, SG_H, SG_NY};
+    const int Kpad[4] = {SG_KIN, SG_H, SG_H, SG_H};
+    const int base[4] = {0, SG_W1, SG_W1 + SG_W2, SG_W1 + SG_W2 + SG_W3};
+    float *bias[4] = {aux.b1, aux.b2, aux.b3, aux.b4};
+    size_t off = 0;
+    for (int l = 0; l < 4; l++) {
+        const int nout = dims[l + 1], nin = dims[l];
+        for (int r = 0; r < nout; r++)
+            for (int k = 0; k < nin; k++)
+                img[base[l] + core_offset(r, k, Kpad[l])] = to_bf16(p[off + (size_t)r * nin + k]);
+        off += (size_t)nout * nin;
+        for (int r = 0; r < nout; r++) bias[l][r] = p[off + r];
+        off += nout;
+    }
+    for (int k = 0; k < SG_KIN; k++) {
+        const bool used = k < SG_NF;
+        aux.in_mean[k] = used ? d->in_mean[k] : 0.f;
+        aux.in_rstd[k] = used && d->in_std[k] > 0.f ? 1.f / d->in_std[k] : 0.f;
+        aux.env_lo[k] = used ? d->env_lo[k] : -3.0e38f;
+        aux.env_hi[k] = used ? d->env_hi[k] : 3.0e38f;
+    }
+    for (int j = 0; j < SG_NOUT; j++) {
+        aux.out_mean[j] = j < SG_NY ? d->out_mean[j] : 0.f;
+        aux.out_std[j] = j < SG_NY ? d->out_std[j] : 0.f;
+    }
+    aux.nah_max = d->nah_max;
+    aux.log_mask = d->log_mask & ((1u << SG_NF) - 1u) & ~1u;   // V stays linear
+    EP_CHECK_ARG(d->v_update == 0 || d->v_update == 1, "v_update must be 0 or 1");
+    aux.v_update = d->v_update;
+    return EP_OK;
+}
+
+int ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CHECK_ARG(h->precision == EP_SURROGATE, "the handle was not created with EP_SURROGATE");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<unsigned short> img;
+    SurrogateAux aux;
+    int rc = pack_surrogate(d, img, aux);
+    if (rc) return rc;
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    if ((rc = upload_raw(h->sg_wimg, img.data(), img.size()))) return rc;
+    if ((rc = upload_raw(h->sg_aux, &aux, 1))) return rc;
+    if (!h->sg_list.p) {
+        if ((rc = h->sg_list.alloc(sizeof(int) * (size_t)h->pitch))) return rc;
+        if ((rc = h->sg_count.alloc(sizeof(int)))) return rc;
+        if ((rc = h->sg_err.alloc(sizeof(unsigned int)))) return rc;
+    }
+    EP_CUDA(cudaMemset(h->sg_err.p, 0, sizeof(unsigned int)));
+    h->has_surrogate = 1;
+    return EP_OK;
+}
+
+int ep_surrogate_forward(const ep_surrogate_desc *d, int32_t n, const float *X, float *Y) {
+    EP_CHECK_ARG(d && X && Y && n > 0, "bad arguments");
+    std::vector<unsigned short> img;
+    SurrogateAux aux;
+    int rc = pack_surrogate(d, img, aux);
+    if (rc) return rc;
+    DBuf dimg, daux, dx, dy, derr, dstat;
+    if ((rc = upload_raw(dimg, img.data(), img.size())) || (rc = upload_raw(daux, &aux, 1)) ||
+        (rc = upload_raw(dx, X, (size_t)n * SG_KIN)) || (rc = dy.alloc(sizeof(float) * (size_t)n * SG_NOUT)) ||
+        (rc = derr.alloc(sizeof(unsigned int))) || (rc = dstat.alloc(sizeof(DevStatus))))
+        return rc;
+    EP_CUDA(cudaMemset(derr.p, 0, sizeof(unsigned int)));
+    EP_CUDA(cudaMemset(dstat.p, 0, sizeof(DevStatus)));
+    SurrogateArgs sa;
+    std::memset(&sa, 0, sizeof sa);
+    sa.n = n;
+    sa.wimg = dimg.as<unsigned short>();
+    sa.aux = daux.as<SurrogateAux>();
+    sa.rawX = dx.as<float>();
+    sa.rawY = dy.as<float>();
+    sa.err = derr.as<unsigned int>();
+    sa.status = dstat.as<DevStatus>();
+    if ((rc = launch_surrogate(sa, 0))) return rc;
+    EP_CUDA(cudaDeviceSynchronize());
+    unsigned int err = 0;
+    EP_CUDA(cudaMemcpy(&err, derr.p, sizeof err, cudaMemcpyDeviceToHost));
+    EP_CUDA(cudaMemcpy(Y, dy.p, sizeof(float) * (size_t)n * SG_NOUT, cudaMemcpyDeviceToHost));
+    if (err) { set_error("a tensor-core completion wait gave up"); return EP_ERR_TIMEOUT; }
     return EP_OK;
 }
 
@@ -772,9 +932,13 @@ int ep_read_restart(ep_handle *h, double t, const char *dir) {
     return EP_OK;
 }
 
-int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double dt, double Cm,
-                  const double *V, const double *istim, double *states, double *dvdt) {
-    EP_CHECK_ARG(md && V && states && dvdt && n > 0, "bad arguments");
+// Independent cells through the ionic kernel: one Compute_Ion call per cell
+// returning dV/dt (dvdt != NULL, V unchanged), or a whole ionic phase of
+// sub-steps with the V update (dvdt == NULL, V advanced in place).
+static int ionic_batch(const ep_model_desc *md, int32_t precision, int32_t n, double dt,
+                       double ionic_dt, double Cm, double *V, const double *istim, double *states,
+                       double *dvdt) {
+    EP_CHECK_ARG(md && V && states && n > 0, "bad arguments");
     EP_CHECK_ARG(precision == EP_FP64 || precision == EP_FP32, "unsupported precision");
     const int nst = ep_model_nstate(md->model);
     EP_CHECK_ARG(nst > 0, "unknown model");
@@ -785,11 +949,15 @@ int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double 
     h.n = n; h.pitch = (n + 31) / 32 * 32; h.model = md->model; h.precision = precision;
     h.nstate = nst; h.ns = is_lr(md->model) ? 7 : nst - 1; h.ntypes = ntypes;
     h.dt = dt; h.nsub = 1; h.sub_dt[0] = dt; h.Cm = Cm;
+    if (!dvdt) {
+        h.nsub = substeps(dt, ionic_dt > 0 ? ionic_dt : dt, h.sub_dt);
+        EP_CHECK_ARG(h.nsub > 0, "more than 64 ionic sub-steps");
+    }
     h.Xi = md->user_xi > 0 ? md->user_xi : model_xi(md->model);
     h.tt.newton_cap = md->newton_cap > 0 ? md->newton_cap : 100;
     h.tt.jac_true = md->tt_jacobian == EP_TT_JAC_TRUE ? 1 : 0;
     h.tt.fp32_scaled_tol = precision == EP_FP64 ? 0 : 1;
-    h.tt.newton_tol = 1e-6;
+    h.tt.newton_tol = md->newton_tol > 0 ? md->newton_tol : 1e-6;
     h.mh_abs = md->mh_abs_mode ? 1 : 0;
     const int nc = ep_model_nconst(md->model);
     std::vector<double> consts((size_t)ntypes * nc);
@@ -840,17 +1008,20 @@ int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double 
         IonicArgs<R> a;
         fill_ionic_args<R>(&h, a);
         a.track = nullptr;
-        a.dvdt_out = dvd.as<R>();
+        a.dvdt_out = dvdt ? dvd.as<R>() : nullptr;
         if ((r2 = launch_ionic<R>(h.model, a, h.stream))) return r2;
         EP_CUDA(cudaStreamSynchronize(h.stream));
         std::vector<double> o, so;
-        if ((r2 = download<R>(dvd, o, n, h.stream))) return r2;
+        if ((r2 = download<R>(dvdt ? dvd : h.V, o, n, h.stream))) return r2;
         if ((r2 = download<R>(h.S, so, (size_t)h.ns * h.pitch, h.stream))) return r2;
         for (int i = 0; i < n; i++) {
-            dvdt[i] = o[i];
+            if (dvdt) dvdt[i] = o[i];
+            else V[i] = o[i];
             double *s = states + (size_t)i * nst;
-            if (is_lr(md->model)) for (int k = 0; k < 7; k++) s[k] = so[(size_t)k * h.pitch + i];
-            else {
+            if (is_lr(md->model)) {
+                for (int k = 0; k < 7; k++) s[k] = so[(size_t)k * h.pitch + i];
+                s[7] = V[i];
+            } else {
                 s[0] = V[i];
                 for (int k = 0; k < h.ns; k++) s[k + 1] = so[(size_t)k * h.pitch + i];
             }
@@ -861,6 +1032,18 @@ int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double 
     cudaStreamDestroy(h.stream);
     h.stream = nullptr;
     return rc;
+}
+
+int ep_ionic_step(const ep_model_desc *md, int32_t precision, int32_t n, double dt, double Cm,
+                  const double *V, const double *istim, double *states, double *dvdt) {
+    EP_CHECK_ARG(V && dvdt, "null V or dvdt");
+    std::vector<double> v(V, V + (n > 0 ? n : 0));
+    return ionic_batch(md, precision, n, dt, 0.0, Cm, v.data(), istim, states, dvdt);
+}
+
+int ep_ionic_phase(const ep_model_desc *md, int32_t precision, int32_t n, double dt,
+                   double ionic_dt, double Cm, double *V, const double *istim, double *states) {
+    return ionic_batch(md, precision, n, dt, ionic_dt, Cm, V, istim, states, nullptr);
 }
 
 }  // extern "C"

@@ -10,6 +10,41 @@ namespace ep {
 // Per-node activation record {t_act, t_rep, v_peak, v_rest}; -1 = not yet.
 struct Track { float t_act, t_rep, v_peak, v_rest; };
 
+// Update the record over one interval [t0, t0 + h] in which V goes v0 -> v1
+// (an ionic sub-step, or a whole learned step).  A crossing inside the
+// interval is interpolated linearly; a node already past the threshold at
+// the interval's start crossed during the preceding diffusion half step and
+// is stamped t0 (at most dt/2 late).  Activation: upward crossing of thr;
+// repolarisation (APD90): downward crossing of v_peak - 0.9 (v_peak - v_rest)
+// later than 5 ms after activation.
+__device__ __forceinline__ void track_interval(Track &tr, bool &dirty, float v0, float v1, double t0, float h,
+                                               float thr) {
+    if (tr.t_act < 0.f) {
+        if (v0 < tr.v_rest) { tr.v_rest = v0; dirty = true; }
+        if (v0 >= thr) {
+            tr.t_act = (float)t0;
+            tr.v_peak = fmaxf(v0, v1);
+            dirty = true;
+        } else if (v1 >= thr) {
+            tr.t_act = (float)(t0 + (double)((thr - v0) / (v1 - v0) * h));
+            tr.v_peak = v1;
+            dirty = true;
+        }
+    } else if (tr.t_rep < 0.f) {
+        if (v1 > tr.v_peak) { tr.v_peak = v1; dirty = true; }
+        const float v90 = tr.v_peak - 0.9f * (tr.v_peak - tr.v_rest);
+        if ((float)t0 > tr.t_act + 5.f) {
+            if (v0 < v90) {
+                tr.t_rep = (float)t0;
+                dirty = true;
+            } else if (v1 < v90) {
+                tr.t_rep = (float)(t0 + (double)((v0 - v90) / (v0 - v1) * h));
+                dirty = true;
+            }
+        }
+    }
+}
+
 // Ionic phase of one global step for all nodes: the reference loop of
 // EP_CrankNicholson::Solve (Solvers/EP_CrankNicholson.cc:114-143) with
 // CardiacBody::getIonicCurrent (Body/CardiacBody.cc:405-435) inside.
@@ -35,6 +70,8 @@ template <typename R> struct IonicArgs {
     int nconst;
     R *dvdt_out;                 // non-null: plugin mode -- write the returned
                                  // dV/dt, leave V unchanged (one sub-step)
+    const int *node_list;        // non-null: run only these nodes (count on the device)
+    const int *list_count;
     // model options
     TTOpts tt;
     int mh_abs;

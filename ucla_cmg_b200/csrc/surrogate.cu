@@ -1,0 +1,372 @@
+// surrogate.cu -- BF16 tensor-core (tcgen05) inference of the learned ionic
+// step, one persistent CTA per half SM.
+//
+// Per tile of 128 nodes (one node per thread = one TMEM lane):
+//   1. features of the node (V, 18 states, I_stim, G_Ks, G_to, s-gate) ->
+//      normalised -> BF16 row of the A operand in shared memory;
+//   2. four layers: one elected thread issues tcgen05.mma (kind::f16, BF16 x
+//      BF16 -> FP32 in TMEM, M = 128, N = 128 or 32, K = 16 per instruction)
+//      with A = activations and B = the layer's weights, both resident in
+//      shared memory as no-swizzle K-major core matrices, then
+//      tcgen05.commit arrives on an mbarrier;
+//   3. every warp reads its 32 TMEM lanes back (tcgen05.ld 32x32b), adds the
+//      bias, applies tanh.approx and writes the next BF16 A operand;
+//   4. the output layer's 19 values are de-normalised and added to the
+//      node's state; nodes outside the training envelope (input box, fast
+//      Na-gate product m^3 h, an active stimulus) are appended to a fallback
+//      list that the plain FP32 kernel then runs.
+// The weights (80 KB) are loaded once per CTA.  Shared memory 112 KB and
+// 256 TMEM columns per CTA, so two CTAs share an SM and one's epilogue
+// overlaps the other's MMAs.  Every mbarrier wait is bounded; on timeout the
+// CTA records the error, frees its TMEM and leaves.
+#include <cuda_bf16.h>
+
+#include "surrogate.cuh"
+#include "tt.cuh"
+
+namespace ep {
+
+constexpr int OFF_W1 = 0;
+constexpr int OFF_W2 = OFF_W1 + SG_W1 * 2;
+constexpr int OFF_W3 = OFF_W2 + SG_W2 * 2;
+constexpr int OFF_W4 = OFF_W3 + SG_W3 * 2;
+constexpr int OFF_A = OFF_W4 + SG_W4 * 2;                 // 128 x 128 bf16
+constexpr int OFF_MISC = OFF_A + SG_M * SG_H * 2;
+constexpr int SG_SMEM = OFF_MISC + 64;
+constexpr uint32_t SG_TMEM_COLS = 256;
+
+size_t surrogate_smem_bytes() { return SG_SMEM; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor: no swizzle, K-major; lbo/sbo in bytes
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: BF16 x BF16 -> F32, both K-major
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *holder, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(holder)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// issue one layer: D[128 x N] = A[128 x K] W^T, W = [N x K]; thread 0 only
+__device__ __forceinline__ void issue_layer(uint32_t d, uint32_t sA, uint32_t sW, int K, int N, uint64_t *bar) {
+    const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+    const uint32_t id = idesc_bf16(SG_M, N);
+    for (int kk = 0; kk < K / 16; kk++) {
+        const uint32_t off = (uint32_t)kk * 256u;          // two 128-byte core matrices along K
+        umma_bf16(d, umma_desc(sA + off, 128u, sbo), umma_desc(sW + off, 128u, sbo), id, kk > 0 ? 1u : 0u);
+    }
+    umma_commit(bar);
+}
+
+// block-uniform bounded wait for the next commit of this CTA
+__device__ __forceinline__ bool wait_commit(uint64_t *bar, uint32_t &phase, unsigned int *err) {
+    bool ok = false;
+    for (int it = 0; it < (1 << 22); it++)
+        if (mbar_try_wait(bar, phase)) { ok = true; break; }
+    phase ^= 1u;
+    const int bad = __syncthreads_or(ok ? 0 : 1);
+    if (bad) {
+        if (threadIdx.x == 0) atomicExch(err, 1u);
+        return false;
+    }
+    tc_fence_after();
+    return true;
+}
+
+// hidden-layer epilogue: TMEM -> +bias -> tanh -> BF16 A row (K = 128 layout)
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *__restrict__ bias, unsigned char *A) {
+    const int r = threadIdx.x;
+#pragma unroll 1
+    for (int q = 0; q < SG_H / 32; q++) {
+        uint32_t v[32];
+        tmem_ld32(tmem_row + 32u * q, v);
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const float a0 = tanh_fast(__uint_as_float(v[2 * j]) + __ldg(bias + 32 * q + 2 * j));
+            const float a1 = tanh_fast(__uint_as_float(v[2 * j + 1]) + __ldg(bias + 32 * q + 2 * j + 1));
+            w[j] = pack_bf16(a0, a1);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int chunk = 4 * q + c;
+            uint4 *dst = (uint4 *)(A + ((r >> 3) * (SG_H / 8) + chunk) * 128 + (r & 7) * 16);
+            *dst = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint64_t *bar = (uint64_t *)(smem + OFF_MISC);
+    uint32_t *holder = (uint32_t *)(smem + OFF_MISC + 16);
+    unsigned char *A = smem + OFF_A;
+    const SurrogateAux *aux = a.aux;
+
+    // weights: global image -> shared (already in core-matrix order)
+    {
+        const uint4 *src = (const uint4 *)a.wimg;
+        uint4 *dst = (uint4 *)smem;
+        for (int i = tid; i < SG_WTOT * 2 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    if (tid == 0) mbar_init(bar, 1);
+    if (warp == 0) tmem_alloc(holder, SG_TMEM_COLS);
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *holder;
+    const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+    const uint32_t d_hid = tmem, d_out = tmem + 128u;
+    const uint32_t sW1 = smem_u32(smem + OFF_W1), sW2 = smem_u32(smem + OFF_W2);
+    const uint32_t sW3 = smem_u32(smem + OFF_W3), sW4 = smem_u32(smem + OFF_W4);
+    const uint32_t sA = smem_u32(A);
+    uint32_t phase = 0;
+    unsigned int my_fb = 0;
+    const bool raw = a.rawX != nullptr;
+    const long long step = raw ? 0 : *a.step_ptr;
+    const double t0 = (double)step * a.t_per_step;
+    const int ntiles = (a.n + SG_M - 1) / SG_M;
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int i = tile * SG_M + tid;
+        const bool valid = i < a.n;
+        float x[SG_NF];
+        float xn[SG_KIN];
+        bool inside = false;
+        float istim = 0.f;
+        const float *c = a.consts;
+        float gks_i = 1.f;
+#pragma unroll
+        for (int k = 0; k < SG_KIN; k++) xn[k] = 0.f;
+        if (valid && raw) {
+#pragma unroll
+            for (int k = 0; k < SG_KIN; k++) xn[k] = a.rawX[(size_t)i * SG_KIN + k];
+        } else if (valid) {
+            x[0] = a.V[i];
+#pragma unroll
+            for (int k = 0; k < 18; k++) x[k + 1] = a.S[(size_t)k * a.pitch + i];
+            const int ty = a.type ? a.type[i] : 0;
+            c = a.consts + (size_t)ty * a.nconst;
+            gks_i = a.gks ? a.gks[i] : 1.f;
+            if (a.stim_head) {
+                int k = a.stim_head[i];
+                long long best = -1;
+                while (k >= 0) {
+                    const long long on = a.stim_on[k], off = a.stim_off[k];
+                    if (step >= on && step < off && on > best) { best = on; istim = a.stim_amp[k]; }
+                    k = a.stim_next[k];
+                }
+            }
+            x[19] = istim / (a.Cm * a.Xi);
+            x[20] = c[15] * gks_i;
+            x[21] = c[20];
+            x[22] = c[53];
+            inside = (istim == 0.f);
+            const float m = x[7], h = x[8];
+            inside = inside && (m * m * m * h <= aux->nah_max);
+            const unsigned int lm = aux->log_mask;
+#pragma unroll
+            for (int k = 0; k < SG_NF; k++) {
+                // quantities spanning decades enter as logarithms
+                const float xt = ((lm >> k) & 1u) ? __logf(fmaxf(x[k], 1e-30f)) : x[k];
+                inside = inside && (xt >= aux->env_lo[k]) && (xt <= aux->env_hi[k]);
+                xn[k] = (xt - aux->in_mean[k]) * aux->in_rstd[k];
+            }
+        }
+        // input row (K = 32 layout)
+        {
+            uint32_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) w[j] = pack_bf16(xn[2 * j], xn[2 * j + 1]);
+#pragma unroll
+            for (int cch = 0; cch < 4; cch++) {
+                uint4 *dst = (uint4 *)(A + ((tid >> 3) * (SG_KIN / 8) + cch) * 128 + (tid & 7) * 16);
+                *dst = make_uint4(w[4 * cch], w[4 * cch + 1], w[4 * cch + 2], w[4 * cch + 3]);
+            }
+        }
+        // layer 1 (K = 32), 2, 3 (K = 128): hidden, tanh
+        const uint32_t sW[3] = {sW1, sW2, sW3};
+        const float *bias[3] = {aux->b1, aux->b2, aux->b3};
+        bool ok = true;
+#pragma unroll 1
+        for (int l = 0; l < 3 && ok; l++) {
+            fence_proxy_async();
+            tc_fence_before();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                issue_layer(d_hid, sA, sW[l], l == 0 ? SG_KIN : SG_H, SG_H, bar);
+            }
+            ok = wait_commit(bar, phase, a.err);
+            if (ok) hidden_epilogue(d_hid + lane_off, bias[l], A);
+        }
+        if (!ok) break;
+        // output layer (K = 128, N = 32)
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            issue_layer(d_out, sA, sW4, SG_H, SG_NOUT, bar);
+        }
+        if (!wait_commit(bar, phase, a.err)) break;
+        uint32_t yv[32];
+        tmem_ld32(d_out + lane_off, yv);
+        tc_fence_before();
+        if (valid && raw) {
+#pragma unroll
+            for (int j = 0; j < SG_NOUT; j++) a.rawY[(size_t)i * SG_NOUT + j] = __uint_as_float(yv[j]) + aux->b4[j];
+        } else if (valid && inside) {
+            float d[SG_NY];
+#pragma unroll
+            for (int j = 0; j < SG_NY; j++)
+                d[j] = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+            const unsigned int lm = aux->log_mask;
+            float sn[18];
+#pragma unroll
+            for (int k = 0; k < 18; k++) {
+                // log-scaled states are updated multiplicatively: x' = x exp(d)
+                const float xk = x[k + 1];
+                sn[k] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
+                a.S[(size_t)k * a.pitch + i] = sn[k];
+            }
+            const float V0 = x[0];
+            float V1 = x[0] + d[0];
+            if (aux->v_update == 1) {
+                // midpoint rule on the model's own current balance: the
+                // network's dV only places the midpoint; the states there are
+                // the mean of the old and the predicted new states
+                float sm[18];
+#pragma unroll
+                for (int k = 0; k < 18; k++) sm[k] = 0.5f * (x[k + 1] + sn[k]);
+                const float dt = (float)a.t_per_step;
+                V1 = V0 + dt * tt_dvdt<float>(V0 + 0.5f * d[0], sm, c, 0.f, gks_i);
+            }
+            a.V[i] = V1;
+            if (a.track) {
+                Track tr = a.track[i];
+                if (tr.t_rep < 0.f) {
+                    bool dirty = false;
+                    track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
+                    if (dirty) a.track[i] = tr;
+                }
+            }
+        } else if (valid) {
+            const int slot = atomicAdd(a.fallback_count, 1);
+            a.fallback_list[slot] = i;
+            my_fb++;
+        }
+    }
+    // count fallback node-steps
+    for (int o = 16; o > 0; o >>= 1) my_fb += __shfl_xor_sync(0xffffffffu, my_fb, o);
+    if ((tid & 31) == 0 && my_fb && a.status) atomicAdd(&a.status->fallback, (unsigned long long)my_fb);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, SG_TMEM_COLS);
+}
+
+int launch_surrogate(const SurrogateArgs &a, cudaStream_t s) {
+    static int configured = 0;
+    if (!configured) {
+        EP_CUDA(cudaFuncSetAttribute(k_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, SG_SMEM));
+        configured = 1;
+    }
+    int dev = 0, nsm = 148;
+    EP_CUDA(cudaGetDevice(&dev));
+    EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int ntiles = (a.n + SG_M - 1) / SG_M;
+    const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
+    if (grid <= 0) return EP_OK;
+    k_surrogate<<<grid, 128, SG_SMEM, s>>>(a);
+    EP_CUDA(cudaGetLastError());
+    return EP_OK;
+}
+
+}  // namespace ep

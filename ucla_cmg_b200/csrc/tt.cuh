@@ -203,6 +203,22 @@ EP_HD void tt_nr_rates(const R x[6], const TTRev<R> &e, const TTFixed<R> &f,
                     - (j_xfer * c[4]) / c[52]);
 }
 
+// dV/dt of the model at an arbitrary state (the current balance of
+// ComputeRates, Tusscher.cc:56-78), s = the 18 stored states
+template <typename R>
+EP_HD R tt_dvdt(R V, const R *s, const R *__restrict__ c, R ist, R gks) {
+    const TTFixed<R> f = tt_fixed<R>(V, s, c, ist, gks);
+    TTRev<R> e;
+    tt_rev_na(e, s[1], c, f);
+    tt_rev_k(e, s[0], c, f);
+    tt_rev_ks(e, s[0], s[1], c, f);
+    tt_rev_ca(e, s[2], c, f);
+    const R x[6] = {s[0], s[1], s[2], s[9], s[16], s[17]};
+    R r[6], dvdt;
+    tt_nr_rates(x, e, f, c, r, dvdt);
+    return dvdt;
+}
+
 // In-register 6x6 solve A x = b, A column-major (LAPACK convention),
 // partial pivoting in the getf2 order; b is overwritten with x.
 template <typename R>
