@@ -72,7 +72,7 @@ typedef struct ep_mesh_desc {
  * (Body/CardiacBody.cc:975-1101, IonicModel/SetUpIonicConstants.h). */
 typedef struct ep_model_desc {
     int32_t model;              /* EP_TUSSCHER, ... */
-    int32_t n_types;            /* parameter sets (<= 16) */
+    int32_t n_types;            /* parameter sets (<= 256) */
     const double *type_consts;  /* n_types * ep_model_nconst(model), or NULL:
                                    the reference constants for type 0..n_types-1 */
     const uint8_t *node_type;   /* n_nodes or NULL (all type 0) */
@@ -206,6 +206,50 @@ int  ep_cn_half_step_noalloc(int32_t precision, int32_t n, int32_t nslices,
 /* simulated time (ms) and step count */
 int  ep_get_time(ep_handle *h, double *t, int64_t *step);
 
+/* Batches of independent tissue instances.  No counterpart in the
+ * reference (one EPSimulator per mesh).  n_inst meshes of any sizes, each
+ * with its own parameter sets, stimuli, activation trackers and CG stop
+ * test, advanced together: every kernel of a step covers all instances at
+ * once, and the persistent CG launch gives each instance its own group of
+ * CTAs (in proportion to its rows) with its own grid barrier, so the
+ * instances never wait for one another inside a solve.  Nodes (and every
+ * per-node array of the API) are the instances' nodes concatenated in
+ * order; node_offset[k] is where instance k starts.  All instances share
+ * the cell model, C_m and the solver settings; the type tables are
+ * concatenated (at most 256 parameter sets in all).  The pseudo-ECG is not
+ * available on a batch handle. */
+int  ep_batch_create(int32_t n_inst, const ep_mesh_desc *meshes, const ep_model_desc *models,
+                     const ep_solver_desc *solver, int device, ep_handle **out);
+/* n_inst, node_offset[n_inst + 1] and cta_offset[n_inst + 1] (CG groups);
+ * any pointer may be NULL */
+int  ep_batch_layout(const ep_handle *h, int32_t *n_inst, int32_t *node_offset, int32_t *cta_offset);
+/* per instance: CG iterations and ||r||/||r0|| of the latest solve */
+int  ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres);
+/* The CTA-group split itself (host only, for tests): every instance at
+ * least one CTA, the remaining grid - n_inst in proportion to its SELL-32
+ * slices by largest remainder.  inst_blk[n_inst + 1]. */
+int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_t *inst_blk);
+
+/* Launch shape of ep_step (no reference counterpart).  cg_block: threads
+ * per CTA of the persistent CG launch (128 or 256); cg_per_sm: its CTAs per
+ * SM (0 = as many as are co-resident); ionic_block: threads per CTA of the
+ * ionic kernel (64 or 128); graph_steps: 0 launches every kernel from the
+ * host, k > 0 replays the steps from an instantiated CUDA graph of k steps
+ * (rounded up to a multiple of the ECG interval). */
+typedef struct ep_launch_config {
+    int32_t cg_block, cg_per_sm, ionic_block, graph_steps;
+} ep_launch_config;
+int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
+int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);
+/* Autotuner: times trial_steps steps (after one untimed pass) for the
+ * current shape, then by coordinate descent over the CG block size and CTAs
+ * per SM, the ionic block size and graph replay, keeps the fastest and sets
+ * it.  The simulation state (V, states, trackers, step, ECG samples) is put
+ * back afterwards.  best_ms / start_ms: device ms per step of the chosen and
+ * of the starting shape; any output may be NULL. */
+int  ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, double *best_ms,
+                 double *start_ms, int32_t *n_tried);
+
 /* Activation time (first upward crossing of act_threshold, ms, -1 if none)
  * and APD90 (ms, -1 if not repolarised) per node. */
 int  ep_get_activation(ep_handle *h, double *t_act, double *apd90);
@@ -270,10 +314,17 @@ typedef struct ep_surrogate_desc {
     uint32_t log_mask;              /* bit k: feature k enters as log(x); for the
                                        states (k < 19) the output is then the
                                        change of log(x) and x' = x exp(out) */
+    const float *out_scale;         /* NULL, or per output s_j > 0: the network
+                                       predicts asinh(delta_j / s_j) (0: delta_j) */
     int32_t v_update;               /* 0: V' = V + dV from the network;
                                        1: V' = V + dt dV/dt(V + dV/2, (s + s')/2),
                                        the cell model's own current balance at
-                                       the step midpoint */
+                                       the step midpoint;
+                                       2: only the six Newton concentrations
+                                       (Ki, Nai, Cai, Cass, CaSR, R') come from
+                                       the network (interpolated over the
+                                       sub-steps); the gates and V follow the
+                                       reference sub-step scheme */
 } ep_surrogate_desc;
 int  ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d);
 /* The deployed network alone on host buffers (tests): X [n x 32] already

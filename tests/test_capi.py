@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from ucla_cmg_b200 import capi
 
@@ -54,3 +55,21 @@ def test_bad_arguments_return_codes():
     h = C.c_void_p()
     rc = L.ep_create(None, None, None, 0, C.byref(h))
     assert rc == -1 and b"null" in L.ep_last_error()
+
+
+def test_batch_plan_host():
+    """CTA groups of the batched CG launch: at least one CTA per instance,
+    all CTAs used, the rest in proportion to the SELL-32 slices."""
+    from ucla_cmg_b200.simulation import batch_plan
+    rng = np.random.default_rng(3)
+    sizes = rng.integers(2646, 112212, 64)
+    row = np.concatenate([[0], np.cumsum(sizes)])
+    for grid in (64, 148, 296, 592):
+        blk = batch_plan(row, grid)
+        cnt = np.diff(blk)
+        assert blk[0] == 0 and blk[-1] == grid and cnt.min() >= 1
+        slices = (row[1:] + 31) // 32 - row[:-1] // 32
+        ideal = 1 + (grid - 64) * slices / slices.sum()
+        assert np.all(np.abs(cnt - ideal) < 1.0 + 1e-9)
+    with pytest.raises(capi.EPError):
+        batch_plan(row, 63)

@@ -62,6 +62,24 @@ class StepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SurrogateDesc(C.Structure):
+    _fields_ = [("n_in", C.c_int32), ("n_hidden", C.c_int32), ("n_hidden_layers", C.c_int32),
+                ("n_out", C.c_int32), ("params", C.POINTER(C.c_float)),
+                ("in_mean", C.POINTER(C.c_float)), ("in_std", C.POINTER(C.c_float)),
+                ("out_mean", C.POINTER(C.c_float)), ("out_std", C.POINTER(C.c_float)),
+                ("env_lo", C.POINTER(C.c_float)), ("env_hi", C.POINTER(C.c_float)),
+                ("nah_max", C.c_float), ("log_mask", C.c_uint32),
+                ("out_scale", C.POINTER(C.c_float)), ("v_update", C.c_int32)]
+
+
+class LaunchConfig(C.Structure):
+    _fields_ = [("cg_block", C.c_int32), ("cg_per_sm", C.c_int32), ("ionic_block", C.c_int32),
+                ("graph_steps", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _L = None
 
 
@@ -74,6 +92,8 @@ def lib():
         raise RuntimeError(f"{LIB_PATH} is not built: run `python -m ucla_cmg_b200.build`")
     L = C.CDLL(LIB_PATH)
     H = C.c_void_p
+    fp = C.POINTER(C.c_float)
+    ip = C.POINTER(C.c_int32)
     sig = {
         "ep_version": ([], C.c_int),
         "ep_last_error": ([], C.c_char_p),
@@ -107,6 +127,26 @@ def lib():
         "ep_read_restart": ([H, C.c_double, C.c_char_p], C.c_int),
         "ep_ionic_step": ([C.POINTER(ModelDesc), C.c_int32, C.c_int32, C.c_double, C.c_double,
                            dp, dp, dp, dp], C.c_int),
+        "ep_ionic_phase": ([C.POINTER(ModelDesc), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                            C.c_double, dp, dp, dp], C.c_int),
+        "ep_mlp_create": ([C.c_int32, C.POINTER(C.c_int32), C.c_uint64, C.c_int, C.POINTER(H)], C.c_int),
+        "ep_mlp_destroy": ([H], None),
+        "ep_mlp_num_params": ([H], C.c_int),
+        "ep_mlp_get_params": ([H, fp], C.c_int),
+        "ep_mlp_set_params": ([H, fp], C.c_int),
+        "ep_mlp_forward": ([H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+        "ep_mlp_loss_grad": ([H, C.c_void_p, C.c_void_p, fp, C.c_int32, dp, fp, C.c_void_p], C.c_int),
+        "ep_mlp_adam_step": ([H, C.c_float, C.c_float, C.c_float, C.c_float], C.c_int),
+        "ep_set_surrogate": ([H, C.POINTER(SurrogateDesc)], C.c_int),
+        "ep_surrogate_forward": ([C.POINTER(SurrogateDesc), C.c_int32, fp, fp], C.c_int),
+        "ep_batch_create": ([C.c_int32, C.POINTER(MeshDesc), C.POINTER(ModelDesc), C.POINTER(SolverDesc),
+                             C.c_int, C.POINTER(H)], C.c_int),
+        "ep_batch_layout": ([H, ip, ip, ip], C.c_int),
+        "ep_batch_cg_last": ([H, ip, dp], C.c_int),
+        "ep_batch_plan": ([C.c_int32, ip, C.c_int32, ip], C.c_int),
+        "ep_get_launch_config": ([H, C.POINTER(LaunchConfig)], C.c_int),
+        "ep_set_launch_config": ([H, C.POINTER(LaunchConfig)], C.c_int),
+        "ep_autotune": ([H, C.c_int32, C.POINTER(LaunchConfig), dp, dp, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -150,46 +190,3 @@ def default_consts(model, ctype=0):
     out = np.zeros(nc)
     check(lib().ep_model_default_consts(model, ctype, ptr(out)))
     return out
-
-
-class SurrogateDesc(C.Structure):
-    _fields_ = [("n_in", C.c_int32), ("n_hidden", C.c_int32), ("n_hidden_layers", C.c_int32),
-                ("n_out", C.c_int32), ("params", C.POINTER(C.c_float)),
-                ("in_mean", C.POINTER(C.c_float)), ("in_std", C.POINTER(C.c_float)),
-                ("out_mean", C.POINTER(C.c_float)), ("out_std", C.POINTER(C.c_float)),
-                ("env_lo", C.POINTER(C.c_float)), ("env_hi", C.POINTER(C.c_float)),
-                ("nah_max", C.c_float), ("log_mask", C.c_uint32), ("v_update", C.c_int32)]
-
-
-def _bind_learned(L):
-    fp = C.POINTER(C.c_float)
-    H = C.c_void_p
-    sig = {
-        "ep_ionic_phase": ([C.POINTER(ModelDesc), C.c_int32, C.c_int32, C.c_double, C.c_double,
-                            C.c_double, dp, dp, dp], C.c_int),
-        "ep_mlp_create": ([C.c_int32, C.POINTER(C.c_int32), C.c_uint64, C.c_int, C.POINTER(H)], C.c_int),
-        "ep_mlp_destroy": ([H], None),
-        "ep_mlp_num_params": ([H], C.c_int),
-        "ep_mlp_get_params": ([H, fp], C.c_int),
-        "ep_mlp_set_params": ([H, fp], C.c_int),
-        "ep_mlp_forward": ([H, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
-        "ep_mlp_loss_grad": ([H, C.c_void_p, C.c_void_p, fp, C.c_int32, dp, fp, C.c_void_p], C.c_int),
-        "ep_mlp_adam_step": ([H, C.c_float, C.c_float, C.c_float, C.c_float], C.c_int),
-        "ep_set_surrogate": ([H, C.POINTER(SurrogateDesc)], C.c_int),
-        "ep_surrogate_forward": ([C.POINTER(SurrogateDesc), C.c_int32, fp, fp], C.c_int),
-    }
-    for name, (args, res) in sig.items():
-        f = getattr(L, name)
-        f.argtypes = args
-        f.restype = res
-
-
-_lib_plain = lib
-
-
-def lib():  # noqa: F811  (extends the binding with the learned-step entry points)
-    L = _lib_plain()
-    if not getattr(L, "_learned_bound", False):
-        _bind_learned(L)
-        L._learned_bound = True
-    return L

@@ -6,6 +6,7 @@
 #include <vector>
 #include <string>
 #include <memory>
+#include <algorithm>
 
 #include "kernels.cuh"
 #include "host_fem.h"
@@ -89,6 +90,17 @@ struct ep_handle {
     // learned ionic step (EP_SURROGATE)
     DBuf sg_wimg, sg_aux, sg_list, sg_count, sg_err;
     int has_surrogate = 0;
+    // independent instances sharing the launches (ep_batch_create)
+    int ninst = 1;
+    std::vector<int> inst_row;           // ninst + 1 node offsets
+    std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
+    DBuf d_inst_row, d_inst_blk;
+    // launch shape (ep_set_launch_config / ep_autotune)
+    int cg_per_sm = 0, ionic_block = 128, graph_steps = 0;
+    cudaGraphExec_t gexec = nullptr;
+    int g_steps = 0;                     // steps in the instantiated graph
+    long long g_launches = 0;            // kernel launches per graph replay
+    DBuf ecg_slot;                       // next ECG sample slot (device counter)
 };
 
 namespace {
@@ -183,11 +195,14 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.iters_max = (unsigned int *)(st + 1);
     a.fails = (unsigned int *)(st + 1) + 1;
     a.last = h->cg_last.as<double>();
+    a.ninst = h->ninst;
+    a.inst_row = h->d_inst_row.as<int>();
+    a.inst_blk = h->d_inst_blk.as<int>();
 }
 
 template <typename R>
 int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &states_nm,
-                 const std::vector<double> &consts, const ep_model_desc *md) {
+                 const std::vector<double> &consts, const std::vector<double> &gks) {
     const int n = h->n;
     int rc;
     // operators
@@ -226,20 +241,85 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
     if ((rc = upload<R>(h->V, V))) return rc;
     if ((rc = upload<R>(h->S, S))) return rc;
     if ((rc = upload<R>(h->consts, consts))) return rc;
-    if (md->node_gks_scale) {
-        std::vector<double> g(md->node_gks_scale, md->node_gks_scale + n);
-        if ((rc = upload<R>(h->gks, g))) return rc;
+    if (!gks.empty()) {
+        if ((rc = upload<R>(h->gks, gks))) return rc;
     }
     if (h->model == EP_LUORUDYWITHGATE) {
         std::vector<double> tab;
         lr_gate_table(tab);
         if ((rc = upload<R>(h->lr_table, tab))) return rc;
     }
-    rc = cg_grid_size<R>(h->cg_block, &h->cg_grid);
-    return rc;
+    return EP_OK;
 }
 
 }  // namespace
+
+// CTA groups of the persistent CG launch: every instance gets at least one
+// CTA, the rest in proportion to its SELL slices (largest remainder).
+// Returns -1 if there are more instances than CTAs.
+extern "C" int ep_batch_plan(int32_t ninst, const int32_t *inst_row, int32_t grid, int32_t *inst_blk) {
+    if (ninst <= 0 || !inst_row || !inst_blk || grid < ninst) return EP_ERR_ARG;
+    std::vector<long long> sl(ninst);
+    long long tot = 0;
+    for (int k = 0; k < ninst; k++) {
+        if (inst_row[k + 1] < inst_row[k]) return EP_ERR_ARG;
+        sl[k] = (inst_row[k + 1] + kSlice - 1) / kSlice - inst_row[k] / kSlice;
+        tot += sl[k];
+    }
+    const int spare = grid - ninst;
+    std::vector<int> cnt(ninst, 1);
+    std::vector<std::pair<double, int>> rem(ninst);
+    int used = 0;
+    for (int k = 0; k < ninst; k++) {
+        const double share = tot > 0 ? (double)spare * (double)sl[k] / (double)tot : 0.0;
+        const int whole = (int)share;
+        cnt[k] += whole;
+        used += whole;
+        rem[k] = {share - whole, k};
+    }
+    std::stable_sort(rem.begin(), rem.end(), [](const std::pair<double, int> &x, const std::pair<double, int> &y) {
+        return x.first > y.first;
+    });
+    for (int k = 0; used < spare; k = (k + 1) % ninst, used++) cnt[rem[k].second]++;
+    inst_blk[0] = 0;
+    for (int k = 0; k < ninst; k++) inst_blk[k + 1] = inst_blk[k] + cnt[k];
+    return EP_OK;
+}
+
+// (re)size the CG launch for the handle's launch shape: grid, CTA groups,
+// partials, barriers and per-instance results
+static int plan_cg(ep_handle *h) {
+    int rc = h->precision == EP_FP64 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm)
+                                     : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm);
+    if (rc) return rc;
+    if (h->ninst > h->cg_grid) {
+        set_error("%d instances but only %d CTAs in the persistent launch", h->ninst, h->cg_grid);
+        return EP_ERR_ARG;
+    }
+    h->inst_blk.assign(h->ninst + 1, 0);
+    if ((rc = ep_batch_plan(h->ninst, h->inst_row.data(), h->cg_grid, h->inst_blk.data()))) {
+        set_error("bad instance layout");
+        return rc;
+    }
+    if ((rc = upload_raw(h->d_inst_row, h->inst_row.data(), h->inst_row.size()))) return rc;
+    if ((rc = upload_raw(h->d_inst_blk, h->inst_blk.data(), h->inst_blk.size()))) return rc;
+    if ((rc = h->partial.alloc(sizeof(double) * 4 * (size_t)h->cg_grid))) return rc;
+    if (h->bar.bytes != sizeof(GridBarrier) * (size_t)h->ninst) {
+        if ((rc = h->bar.alloc(sizeof(GridBarrier) * (size_t)h->ninst))) return rc;
+        EP_CUDA(cudaMemset(h->bar.p, 0, sizeof(GridBarrier) * (size_t)h->ninst));
+    }
+    if (h->cg_last.bytes != 2 * sizeof(double) * (size_t)h->ninst) {
+        if ((rc = h->cg_last.alloc(2 * sizeof(double) * (size_t)h->ninst))) return rc;
+        EP_CUDA(cudaMemset(h->cg_last.p, 0, 2 * sizeof(double) * (size_t)h->ninst));
+    }
+    return EP_OK;
+}
+
+static void drop_graph(ep_handle *h) {
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+    h->g_steps = 0;
+}
 
 static int ensure_ecg_cap(ep_handle *h, int need) {
     if (need <= h->ecg_cap) return EP_OK;
@@ -254,6 +334,7 @@ static int ensure_ecg_cap(ep_handle *h, int need) {
     std::swap(h->ecg_buf.p, nb.p);
     std::swap(h->ecg_buf.bytes, nb.bytes);
     h->ecg_cap = cap;
+    drop_graph(h);
     return EP_OK;
 }
 
@@ -265,6 +346,8 @@ static void fill_surrogate_args(ep_handle *h, const IonicArgs<float> &ia, Surrog
     sa.stim_head = ia.stim_head; sa.stim_next = ia.stim_next;
     sa.stim_on = ia.stim_on; sa.stim_off = ia.stim_off; sa.stim_amp = ia.stim_amp;
     sa.step_ptr = ia.step_ptr; sa.t_per_step = h->dt;
+    sa.nsub = ia.nsub;
+    for (int k = 0; k < ia.nsub; k++) sa.sub_dt[k] = ia.sub_dt[k];
     sa.Cm = ia.Cm; sa.Xi = ia.Xi; sa.act_thr = ia.act_thr;
     sa.track = ia.track;
     sa.wimg = h->sg_wimg.as<unsigned short>();
@@ -290,7 +373,7 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
-    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream);
+    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block);
 }
 
 enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
@@ -325,11 +408,11 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if (h->precision == EP_SURROGATE) {
                 if ((rc = launch_learned_phase(h, ia))) return rc;
                 h->launches += 2;
-            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream))) {
+            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block))) {
                 return rc;
             }
         } else {
-            if ((rc = launch_ionic<R>(h->model, ia, h->stream))) return rc;
+            if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
         if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
@@ -340,8 +423,8 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
         if (h->ecg_every && h->ne > 0 && h->step % h->ecg_every == 0) {
             if ((rc = mark(h, ne, K_ECG))) return rc;
             rc = launch_ecg<R>(h->n, h->ne, h->W.as<R>(), h->pitch, h->V.as<R>(), h->ecg_partial.as<double>(),
-                               h->ecg_counter.as<unsigned int>(),
-                               h->ecg_buf.as<double>() + (size_t)h->ecg_count * h->ne, h->ecg_grid, h->stream);
+                               h->ecg_counter.as<unsigned int>(), h->ecg_buf.as<double>(), h->ecg_grid, h->stream,
+                               h->ecg_slot.as<unsigned int>(), h->ecg_cap);
             if (rc) return rc;
             h->launches += 1;
             h->ecg_count++;
@@ -349,6 +432,64 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
         }
     }
     return mark(h, ne, K_OTHER);
+}
+
+// Steps replayed from one instantiated CUDA graph of g_steps steps.  The
+// graph is captured from the same launch sequence as the direct path; it is
+// only valid while every buffer it names stays in place, so the entry points
+// that reallocate drop it.  A graph that contains ECG samples is captured and
+// replayed only at step counts that are multiples of ecg_every.
+template <typename R>
+static int step_graph(ep_handle *h, int &nsteps) {
+    int k = h->graph_steps;
+    const bool ecg = h->ecg_every && h->ne > 0;
+    if (ecg) k = div_up(k, h->ecg_every) * h->ecg_every;
+    if (ecg && h->step % h->ecg_every != 0) return EP_OK;     // not aligned: direct steps
+    if (nsteps < k) return EP_OK;
+    if (!h->gexec || h->g_steps != k) {
+        drop_graph(h);
+        const long long step0 = h->step, launches0 = h->launches;
+        const int ecg_count0 = h->ecg_count;
+        const size_t ecg_t0 = h->ecg_t.size();
+        size_t ne = 0;
+        EP_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+        int rc = step_typed<R>(h, k, ne);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+        h->step = step0;
+        h->ecg_count = ecg_count0;
+        h->ecg_t.resize(ecg_t0);
+        h->g_launches = h->launches - launches0;
+        h->launches = launches0;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            set_error("CUDA graph capture failed: %s", cudaGetErrorString(ce));
+            return EP_ERR_CUDA;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            cudaGetLastError();
+            h->gexec = nullptr;
+            set_error("CUDA graph instantiation failed: %s", cudaGetErrorString(ie));
+            return EP_ERR_CUDA;
+        }
+        h->g_steps = k;
+    }
+    while (nsteps >= k) {
+        EP_CUDA(cudaGraphLaunch(h->gexec, h->stream));
+        for (int s = 0; s < k; s++) {
+            h->step++;
+            if (ecg && h->step % h->ecg_every == 0) {
+                h->ecg_count++;
+                h->ecg_t.push_back((double)h->step * h->dt);
+            }
+        }
+        h->launches += h->g_launches;
+        nsteps -= k;
+    }
+    return EP_OK;
 }
 
 
@@ -393,6 +534,7 @@ void ep_destroy(ep_handle *h) {
     cudaGetDevice(&cur);
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graph(h);
     for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -401,24 +543,47 @@ void ep_destroy(ep_handle *h) {
     cudaSetDevice(cur);
 }
 
-int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver_desc *sd,
-              int device, ep_handle **out) {
-    EP_CHECK_ARG(mesh && md && sd && out, "null descriptor");
+}  // extern "C"
+
+// One handle over ninst independent meshes (ninst = 1: ep_create).  The
+// instances are concatenated node-wise into one block-diagonal operator;
+// their parameter sets are concatenated into one type table.
+static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_desc *models,
+                        const ep_solver_desc *sd, int device, ep_handle **out) {
+    EP_CHECK_ARG(meshes && models && sd && out, "null descriptor");
     *out = nullptr;
-    EP_CHECK_ARG(mesh->n_nodes > 0 && mesh->n_tets > 0 && mesh->xyz && mesh->tets, "empty mesh");
+    EP_CHECK_ARG(ninst >= 1, "no instances");
+    const ep_model_desc *md = &models[0];
     const int nst = ep_model_nstate(md->model);
     EP_CHECK_ARG(nst > 0, "unknown cell model");
     EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32 ||
                      (sd->precision == EP_SURROGATE && md->model == EP_TUSSCHER),
                  "unsupported precision (EP_SURROGATE needs the ten Tusscher model)");
     EP_CHECK_ARG(sd->dt > 0 && sd->ionic_dt > 0, "dt and ionic_dt must be positive");
-    const int ntypes = md->n_types > 0 ? md->n_types : 1;
+    long long ntot = 0, mtot = 0;
+    int ntypes = 0;
+    bool any_type = false, any_gks = false, all_fib = true;
+    for (int k = 0; k < ninst; k++) {
+        const ep_mesh_desc *mesh = &meshes[k];
+        EP_CHECK_ARG(mesh->n_nodes > 0 && mesh->n_tets > 0 && mesh->xyz && mesh->tets, "empty mesh");
+        EP_CHECK_ARG(models[k].model == md->model, "all instances must use the same cell model");
+        EP_CHECK_ARG((mesh->Cm > 0 ? mesh->Cm : 1.0) == (meshes[0].Cm > 0 ? meshes[0].Cm : 1.0),
+                     "all instances must have the same C_m");
+        ntot += mesh->n_nodes;
+        mtot += mesh->n_tets;
+        ntypes += models[k].n_types > 0 ? models[k].n_types : 1;
+        any_type |= models[k].node_type != nullptr;
+        any_gks |= models[k].node_gks_scale != nullptr;
+        all_fib &= mesh->fibers != nullptr;
+    }
+    EP_CHECK_ARG(ntot < (1ll << 31) - 64 && 4 * mtot < (1ll << 31), "mesh too large");
     EP_CHECK_ARG(ntypes <= kMaxTypes, "too many parameter sets");
     std::unique_ptr<ep_handle> h(new ep_handle());
     h->device = device;
     EP_CUDA(cudaSetDevice(device));
-    const int n = mesh->n_nodes, m = mesh->n_tets;
+    const int n = (int)ntot;
     h->n = n;
+    h->ninst = ninst;
     h->pitch = (n + 31) / 32 * 32;
     h->model = md->model;
     h->precision = sd->precision;
@@ -429,7 +594,7 @@ int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver
     h->dt = sd->dt; h->ionic_dt = sd->ionic_dt;
     h->nsub = substeps(sd->dt, sd->ionic_dt, h->sub_dt);
     EP_CHECK_ARG(h->nsub > 0, "more than 64 ionic sub-steps per step");
-    h->Cm = mesh->Cm > 0 ? mesh->Cm : 1.0;
+    h->Cm = meshes[0].Cm > 0 ? meshes[0].Cm : 1.0;
     h->cg_tol = sd->cg_tol > 0 ? sd->cg_tol : 1e-7;
     h->cg_maxit = sd->cg_maxit > 0 ? sd->cg_maxit : 1000;
     h->ecg_every = sd->ecg_every > 0 ? sd->ecg_every : 0;
@@ -440,37 +605,68 @@ int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver
     h->tt.fp32_scaled_tol = sd->precision == EP_FP64 ? 0 : 1;
     h->tt.newton_tol = sd->newton_tol > 0 ? sd->newton_tol : 1e-6;
     h->mh_abs = md->mh_abs_mode ? 1 : 0;
-    for (int k = 0; k < 3; k++) h->D[k] = mesh->D[k];
-    // mesh (zero-based)
-    h->xyz.assign(mesh->xyz, mesh->xyz + 3 * (size_t)n);
-    h->tets.resize((size_t)m * 4);
-    for (size_t k = 0; k < (size_t)m * 4; k++) {
-        const int v = mesh->tets[k] - (mesh->one_based ? 1 : 0);
-        EP_CHECK_ARG(v >= 0 && v < n, "tet node id out of range");
-        h->tets[k] = v;
-    }
-    if (mesh->fibers) h->fibers.assign(mesh->fibers, mesh->fibers + 9 * (size_t)m);
-    // FEM operators in FP64
-    HostCSR csr;
-    if (assemble_cn(n, h->xyz.data(), m, h->tets.data(), mesh->fibers ? h->fibers.data() : nullptr,
-                    mesh->D, h->Cm, h->dt, sd->smoothing_alpha, csr) != 0) {
-        set_error("mesh has an element with non-positive volume");
-        return EP_ERR_MESH;
-    }
-    // parameter sets
+    for (int k = 0; k < 3; k++) h->D[k] = meshes[0].D[k];
     const int nc = ep_model_nconst(md->model);
     std::vector<double> consts((size_t)ntypes * nc);
-    for (int t = 0; t < ntypes; t++) {
-        if (md->type_consts) std::memcpy(&consts[(size_t)t * nc], md->type_consts + (size_t)t * nc, sizeof(double) * nc);
-        else default_consts(md->model, t, &consts[(size_t)t * nc]);
-    }
-    // initial states, node-major like InterVariables
     std::vector<double> st((size_t)n * nst);
-    for (int i = 0; i < n; i++) {
-        const int t = md->node_type ? md->node_type[i] : 0;
-        if (md->node_type) EP_CHECK_ARG(t < ntypes, "node type beyond n_types");
-        if (md->initial_states) std::memcpy(&st[(size_t)i * nst], md->initial_states + (size_t)i * nst, sizeof(double) * nst);
-        else default_state(md->model, t, &st[(size_t)i * nst]);
+    std::vector<uint8_t> node_type(any_type || ninst > 1 ? n : 0, 0);
+    std::vector<double> gks(any_gks ? n : 0, 1.0);
+    h->xyz.resize(3 * (size_t)n);
+    h->tets.resize(4 * (size_t)mtot);
+    if (all_fib) h->fibers.resize(9 * (size_t)mtot);
+    h->inst_row.assign(ninst + 1, 0);
+    HostCSR csr;
+    csr.n = n;
+    csr.rowptr.assign(1, 0);
+    int noff = 0, toff = 0;
+    long long eoff = 0;
+    for (int k = 0; k < ninst; k++) {
+        const ep_mesh_desc *mesh = &meshes[k];
+        const ep_model_desc *mk = &models[k];
+        const int ni = mesh->n_nodes, mi = mesh->n_tets;
+        const int nti = mk->n_types > 0 ? mk->n_types : 1;
+        std::vector<int> tl((size_t)mi * 4);
+        for (size_t e = 0; e < (size_t)mi * 4; e++) {
+            const int v = mesh->tets[e] - (mesh->one_based ? 1 : 0);
+            EP_CHECK_ARG(v >= 0 && v < ni, "tet node id out of range");
+            tl[e] = v;
+            h->tets[(size_t)eoff * 4 + e] = v + noff;
+        }
+        std::memcpy(&h->xyz[3 * (size_t)noff], mesh->xyz, sizeof(double) * 3 * ni);
+        if (all_fib) std::memcpy(&h->fibers[9 * (size_t)eoff], mesh->fibers, sizeof(double) * 9 * mi);
+        // FEM operators of this instance in FP64, appended block-diagonally
+        HostCSR ci;
+        if (assemble_cn(ni, mesh->xyz, mi, tl.data(), mesh->fibers, mesh->D, h->Cm, h->dt,
+                        sd->smoothing_alpha, ci) != 0) {
+            set_error("mesh %d has an element with non-positive volume", k);
+            return EP_ERR_MESH;
+        }
+        const int base = csr.rowptr.back();
+        for (int i = 0; i < ni; i++) csr.rowptr.push_back(base + ci.rowptr[i + 1]);
+        for (int c : ci.col) csr.col.push_back(c + noff);
+        csr.A.insert(csr.A.end(), ci.A.begin(), ci.A.end());
+        csr.B.insert(csr.B.end(), ci.B.begin(), ci.B.end());
+        csr.CL.insert(csr.CL.end(), ci.CL.begin(), ci.CL.end());
+        // parameter sets
+        for (int t = 0; t < nti; t++) {
+            double *dst = &consts[(size_t)(toff + t) * nc];
+            if (mk->type_consts) std::memcpy(dst, mk->type_consts + (size_t)t * nc, sizeof(double) * nc);
+            else default_consts(md->model, t, dst);
+        }
+        // initial states, node-major like InterVariables
+        for (int i = 0; i < ni; i++) {
+            const int t = mk->node_type ? mk->node_type[i] : 0;
+            if (mk->node_type) EP_CHECK_ARG(t < nti, "node type beyond n_types");
+            double *dst = &st[(size_t)(noff + i) * nst];
+            if (mk->initial_states) std::memcpy(dst, mk->initial_states + (size_t)i * nst, sizeof(double) * nst);
+            else default_state(md->model, t, dst);
+            if (!node_type.empty()) node_type[noff + i] = (uint8_t)(toff + t);
+            if (mk->node_gks_scale) gks[noff + i] = mk->node_gks_scale[i];
+        }
+        noff += ni;
+        toff += nti;
+        eoff += mi;
+        h->inst_row[k + 1] = noff;
     }
     h->model_V0.assign(n, 0.0);
     if (is_mh(md->model))
@@ -479,27 +675,62 @@ int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver
     EP_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     EP_CUDA(cudaEventCreate(&h->ev0));
     EP_CUDA(cudaEventCreate(&h->ev1));
-    if (md->node_type) {
-        if ((rc = upload_raw(h->type, md->node_type, (size_t)n))) return rc;
+    if (!node_type.empty()) {
+        if ((rc = upload_raw(h->type, node_type.data(), node_type.size()))) return rc;
     }
-    if (h->precision == EP_FP64) rc = create_typed<double>(h.get(), csr, st, consts, md);
-    else rc = create_typed<float>(h.get(), csr, st, consts, md);
+    if (h->precision == EP_FP64) rc = create_typed<double>(h.get(), csr, st, consts, gks);
+    else rc = create_typed<float>(h.get(), csr, st, consts, gks);
     if (rc) return rc;
     // solver scratch and status
-    if ((rc = h->partial.alloc(sizeof(double) * 4 * (size_t)h->cg_grid))) return rc;
-    if ((rc = h->bar.alloc(sizeof(GridBarrier)))) return rc;
+    if ((rc = plan_cg(h.get()))) return rc;
     if ((rc = h->status.alloc(sizeof(DevStatus)))) return rc;
     if ((rc = h->cg_stats.alloc(32))) return rc;
-    if ((rc = h->cg_last.alloc(2 * sizeof(double)))) return rc;
     if ((rc = h->d_step.alloc(sizeof(long long)))) return rc;
-    EP_CUDA(cudaMemset(h->bar.p, 0, sizeof(GridBarrier)));
+    if ((rc = h->ecg_slot.alloc(sizeof(unsigned int)))) return rc;
     EP_CUDA(cudaMemset(h->status.p, 0, sizeof(DevStatus)));
     EP_CUDA(cudaMemset(h->cg_stats.p, 0, 32));
     EP_CUDA(cudaMemset(h->d_step.p, 0, sizeof(long long)));
+    EP_CUDA(cudaMemset(h->ecg_slot.p, 0, sizeof(unsigned int)));
     std::vector<Track> tr(n, Track{-1.f, -1.f, -1.f, 1e30f});
     if ((rc = upload_raw(h->track, tr.data(), tr.size()))) return rc;
     EP_CUDA(cudaDeviceSynchronize());
     *out = h.release();
+    return EP_OK;
+}
+
+extern "C" {
+
+int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver_desc *sd,
+              int device, ep_handle **out) {
+    return create_multi(1, mesh, md, sd, device, out);
+}
+
+int ep_batch_create(int32_t n_inst, const ep_mesh_desc *meshes, const ep_model_desc *models,
+                    const ep_solver_desc *sd, int device, ep_handle **out) {
+    return create_multi(n_inst, meshes, models, sd, device, out);
+}
+
+int ep_batch_layout(const ep_handle *h, int32_t *n_inst, int32_t *node_offset, int32_t *cta_offset) {
+    EP_CHECK_ARG(h, "null handle");
+    if (n_inst) *n_inst = h->ninst;
+    for (int k = 0; k <= h->ninst; k++) {
+        if (node_offset) node_offset[k] = h->inst_row[k];
+        if (cta_offset) cta_offset[k] = h->inst_blk[k];
+    }
+    return EP_OK;
+}
+
+int ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CUDA(cudaSetDevice(h->device));
+    std::vector<double> last(2 * (size_t)h->ninst);
+    EP_CUDA(cudaMemcpyAsync(last.data(), h->cg_last.p, sizeof(double) * last.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < h->ninst; k++) {
+        if (iters) iters[k] = (int32_t)last[2 * k];
+        if (relres) relres[k] = last[2 * k + 1];
+    }
     return EP_OK;
 }
 
@@ -572,6 +803,7 @@ int ep_set_stimulus(ep_handle *h, int32_t n, const int32_t *ids, const double *t
     EP_CHECK_ARG(n >= 0 && (n == 0 || (ids && t_on && t_off && amp)), "bad stimulus table");
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
     std::vector<int> head(h->n, -1), next(n, -1);
     std::vector<long long> on(n), off(n);
     std::vector<double> a(n);
@@ -596,8 +828,13 @@ int ep_set_stimulus(ep_handle *h, int32_t n, const int32_t *ids, const double *t
 int ep_set_electrodes(ep_handle *h, int32_t ne, const double *xyz, const double *D_ecg) {
     EP_CHECK_ARG(h, "null handle");
     EP_CHECK_ARG(ne >= 0 && ne <= 16 && (ne == 0 || xyz), "1..16 electrodes");
+    if (h->ninst > 1) {
+        set_error("pseudo-ECG electrodes are per mesh; not available on a batch handle");
+        return EP_ERR_UNSUPPORTED;
+    }
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
     const double *D = D_ecg ? D_ecg : h->D;
     std::vector<double> W;
     ecg_weights(h->n, h->xyz.data(), (int)(h->tets.size() / 4), h->tets.data(),
@@ -616,6 +853,7 @@ int ep_set_electrodes(ep_handle *h, int32_t ne, const double *xyz, const double 
     if ((rc = h->ecg_partial.alloc(sizeof(double) * 16 * (size_t)h->ecg_grid))) return rc;
     if ((rc = h->ecg_counter.alloc(sizeof(unsigned int)))) return rc;
     EP_CUDA(cudaMemset(h->ecg_counter.p, 0, sizeof(unsigned int)));
+    EP_CUDA(cudaMemset(h->ecg_slot.p, 0, sizeof(unsigned int)));
     h->ecg_cap = 0; h->ecg_count = 0; h->ecg_t.clear();
     h->ecg_buf.alloc(0);
     return EP_OK;
@@ -633,7 +871,21 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
     EP_CUDA(cudaEventRecord(h->ev0, h->stream));
     size_t ne = 0;
     h->launches = 0;
-    int rc = h->precision == EP_FP64 ? step_typed<double>(h, nsteps, ne) : step_typed<float>(h, nsteps, ne);
+    int rc = EP_OK;
+    int left = nsteps;
+    if (h->graph_steps > 0 && !h->profile) {
+        // direct steps up to the ECG sampling phase, then whole graphs
+        if (h->ecg_every && h->ne > 0) {
+            const int lead = (int)((h->ecg_every - h->step % h->ecg_every) % h->ecg_every);
+            const int d = std::min(lead, left);
+            rc = h->precision == EP_FP64 ? step_typed<double>(h, d, ne) : step_typed<float>(h, d, ne);
+            if (rc) return rc;
+            left -= d;
+        }
+        rc = h->precision == EP_FP64 ? step_graph<double>(h, left) : step_graph<float>(h, left);
+        if (rc) return rc;
+    }
+    rc = h->precision == EP_FP64 ? step_typed<double>(h, left, ne) : step_typed<float>(h, left, ne);
     if (rc) return rc;
     EP_CUDA(cudaEventRecord(h->ev1, h->stream));
     EP_CUDA(cudaEventSynchronize(h->ev1));
@@ -648,7 +900,12 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
     GridBarrier bar;
     EP_CUDA(cudaMemcpy(&st, h->status.p, sizeof st, cudaMemcpyDeviceToHost));
     EP_CUDA(cudaMemcpy(cgs, h->cg_stats.p, 32, cudaMemcpyDeviceToHost));
-    EP_CUDA(cudaMemcpy(&bar, h->bar.p, sizeof bar, cudaMemcpyDeviceToHost));
+    {
+        std::vector<GridBarrier> bars(h->ninst);
+        EP_CUDA(cudaMemcpy(bars.data(), h->bar.p, sizeof(GridBarrier) * bars.size(), cudaMemcpyDeviceToHost));
+        bar = bars[0];
+        for (const GridBarrier &b : bars) bar.err |= b.err;
+    }
     float ms = 0.f;
     EP_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     if (stats) {
@@ -749,10 +1006,12 @@ static int pack_surrogate(const ep_surrogate_desc *d, std::vector<unsigned short
     for (int j = 0; j < SG_NOUT; j++) {
         aux.out_mean[j] = j < SG_NY ? d->out_mean[j] : 0.f;
         aux.out_std[j] = j < SG_NY ? d->out_std[j] : 0.f;
+        aux.out_scale[j] = (j < SG_NY && d->out_scale) ? d->out_scale[j] : 0.f;
+        EP_CHECK_ARG(aux.out_scale[j] >= 0.f, "out_scale must be >= 0");
     }
     aux.nah_max = d->nah_max;
     aux.log_mask = d->log_mask & ((1u << SG_NF) - 1u) & ~1u;   // V stays linear
-    EP_CHECK_ARG(d->v_update == 0 || d->v_update == 1, "v_update must be 0 or 1");
+    EP_CHECK_ARG(d->v_update >= 0 && d->v_update <= 2, "v_update must be 0, 1 or 2");
     aux.v_update = d->v_update;
     return EP_OK;
 }
@@ -761,6 +1020,7 @@ int ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d) {
     EP_CHECK_ARG(h, "null handle");
     EP_CHECK_ARG(h->precision == EP_SURROGATE, "the handle was not created with EP_SURROGATE");
     EP_CUDA(cudaSetDevice(h->device));
+    drop_graph(h);
     std::vector<unsigned short> img;
     SurrogateAux aux;
     int rc = pack_surrogate(d, img, aux);
@@ -813,6 +1073,155 @@ int ep_set_profiling(ep_handle *h, int on) {
     EP_CHECK_ARG(h, "null handle");
     h->profile = on ? 1 : 0;
     return EP_OK;
+}
+
+int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
+    EP_CHECK_ARG(h && cfg, "null argument");
+    cfg->cg_block = h->cg_block;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cfg->cg_per_sm = h->cg_grid / std::max(1, nsm);
+    cfg->ionic_block = h->ionic_block;
+    cfg->graph_steps = h->graph_steps;
+    return EP_OK;
+}
+
+int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
+    EP_CHECK_ARG(h && cfg, "null argument");
+    EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256, "cg_block must be 128 or 256");
+    EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
+    EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
+    EP_CHECK_ARG(cfg->graph_steps >= 0 && cfg->graph_steps <= 100000, "graph_steps out of range");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    const int ob = h->cg_block, op = h->cg_per_sm;
+    h->cg_block = cfg->cg_block;
+    h->cg_per_sm = cfg->cg_per_sm;
+    int rc = plan_cg(h);
+    if (rc) {
+        h->cg_block = ob; h->cg_per_sm = op;
+        plan_cg(h);
+        return rc;
+    }
+    h->ionic_block = cfg->ionic_block;
+    h->graph_steps = cfg->graph_steps;
+    return EP_OK;
+}
+
+namespace {
+// device state that stepping changes, saved and put back around tuning trials
+struct Snapshot {
+    DBuf V, S, track, d_step, slot;
+    long long step = 0;
+    int ecg_count = 0;
+    std::vector<double> ecg_t;
+};
+
+int snap_copy(DBuf &dst, const DBuf &src, cudaStream_t s, bool to_snapshot) {
+    if (!src.p) return EP_OK;
+    if (to_snapshot) {
+        int rc = dst.alloc(src.bytes);
+        if (rc) return rc;
+        EP_CUDA(cudaMemcpyAsync(dst.p, src.p, src.bytes, cudaMemcpyDeviceToDevice, s));
+    } else {
+        EP_CUDA(cudaMemcpyAsync((void *)src.p, dst.p, src.bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    return EP_OK;
+}
+
+int snapshot(ep_handle *h, Snapshot &sn, bool save) {
+    int rc;
+    if ((rc = snap_copy(sn.V, h->V, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.S, h->S, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.track, h->track, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.d_step, h->d_step, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.slot, h->ecg_slot, h->stream, save))) return rc;
+    if (save) {
+        sn.step = h->step; sn.ecg_count = h->ecg_count; sn.ecg_t = h->ecg_t;
+    } else {
+        h->step = sn.step; h->ecg_count = sn.ecg_count; h->ecg_t = sn.ecg_t;
+    }
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    return EP_OK;
+}
+}  // namespace
+
+int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, double *best_ms,
+                double *start_ms, int32_t *n_tried) {
+    EP_CHECK_ARG(h && trial_steps > 0, "bad arguments");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    Snapshot sn;
+    int rc = snapshot(h, sn, true);
+    if (rc) return rc;
+    const int prof = h->profile;
+    h->profile = 0;
+    int dev = 0, nsm = 148;
+    EP_CUDA(cudaGetDevice(&dev));
+    EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    ep_launch_config cur;
+    cur.cg_block = h->cg_block;
+    cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
+    cur.ionic_block = h->ionic_block;
+    cur.graph_steps = h->graph_steps;
+    int tried = 0;
+    // ms per step of one configuration (negative: it could not run)
+    auto trial = [&](const ep_launch_config &c) -> double {
+        if (ep_set_launch_config(h, &c) != EP_OK) return -1.0;
+        ep_step_stats st;
+        for (int pass = 0; pass < 2; pass++) {      // the first pass warms up (and captures)
+            if (snapshot(h, sn, false) != EP_OK) return -1.0;
+            if (ep_step(h, trial_steps, &st) != EP_OK) return -1.0;
+        }
+        tried++;
+        return st.device_ms / trial_steps;
+    };
+    double t_best = trial(cur);
+    const double t_start = t_best;
+    ep_launch_config b = cur;
+    if (t_best < 0) {
+        h->profile = prof;
+        snapshot(h, sn, false);
+        return EP_ERR_CUDA;
+    }
+    // coordinate descent: CG shape, then ionic block, then graphs
+    for (int blk : {128, 256}) {
+        int maxper = 1;
+        if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper) : cg_max_per_sm<float>(blk, &maxper)))
+            continue;
+        for (int per = 1; per <= std::min(maxper, 8); per++) {
+            ep_launch_config c = b;
+            c.cg_block = blk; c.cg_per_sm = per;
+            if (c.cg_block == b.cg_block && c.cg_per_sm == b.cg_per_sm) continue;
+            if (per * nsm < h->ninst) continue;
+            const double t = trial(c);
+            if (t >= 0 && t < t_best) { t_best = t; b = c; }
+        }
+    }
+    for (int ib : {64, 128}) {
+        if (ib == b.ionic_block) continue;
+        ep_launch_config c = b;
+        c.ionic_block = ib;
+        const double t = trial(c);
+        if (t >= 0 && t < t_best) { t_best = t; b = c; }
+    }
+    for (int gs : {0, trial_steps}) {
+        if (gs == b.graph_steps) continue;
+        ep_launch_config c = b;
+        c.graph_steps = gs;
+        const double t = trial(c);
+        if (t >= 0 && t < t_best) { t_best = t; b = c; }
+    }
+    rc = ep_set_launch_config(h, &b);
+    h->profile = prof;
+    const int rc2 = snapshot(h, sn, false);
+    if (best) *best = b;
+    if (best_ms) *best_ms = t_best;
+    if (start_ms) *start_ms = t_start;
+    if (n_tried) *n_tried = tried;
+    return rc ? rc : rc2;
 }
 
 int ep_get_time(ep_handle *h, double *t, int64_t *step) {

@@ -53,16 +53,16 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double *out,
     __syncthreads();
 }
 
-// every block sums the grid's partials in the same order
+// every block of a group sums the group's partials in the same order
 template <int NV>
-__device__ __forceinline__ void grid_total(const double *partial, int stride, int nblk, double (&tot)[NV]) {
+__device__ __forceinline__ void grid_total(const double *partial, int stride, int b0, int nblk, double (&tot)[NV]) {
     __shared__ double sh[NV];
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             double t = 0.0;
-            for (int b = lane; b < nblk; b += 32) t += __ldcg(partial + k * stride + b);
+            for (int b = lane; b < nblk; b += 32) t += __ldcg(partial + k * stride + b0 + b);
             for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
             if (lane == 0) sh[k] = t;
         }
@@ -76,15 +76,29 @@ __device__ __forceinline__ void grid_total(const double *partial, int stride, in
 template <typename R>
 __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
     const int lane = threadIdx.x & 31;
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const unsigned int nblk = gridDim.x;
-    const int G = gridDim.x;
+    const int G = gridDim.x;                 // partial-array stride
+    // this CTA's instance: its rows, its CTA group and its barrier
+    int inst = 0, b0 = 0, nb = G, rb = 0, re = a.n;
+    if (a.ninst > 1) {
+        int lo = 0, hi = a.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.inst_blk[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        }
+        inst = lo;
+        b0 = a.inst_blk[inst]; nb = a.inst_blk[inst + 1] - b0;
+        rb = a.inst_row[inst]; re = a.inst_row[inst + 1];
+    }
+    GridBarrier *bar = a.bar + inst;
+    const unsigned int nblk = nb;
+    const int s_lo = rb / kSlice, s_hi = (re + kSlice - 1) / kSlice;
+    const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
+    const int nwarps = (nb * (int)blockDim.x) >> 5;
 
     // ---- prologue: r = B x - A x, z = dinv r, p = 0 ----
     {
         double v[3] = {0.0, 0.0, 0.0};
-        for (int s = gwarp; s < a.nslices; s += nwarps) {
+        for (int s = gwarp; s < s_hi; s += nwarps) {
             const int row = s * kSlice + lane;
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
             R ax = R(0), bx = R(0);
@@ -95,7 +109,7 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
                 ax += __ldg(a.Aval + idx) * xv;
                 bx += __ldg(a.Bval + idx) * xv;
             }
-            if (row < a.n) {
+            if (row >= rb && row < re) {
                 const R r = bx - ax;
                 const R z = __ldg(a.dinv + row) * r;
                 a.r[row] = r;
@@ -107,11 +121,11 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
         }
         block_reduce_store<3>(v, a.partial, G);
     }
-    if (!grid_sync(a.bar, nblk)) return;
+    if (!grid_sync(bar, nblk)) return;
     double rz, rr0, bb;
     {
         double t[3];
-        grid_total<3>(a.partial, G, G, t);
+        grid_total<3>(a.partial, G, b0, nb, t);
         rz = t[0]; rr0 = t[1]; bb = t[2];
     }
     // ||r|| <= tol ||r0||, or the residual is at the resolution of b in the
@@ -129,7 +143,7 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
         {
             double v[1] = {0.0};
             const R bR = (R)beta;
-            for (int s = gwarp; s < a.nslices; s += nwarps) {
+            for (int s = gwarp; s < s_hi; s += nwarps) {
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
                 R q = R(0);
@@ -139,7 +153,7 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
                     const R pj = pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pc + c));
                     q += __ldg(a.Aval + idx) * pj;
                 }
-                if (row < a.n) {
+                if (row >= rb && row < re) {
                     const R pi = pdir(__ldg(a.dinv + row), a.r[row], bR, ldcg(pc + row));
                     pn[row] = pi;
                     a.q[row] = q;
@@ -148,11 +162,11 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
             }
             block_reduce_store<1>(v, a.partial + 3 * G, G);   // disjoint from the neighbours' slots
         }
-        if (!grid_sync(a.bar, nblk)) return;
+        if (!grid_sync(bar, nblk)) return;
         double pq;
         {
             double t[1];
-            grid_total<1>(a.partial + 3 * G, G, G, t);
+            grid_total<1>(a.partial + 3 * G, G, b0, nb, t);
             pq = t[0];
         }
         const double alpha = rz / pq;
@@ -160,9 +174,9 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
         {
             double v[2] = {0.0, 0.0};
             const R aR = (R)alpha;
-            for (int s = gwarp; s < a.nslices; s += nwarps) {
+            for (int s = gwarp; s < s_hi; s += nwarps) {
                 const int row = s * kSlice + lane;
-                if (row < a.n) {
+                if (row >= rb && row < re) {
                     const R pi = pn[row];
                     a.x[row] += aR * pi;
                     const R r = a.r[row] - aR * a.q[row];
@@ -174,9 +188,9 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
             }
             block_reduce_store<2>(v, a.partial, G);
         }
-        if (!grid_sync(a.bar, nblk)) return;
+        if (!grid_sync(bar, nblk)) return;
         double t[2];
-        grid_total<2>(a.partial, G, G, t);
+        grid_total<2>(a.partial, G, b0, nb, t);
         it++;
         rr_last = t[1];
         converged = (t[1] <= stop2);
@@ -184,24 +198,32 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
         rz = t[0];
         R *tmp = pc; pc = pn; pn = tmp;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if ((int)blockIdx.x == b0 && threadIdx.x == 0) {
         atomicAdd(a.iters_total, (unsigned long long)it);
         atomicMax(a.iters_max, (unsigned int)it);
         if (!converged) atomicAdd(a.fails, 1u);
         if (a.last) {
-            a.last[0] = (double)it;
-            a.last[1] = rr0 > 0.0 ? sqrt(rr_last / rr0) : 0.0;
+            a.last[2 * inst] = (double)it;
+            a.last[2 * inst + 1] = rr0 > 0.0 ? sqrt(rr_last / rr0) : 0.0;
         }
     }
 }
 
 template <typename R>
-int cg_grid_size(int block, int *grid) {
+int cg_max_per_sm(int block, int *per) {
+    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R>, block, 0));
+    if (*per < 1) { set_error("CG kernel cannot be resident"); return EP_ERR_CUDA; }
+    return EP_OK;
+}
+
+template <typename R>
+int cg_grid_size(int block, int *grid, int per_sm) {
     int dev = 0, nsm = 0, per = 0;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cn_half<R>, block, 0));
-    if (per < 1) { set_error("CG kernel cannot be resident"); return EP_ERR_CUDA; }
+    int rc = cg_max_per_sm<R>(block, &per);
+    if (rc) return rc;
+    if (per_sm > 0 && per_sm < per) per = per_sm;
     *grid = nsm * per;
     return EP_OK;
 }
@@ -224,8 +246,10 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s) {
 
 template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t);
 template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t);
-template int cg_grid_size<float>(int, int *);
-template int cg_grid_size<double>(int, int *);
+template int cg_grid_size<float>(int, int *, int);
+template int cg_grid_size<double>(int, int *, int);
+template int cg_max_per_sm<float>(int, int *);
+template int cg_max_per_sm<double>(int, int *);
 
 // ---------------------------------------------------------------------------
 // pseudo-ECG: out[k] = sum_i W[k * wpitch + i] V[i], FP64 accumulation.
@@ -233,7 +257,7 @@ template int cg_grid_size<double>(int, int *);
 template <typename R>
 __global__ void __launch_bounds__(256) k_ecg(int n, int ne, const R *__restrict__ W, int wpitch,
                                              const R *__restrict__ V, double *partial,
-                                             unsigned int *counter, double *out) {
+                                             unsigned int *counter, double *out, unsigned int *slot, int cap) {
     constexpr int MAXE = 16;
     double acc[MAXE];
 #pragma unroll
@@ -265,29 +289,36 @@ __global__ void __launch_bounds__(256) k_ecg(int n, int ne, const R *__restrict_
     __syncthreads();
     if (last) {
         __threadfence();
-        if (threadIdx.x < ne) {
+        // with a slot counter the sample goes to row *slot of out (the
+        // counter lives on the device so that replayed graphs advance it)
+        const unsigned int row = slot ? *(volatile unsigned int *)slot : 0u;
+        if (threadIdx.x < ne && (int)row < cap) {
             double t = 0.0;
             for (int b = 0; b < (int)gridDim.x; b++) t += __ldcg(partial + (size_t)threadIdx.x * gridDim.x + b);
-            out[threadIdx.x] = t;
+            out[(size_t)row * ne + threadIdx.x] = t;
         }
-        if (threadIdx.x == 0) *counter = 0;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            if (slot) *slot = row + 1u;
+        }
     }
 }
 
 template <typename R>
 int launch_ecg(int n, int ne, const R *W, int wpitch, const R *V, double *partial,
-               unsigned int *counter, double *out, int grid, cudaStream_t s) {
+               unsigned int *counter, double *out, int grid, cudaStream_t s, unsigned int *slot, int cap) {
     if (ne <= 0) return EP_OK;
     if (ne > 16) { set_error("at most 16 electrodes"); return EP_ERR_ARG; }
-    k_ecg<R><<<grid, 256, 0, s>>>(n, ne, W, wpitch, V, partial, counter, out);
+    k_ecg<R><<<grid, 256, 0, s>>>(n, ne, W, wpitch, V, partial, counter, out, slot, slot ? cap : 1);
     EP_CUDA(cudaGetLastError());
     return EP_OK;
 }
 
 template int launch_ecg<float>(int, int, const float *, int, const float *, double *, unsigned int *,
-                               double *, int, cudaStream_t);
+                               double *, int, cudaStream_t, unsigned int *, int);
 template int launch_ecg<double>(int, int, const double *, int, const double *, double *,
-                                unsigned int *, double *, int, cudaStream_t);
+                                unsigned int *, double *, int, cudaStream_t, unsigned int *, int);
 
 __global__ void k_step_inc(long long *step) { *step += 1; }
 void launch_step_inc(long long *step, cudaStream_t s) { k_step_inc<<<1, 1, 0, s>>>(step); }

@@ -32,7 +32,7 @@ const char *last_error();
         if (!(cond)) { ::ep::set_error("%s", msg); return EP_ERR_ARG; }        \
     } while (0)
 
-constexpr int kMaxTypes = 16;      // parameter sets per handle
+constexpr int kMaxTypes = 256;     // parameter sets per handle (uint8 node types)
 constexpr int kMaxSub = 64;        // ionic sub-steps per global step
 constexpr int kSlice = 32;         // SELL slice height (one warp)
 

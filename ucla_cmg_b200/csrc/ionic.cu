@@ -133,8 +133,8 @@ __global__ void __launch_bounds__(128) k_ionic(const IonicArgs<R> a) {
 }
 
 template <typename R>
-int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st) {
-    const int block = 128;
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block) {
+    if (block != 64 && block != 128) { set_error("ionic block must be 64 or 128"); return EP_ERR_ARG; }
     int grid = div_up(a.n, block);
     if (a.n == 0) return EP_OK;
     if (a.node_list) {
@@ -164,7 +164,7 @@ int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st) {
     return EP_OK;
 }
 
-template int launch_ionic<float>(int, const IonicArgs<float> &, cudaStream_t);
-template int launch_ionic<double>(int, const IonicArgs<double> &, cudaStream_t);
+template int launch_ionic<float>(int, const IonicArgs<float> &, cudaStream_t, int);
+template int launch_ionic<double>(int, const IonicArgs<double> &, cudaStream_t, int);
 
 }  // namespace ep

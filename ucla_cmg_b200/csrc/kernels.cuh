@@ -79,7 +79,7 @@ template <typename R> struct IonicArgs {
 };
 
 template <typename R>
-int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t s);
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t s, int block = 128);
 
 // Crank-Nicolson half diffusion step: x <- A^-1 (B x) by Jacobi-PCG in one
 // persistent cooperative launch (Solvers/EP_CrankNicholson.cc:99-104).
@@ -96,19 +96,29 @@ template <typename R> struct CGArgs {
     int maxit;
     unsigned long long *iters_total;
     unsigned int *iters_max, *fails;
-    double *last;                // [0] iterations, [1] ||r||/||r0|| of this solve
+    double *last;                // per instance: [2k] iterations, [2k+1] ||r||/||r0||
+    // independent instances (block-diagonal operator): instance k owns rows
+    // [inst_row[k], inst_row[k+1]) and CTAs [inst_blk[k], inst_blk[k+1]),
+    // solves on its own (own dots, stop test and barrier bar[k]).  ninst <= 1:
+    // one instance owning every row and CTA.
+    int ninst;
+    const int *inst_row, *inst_blk;
 };
 
 template <typename R>
 int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s);
+// CTAs of the persistent launch: per_sm (0 = as many as fit) x SM count
 template <typename R>
-int cg_grid_size(int block, int *grid);
+int cg_grid_size(int block, int *grid, int per_sm = 0);
+template <typename R>
+int cg_max_per_sm(int block, int *per);
 
 // ECG_k = sum_i W[k n + i] V[i] (ComputeECG.h:172-189 in per-node form),
 // deterministic two-level reduction, written to out[k].
 template <typename R>
 int launch_ecg(int n, int ne, const R *W, int wpitch, const R *V, double *partial,
-               unsigned int *counter, double *out, int grid, cudaStream_t s);
+               unsigned int *counter, double *out, int grid, cudaStream_t s,
+               unsigned int *slot = nullptr, int cap = 0);
 
 void launch_step_inc(long long *step, cudaStream_t s);
 

@@ -305,8 +305,11 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
         } else if (valid && inside) {
             float d[SG_NY];
 #pragma unroll
-            for (int j = 0; j < SG_NY; j++)
-                d[j] = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+            for (int j = 0; j < SG_NY; j++) {
+                const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+                const float sc = aux->out_scale[j];
+                d[j] = sc > 0.f ? sc * sinhf(u) : u;
+            }
             const unsigned int lm = aux->log_mask;
             float sn[18];
 #pragma unroll
@@ -318,6 +321,44 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
             }
             const float V0 = x[0];
             float V1 = x[0] + d[0];
+            if (aux->v_update == 2) {
+                // the network replaces the Newton solve of Compute_Ion: the
+                // concentrations move from their start to the predicted end
+                // values over the sub-steps (geometrically for log-scaled
+                // ones); gates and V take the reference sub-steps
+                float s[18];
+#pragma unroll
+                for (int k = 0; k < 18; k++) s[k] = x[k + 1];
+                const int slot[6] = {0, 1, 2, 9, 16, 17};
+                float V = V0, tsum = 0.f;
+                const float rdt = 1.f / (float)a.t_per_step;
+                Track tr = {-1.f, -1.f, -1.f, 1e30f};
+                bool dirty = false;
+                const bool trk = a.track != nullptr;
+                if (trk) tr = a.track[i];
+                double tsub = t0;
+                for (int k = 0; k < a.nsub; k++) {
+                    const float h = a.sub_dt[k];
+                    tt_gate_step(s, V, h, c);
+                    tsum += h;
+                    const float w = fminf(tsum * rdt, 1.f);
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        const int q = slot[j];
+                        const float a0 = x[q + 1], a1 = sn[q];
+                        s[q] = ((lm >> (q + 1)) & 1u) ? a0 * __powf(a1 / a0, w) : a0 + w * (a1 - a0);
+                    }
+                    const float v1 = V + h * tt_dvdt<float>(V, s, c, 0.f, gks_i);
+                    if (trk && tr.t_rep < 0.f) track_interval(tr, dirty, V, v1, tsub, h, a.act_thr);
+                    V = v1;
+                    tsub += (double)h;
+                }
+#pragma unroll
+                for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = s[k];
+                a.V[i] = V;
+                if (dirty) a.track[i] = tr;
+                continue;
+            }
             if (aux->v_update == 1) {
                 // midpoint rule on the model's own current balance: the
                 // network's dV only places the midpoint; the states there are

@@ -23,10 +23,12 @@ struct SurrogateAux {
     float b1[SG_H], b2[SG_H], b3[SG_H], b4[SG_NOUT];
     float in_mean[SG_KIN], in_rstd[SG_KIN];
     float out_mean[SG_NOUT], out_std[SG_NOUT];
+    float out_scale[SG_NOUT];   // > 0: output j is asinh(delta / out_scale[j])
     float env_lo[SG_KIN], env_hi[SG_KIN];   // in the transformed (log) space
     float nah_max;
     unsigned int log_mask;      // bit k: feature k (and state output k) is log-scaled
-    int v_update;               // 0: V += network dV; 1: midpoint current balance
+    int v_update;               // 0: V += network dV; 1: midpoint current balance;
+                                // 2: network concentrations, reference gates and V
 };
 
 // element offset of (row r, column k) of an R x K bf16 matrix in the core
@@ -47,6 +49,8 @@ struct SurrogateArgs {
     const long long *stim_on, *stim_off;
     const float *stim_amp;
     const long long *step_ptr;
+    int nsub;                           // ionic sub-steps of one global step
+    float sub_dt[kMaxSub];
     double t_per_step;
     float Cm, Xi, act_thr;
     Track *track;

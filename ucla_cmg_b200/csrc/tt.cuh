@@ -271,6 +271,21 @@ EP_HD void lu6_solve(R a[36], R b[6]) {
     }
 }
 
+// the 12 gates of one Compute_Ion call: semi-implicit (s + dt inf/tau) /
+// (1 + dt/tau) at voltage V (UpdateStateVariables, Tusscher.cc:116-195)
+template <typename R>
+EP_HD void tt_gate_step(R s[TT_NS], R V, R dt, const R *__restrict__ c) {
+    R ginf[12], gtau[12];
+    tt_gates(V, s[9], c, ginf, gtau);
+    const int gidx[12] = {3, 4, 5, 6, 7, 8, 10, 11, 12, 13, 14, 15};
+#pragma unroll
+    for (int g = 0; g < 12; g++) {
+        const R b = R(-1) / gtau[g];
+        const R a = ginf[g] / gtau[g];
+        s[gidx[g]] = (s[gidx[g]] + dt * a) / (R(1) - dt * b);
+    }
+}
+
 struct TTOpts {
     int newton_cap;
     int jac_true;
@@ -284,18 +299,7 @@ struct TTOpts {
 template <typename R>
 EP_HD R tt_compute_ion(R s[TT_NS], R V, R ist, R dt, const R *__restrict__ c,
                                             R gks, const TTOpts &opt, int &iters) {
-    // ---- gates (semi-implicit) ----
-    {
-        R ginf[12], gtau[12];
-        tt_gates(V, s[9], c, ginf, gtau);
-        const int gidx[12] = {3, 4, 5, 6, 7, 8, 10, 11, 12, 13, 14, 15};
-#pragma unroll
-        for (int g = 0; g < 12; g++) {
-            const R b = R(-1) / gtau[g];
-            const R a = ginf[g] / gtau[g];
-            s[gidx[g]] = (s[gidx[g]] + dt * a) / (R(1) - dt * b);
-        }
-    }
+    tt_gate_step(s, V, dt, c);
     const TTFixed<R> f = tt_fixed<R>(V, s, c, ist, gks);
     // Newton slots: Ki s0, Nai s1, Cai s2, Cass s9, CaSR s16, R' s17
     R x[6] = {s[0], s[1], s[2], s[9], s[16], s[17]};

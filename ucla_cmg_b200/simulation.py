@@ -21,6 +21,61 @@ from . import capi
 from .capi import check, ptr
 
 
+def _instance_descs(mesh, model, D, Cm, node_type, type_consts, n_types, gks_scale, user_xi,
+                    newton_cap, tt_jacobian, mh_abs_mode, initial_states):
+    """MeshDesc and ModelDesc of one instance, and the arrays they point to."""
+    keep = {}
+    keep["xyz"] = np.ascontiguousarray(mesh.xyz, dtype=np.float64)
+    keep["tets"] = np.ascontiguousarray(mesh.tets, dtype=np.int32)
+    keep["fib"] = None if mesh.fibers is None else np.ascontiguousarray(mesh.fibers, dtype=np.float64)
+    md = capi.MeshDesc()
+    md.n_nodes = mesh.n
+    md.xyz = ptr(keep["xyz"])
+    md.n_tets = mesh.m
+    md.tets = ptr(keep["tets"], C.POINTER(C.c_int32))
+    md.one_based = 0
+    md.fibers = ptr(keep["fib"])
+    for k in range(3):
+        md.D[k] = float(D[k])
+    md.Cm = float(Cm)
+    mo = capi.ModelDesc()
+    mo.model = model
+    keep["types"] = None if node_type is None else np.ascontiguousarray(node_type, dtype=np.uint8)
+    keep["tc"] = None if type_consts is None else np.ascontiguousarray(type_consts, dtype=np.float64)
+    if n_types is None:
+        if keep["tc"] is not None:
+            n_types = keep["tc"].shape[0]
+        elif keep["types"] is not None and len(keep["types"]):
+            n_types = int(keep["types"].max()) + 1
+        else:
+            n_types = 1
+    mo.n_types = int(n_types)
+    mo.type_consts = ptr(keep["tc"])
+    mo.node_type = ptr(keep["types"], C.POINTER(C.c_uint8))
+    keep["gks"] = None if gks_scale is None else np.ascontiguousarray(gks_scale, dtype=np.float64)
+    mo.node_gks_scale = ptr(keep["gks"])
+    mo.user_xi = float(user_xi)
+    mo.newton_cap = int(newton_cap)
+    mo.tt_jacobian = int(tt_jacobian)
+    mo.mh_abs_mode = int(mh_abs_mode)
+    keep["init"] = None if initial_states is None else np.ascontiguousarray(initial_states, dtype=np.float64)
+    mo.initial_states = ptr(keep["init"])
+    return md, mo, keep
+
+
+def _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, ecg_every,
+                 act_threshold):
+    sd = capi.SolverDesc()
+    sd.dt, sd.ionic_dt = float(dt), float(ionic_dt)
+    sd.cg_tol, sd.cg_maxit = float(cg_tol), int(cg_maxit)
+    sd.smoothing_alpha = float(smoothing_alpha)
+    sd.precision = int(precision)
+    sd.newton_tol = float(newton_tol)
+    sd.ecg_every = int(ecg_every)
+    sd.act_threshold = float(act_threshold)
+    return sd
+
+
 class Monodomain:
     """One tissue instance on one GPU (FP64 or FP32 arithmetic).
 
@@ -40,54 +95,40 @@ class Monodomain:
         self.precision = precision
         self.dt = float(dt)
         self.n = mesh.n
-        self._xyz = np.ascontiguousarray(mesh.xyz, dtype=np.float64)
-        self._tets = np.ascontiguousarray(mesh.tets, dtype=np.int32)
-        self._fib = None if mesh.fibers is None else np.ascontiguousarray(mesh.fibers, dtype=np.float64)
-        md = capi.MeshDesc()
-        md.n_nodes = mesh.n
-        md.xyz = ptr(self._xyz)
-        md.n_tets = mesh.m
-        md.tets = ptr(self._tets, C.POINTER(C.c_int32))
-        md.one_based = 0
-        md.fibers = ptr(self._fib)
-        for k in range(3):
-            md.D[k] = float(D[k])
-        md.Cm = float(Cm)
-        mo = capi.ModelDesc()
-        mo.model = model
-        self._types = None if node_type is None else np.ascontiguousarray(node_type, dtype=np.uint8)
-        self._tc = None if type_consts is None else np.ascontiguousarray(type_consts, dtype=np.float64)
-        if n_types is None:
-            if self._tc is not None:
-                n_types = self._tc.shape[0]
-            elif self._types is not None and len(self._types):
-                n_types = int(self._types.max()) + 1
-            else:
-                n_types = 1
-        mo.n_types = int(n_types)
-        mo.type_consts = ptr(self._tc)
-        mo.node_type = ptr(self._types, C.POINTER(C.c_uint8))
-        self._gks = None if gks_scale is None else np.ascontiguousarray(gks_scale, dtype=np.float64)
-        mo.node_gks_scale = ptr(self._gks)
-        mo.user_xi = float(user_xi)
-        mo.newton_cap = int(newton_cap)
-        mo.tt_jacobian = int(tt_jacobian)
-        mo.mh_abs_mode = int(mh_abs_mode)
-        self._init = None if initial_states is None else np.ascontiguousarray(initial_states, dtype=np.float64)
-        mo.initial_states = ptr(self._init)
-        sd = capi.SolverDesc()
-        sd.dt, sd.ionic_dt = float(dt), float(ionic_dt)
-        sd.cg_tol, sd.cg_maxit = float(cg_tol), int(cg_maxit)
-        sd.smoothing_alpha = float(smoothing_alpha)
-        sd.precision = int(precision)
-        sd.newton_tol = float(newton_tol)
-        sd.ecg_every = int(ecg_every)
-        sd.act_threshold = float(act_threshold)
+        md, mo, self._keep = _instance_descs(mesh, model, D, Cm, node_type, type_consts, n_types, gks_scale,
+                                             user_xi, newton_cap, tt_jacobian, mh_abs_mode, initial_states)
+        sd = _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, ecg_every,
+                          act_threshold)
         h = C.c_void_p()
         check(L.ep_create(C.byref(md), C.byref(mo), C.byref(sd), int(device), C.byref(h)))
         self._h = h
         self.nstate = L.ep_num_states(h)
         self.last_stats = None
+
+    # ---- launch shape ----
+    def launch_config(self):
+        c = capi.LaunchConfig()
+        check(capi.lib().ep_get_launch_config(self._h, C.byref(c)))
+        return c.as_dict()
+
+    def set_launch_config(self, cg_block=None, cg_per_sm=None, ionic_block=None, graph_steps=None):
+        cur = self.launch_config()
+        c = capi.LaunchConfig()
+        c.cg_block = cur["cg_block"] if cg_block is None else int(cg_block)
+        c.cg_per_sm = cur["cg_per_sm"] if cg_per_sm is None else int(cg_per_sm)
+        c.ionic_block = cur["ionic_block"] if ionic_block is None else int(ionic_block)
+        c.graph_steps = cur["graph_steps"] if graph_steps is None else int(graph_steps)
+        check(capi.lib().ep_set_launch_config(self._h, C.byref(c)))
+
+    def autotune(self, trial_steps=20):
+        """Pick the launch shape by timing (ep_autotune); returns
+        (config dict, ms/step chosen, ms/step at the start, configurations tried)."""
+        c = capi.LaunchConfig()
+        best, start = C.c_double(), C.c_double()
+        tried = C.c_int32()
+        check(capi.lib().ep_autotune(self._h, int(trial_steps), C.byref(c), C.byref(best), C.byref(start),
+                                     C.byref(tried)))
+        return c.as_dict(), best.value, start.value, tried.value
 
     # ---- life cycle ----
     def close(self):
@@ -213,6 +254,72 @@ class Monodomain:
         check(capi.lib().ep_read_restart(self._h, float(t), str(directory).encode()))
 
     readRestart = read_restart
+
+
+class Batch(Monodomain):
+    """Independent tissue instances advanced together (ep_batch_create).
+
+    instances: list of dicts with the per-instance keywords of
+    :class:`Monodomain` (mesh, and optionally D, node_type, type_consts,
+    n_types, gks_scale, initial_states); the cell model, C_m and the solver
+    settings are shared.  Every per-node array of the API is the instances'
+    nodes concatenated in order: ``offsets[k]`` is where instance k starts.
+    """
+
+    def __init__(self, instances, model=capi.TUSSCHER, precision=capi.FP32, dt=0.02, ionic_dt=0.02,
+                 Cm=1.0, cg_tol=1e-7, cg_maxit=1000, user_xi=0.0, newton_cap=0,
+                 tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0, smoothing_alpha=0.0, newton_tol=0.0,
+                 act_threshold=-40.0, device=0):
+        L = capi.lib()
+        self.model = model
+        self.precision = precision
+        self.dt = float(dt)
+        self.meshes = [inst["mesh"] for inst in instances]
+        k = len(instances)
+        mds = (capi.MeshDesc * k)()
+        mos = (capi.ModelDesc * k)()
+        self._keep = []
+        for i, inst in enumerate(instances):
+            md, mo, keep = _instance_descs(inst["mesh"], model, inst.get("D", (1e-3, 5e-4, 2.5e-4)), Cm,
+                                           inst.get("node_type"), inst.get("type_consts"), inst.get("n_types"),
+                                           inst.get("gks_scale"), user_xi, newton_cap, tt_jacobian, mh_abs_mode,
+                                           inst.get("initial_states"))
+            mds[i] = md
+            mos[i] = mo
+            self._keep.append(keep)
+        sd = _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, 0,
+                          act_threshold)
+        h = C.c_void_p()
+        check(L.ep_batch_create(k, mds, mos, C.byref(sd), int(device), C.byref(h)))
+        self._h = h
+        self.nstate = L.ep_num_states(h)
+        self.n = L.ep_num_nodes(h)
+        self.last_stats = None
+        self.n_inst = k
+        off = np.zeros(k + 1, np.int32)
+        cta = np.zeros(k + 1, np.int32)
+        check(L.ep_batch_layout(h, None, ptr(off, C.POINTER(C.c_int32)), ptr(cta, C.POINTER(C.c_int32))))
+        self.offsets = off
+        self.cta_offsets = cta
+
+    def split(self, a):
+        """Per-instance views of a concatenated per-node array."""
+        return [a[self.offsets[k]:self.offsets[k + 1]] for k in range(self.n_inst)]
+
+    def cg_last(self):
+        it = np.zeros(self.n_inst, np.int32)
+        rr = np.zeros(self.n_inst)
+        check(capi.lib().ep_batch_cg_last(self._h, ptr(it, C.POINTER(C.c_int32)), ptr(rr)))
+        return it, rr
+
+
+def batch_plan(inst_row, grid):
+    """The CTA-group split of the persistent CG launch (ep_batch_plan)."""
+    row = np.ascontiguousarray(inst_row, dtype=np.int32)
+    out = np.zeros(len(row), np.int32)
+    check(capi.lib().ep_batch_plan(len(row) - 1, ptr(row, C.POINTER(C.c_int32)), int(grid),
+                                   ptr(out, C.POINTER(C.c_int32))))
+    return out
 
 
 def ionic_step(model, V, istim, states, dt, Cm=1.0, precision=capi.FP64, node_type=None,

@@ -67,26 +67,37 @@ class Surrogate:
     env_hi: np.ndarray
     nah_max: float = NAH_MAX
     log_mask: int = LOG_MASK
-    v_update: int = 1
+    v_update: int = 0
+    out_scale: np.ndarray = None       # per output s_j > 0: targets are asinh(delta / s_j)
     meta: dict = field(default_factory=dict)
 
     def save(self, path=DEFAULT_PATH):
         os.makedirs(os.path.dirname(path), exist_ok=True)
+        sc = np.zeros(DIMS[-1], np.float32) if self.out_scale is None else self.out_scale
         np.savez_compressed(path, params=self.params, in_mean=self.in_mean, in_std=self.in_std,
                             out_mean=self.out_mean, out_std=self.out_std, env_lo=self.env_lo,
                             env_hi=self.env_hi, nah_max=self.nah_max, log_mask=self.log_mask,
-                            v_update=self.v_update,
+                            v_update=self.v_update, out_scale=sc,
                             meta=np.array(repr(self.meta)))
 
     @classmethod
     def load(cls, path=DEFAULT_PATH):
         z = np.load(path, allow_pickle=False)
-        return cls(z["params"].astype(np.float32), z["in_mean"].astype(np.float32),
-                   z["in_std"].astype(np.float32), z["out_mean"].astype(np.float32),
-                   z["out_std"].astype(np.float32), z["env_lo"].astype(np.float32),
-                   z["env_hi"].astype(np.float32), float(z["nah_max"]),
+        f32 = lambda k: z[k].astype(np.float32)
+        return cls(f32("params"), f32("in_mean"), f32("in_std"), f32("out_mean"), f32("out_std"),
+                   f32("env_lo"), f32("env_hi"), float(z["nah_max"]),
                    int(z["log_mask"]) if "log_mask" in z else 0,
-                   int(z["v_update"]) if "v_update" in z else 1, {"meta": str(z["meta"])})
+                   int(z["v_update"]) if "v_update" in z else 0,
+                   f32("out_scale") if "out_scale" in z else None, {"meta": str(z["meta"])})
+
+    def decode(self, Yn):
+        """Network outputs (normalised) -> changes over the step (log changes
+        for the log-scaled states)."""
+        U = np.asarray(Yn, np.float64) * self.out_std + self.out_mean
+        if self.out_scale is not None:
+            sc = np.asarray(self.out_scale, np.float64)
+            U = np.where(sc > 0, sc * np.sinh(U), U)
+        return U
 
     def desc(self):
         """capi.SurrogateDesc (and the arrays it points to, keep them alive)."""
@@ -100,6 +111,10 @@ class Surrogate:
         d.nah_max = float(self.nah_max)
         d.log_mask = int(self.log_mask)
         d.v_update = int(self.v_update)
+        if self.out_scale is not None:
+            sc = np.ascontiguousarray(self.out_scale, dtype=np.float32)
+            keep.append(sc)
+            d.out_scale = ptr(sc, fp)
         return d, keep
 
     def deploy(self, sim):
@@ -294,11 +309,24 @@ class Trainer:
             pass
 
 
-def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, w_v=10.0):
-    """Fit the network to normalised (X, Y) on the GPU; returns a Surrogate."""
+def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, w_v=10.0,
+          asinh_q=None):
+    """Fit the network to normalised (X, Y) on the GPU; returns a Surrogate.
+
+    asinh_q: if given, output j is learned as asinh(Y_j / s_j) with s_j the
+    asinh_q quantile of |Y_j|, so that the small changes of the plateau and
+    of rest are fitted to a relative, not an absolute, accuracy."""
     import torch
     X = np.asarray(X, np.float32)
     Y = np.asarray(Y, np.float32)
+    out_scale = None
+    if asinh_q is not None:
+        aY = np.abs(Y[: min(len(Y), 2_000_000)]).astype(np.float64)
+        sc = np.quantile(aY, asinh_q, axis=0)
+        sc = np.maximum(sc, 1e-6 * aY.max(axis=0))
+        sc = np.maximum(sc, 1e-30)
+        out_scale = sc.astype(np.float32)
+        Y = np.arcsinh(Y.astype(np.float64) / sc).astype(np.float32)
     # statistics in FP64 (column sums of millions of FP32 values lose digits)
     X64 = X.astype(np.float64)
     Y64 = Y.astype(np.float64)
@@ -367,7 +395,9 @@ def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, 
     tr.close()
     return Surrogate(p, in_mean, in_std, out_mean, out_std, env_lo.astype(np.float32),
                      env_hi.astype(np.float32), nah_max=NAH_MAX, log_mask=LOG_MASK,
-                     meta={"n_samples": int(n), "epochs": epochs, "history": hist})
+                     out_scale=out_scale,
+                     meta={"n_samples": int(n), "epochs": epochs, "lr": lr, "batch": batch,
+                           "asinh_q": asinh_q, "history": hist})
 
 
 def main():
@@ -378,12 +408,23 @@ def main():
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_PATH)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--asinh-q", type=float, default=None)
+    ap.add_argument("--data", default=None, help="cache of the generated pairs (.npz)")
     args = ap.parse_args()
     t0 = time.time()
-    X, Y = generate(args.samples, seed=args.seed)
+    if args.data and os.path.exists(args.data):
+        z = np.load(args.data)
+        X, Y = z["X"], z["Y"]
+    else:
+        X, Y = generate(args.samples, seed=args.seed)
+        if args.data:
+            np.savez(args.data, X=X, Y=Y)
     print(f"data: {X.shape} in {time.time() - t0:.1f} s", flush=True)
     t1 = time.time()
-    s = train(X, Y, epochs=args.epochs, seed=args.seed)
+    s = train(X, Y, epochs=args.epochs, seed=args.seed, lr=args.lr, batch=args.batch,
+              asinh_q=args.asinh_q)
     print(f"training: {time.time() - t1:.1f} s", flush=True)
     s.save(args.out)
     print("saved", args.out)

@@ -105,3 +105,60 @@ def shell_c2(h=0.0365, n_rho=20, seed=0, n_pmj=200):
     return Workload("shell_c2", m, capi.TUSSCHER, 0.1, 0.02, 500.0, M.sigma_to_D(1.2, 0.2), -85.423,
                     ids, on, on + 2.0, np.full(len(ids), 50.0 * TT_XI), el,
                     node_type=node_type, type_consts=tt_type_consts(), gks_scale=gks)
+
+
+@dataclass
+class BatchWorkload:
+    name: str
+    instances: list          # dicts: mesh, D, node_type, type_consts
+    model: int
+    dt: float
+    ionic_dt: float
+    T: float
+    V0: float
+    stim_ids: np.ndarray     # concatenated node ids
+    stim_on: np.ndarray
+    stim_off: np.ndarray
+    stim_amp: np.ndarray
+
+    @property
+    def n_nodes(self):
+        return sum(inst["mesh"].n for inst in self.instances)
+
+    def create(self, precision=capi.FP32, tt_jacobian=capi.TT_JAC_TRUE, **kw):
+        from .simulation import Batch
+        b = Batch(self.instances, self.model, precision, dt=self.dt, ionic_dt=self.ionic_dt,
+                  tt_jacobian=tt_jacobian, **kw)
+        b.set_voltage(self.V0)
+        b.set_stimulus(self.stim_ids, self.stim_on, self.stim_off, self.stim_amp)
+        return b
+
+
+def batch_c3(n_inst=64, seed=0, h=0.02, lo=(21, 21, 6), hi=(101, 101, 11)):
+    """64 independent ten Tusscher slabs of uneven size (grid uniform in
+    21x21x6 .. 101x101x11 nodes, spacing 0.02 cm), each with G_Ks, G_to and
+    G_CaL scaled by U(0.5, 1.5) and a 5x5-node full-thickness stimulus block
+    at a random one of its four vertical edges (50 uA/cm^2, 1 ms at t = 0);
+    FP32, dt = 0.02 ms, 200 ms."""
+    rng = np.random.default_rng(seed)
+    epi = capi.default_consts(capi.TUSSCHER)
+    inst, ids, off = [], [], 0
+    for k in range(n_inst):
+        nx, ny = (int(v) for v in rng.integers(lo[:2], np.asarray(hi[:2]) + 1))
+        nz = int(rng.integers(lo[2], hi[2] + 1))
+        m = M.slab(nx, ny, nz, (nx - 1) * h, (ny - 1) * h, (nz - 1) * h)
+        tc = epi.copy()
+        for c in (15, 20, 18):                       # G_Ks, G_to, G_CaL
+            tc[c] *= rng.uniform(0.5, 1.5)
+        corner = int(rng.integers(0, 4))
+        ci = (nx - 5) if corner & 1 else 0
+        cj = (ny - 5) if corner & 2 else 0
+        i, j, kk = np.meshgrid(np.arange(ci, ci + 5), np.arange(cj, cj + 5), np.arange(nz), indexing="ij")
+        blk = (i + nx * (j + ny * kk)).ravel()
+        ids.append(blk + off)
+        inst.append(dict(mesh=m, D=M.sigma_to_D(1.2, 0.2), type_consts=tc[None, :], n_types=1))
+        off += m.n
+    ids = np.concatenate(ids).astype(np.int32)
+    k = len(ids)
+    return BatchWorkload("batch_c3", inst, capi.TUSSCHER, 0.02, 0.02, 200.0, -85.423, ids,
+                         np.zeros(k), np.ones(k), np.full(k, 50.0 * TT_XI))
