@@ -316,6 +316,12 @@ typedef struct ep_surrogate_desc {
                                        change of log(x) and x' = x exp(out) */
     const float *out_scale;         /* NULL, or per output s_j > 0: the network
                                        predicts asinh(delta_j / s_j) (0: delta_j) */
+    const float *out_lo, *out_hi;   /* NULL, or the accepted range of each
+                                       de-normalised output (before the asinh
+                                       inverse); a node whose used outputs leave
+                                       it runs the plain model */
+    int32_t hybrid_substeps;        /* v_update 2: gate/V sub-steps per global
+                                       step (0: the handle's ionic sub-steps) */
     int32_t v_update;               /* 0: V' = V + dV from the network;
                                        1: V' = V + dt dV/dt(V + dV/2, (s + s')/2),
                                        the cell model's own current balance at

@@ -69,7 +69,8 @@ class SurrogateDesc(C.Structure):
                 ("out_mean", C.POINTER(C.c_float)), ("out_std", C.POINTER(C.c_float)),
                 ("env_lo", C.POINTER(C.c_float)), ("env_hi", C.POINTER(C.c_float)),
                 ("nah_max", C.c_float), ("log_mask", C.c_uint32),
-                ("out_scale", C.POINTER(C.c_float)), ("v_update", C.c_int32)]
+                ("out_scale", C.POINTER(C.c_float)), ("out_lo", C.POINTER(C.c_float)),
+                ("out_hi", C.POINTER(C.c_float)), ("hybrid_substeps", C.c_int32), ("v_update", C.c_int32)]
 
 
 class LaunchConfig(C.Structure):

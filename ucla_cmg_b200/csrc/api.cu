@@ -1007,12 +1007,20 @@ static int pack_surrogate(const ep_surrogate_desc *d, std::vector<unsigned short
         aux.out_mean[j] = j < SG_NY ? d->out_mean[j] : 0.f;
         aux.out_std[j] = j < SG_NY ? d->out_std[j] : 0.f;
         aux.out_scale[j] = (j < SG_NY && d->out_scale) ? d->out_scale[j] : 0.f;
+        aux.out_lo[j] = (j < SG_NY && d->out_lo) ? d->out_lo[j] : -3.0e38f;
+        aux.out_hi[j] = (j < SG_NY && d->out_hi) ? d->out_hi[j] : 3.0e38f;
         EP_CHECK_ARG(aux.out_scale[j] >= 0.f, "out_scale must be >= 0");
     }
     aux.nah_max = d->nah_max;
     aux.log_mask = d->log_mask & ((1u << SG_NF) - 1u) & ~1u;   // V stays linear
     EP_CHECK_ARG(d->v_update >= 0 && d->v_update <= 2, "v_update must be 0, 1 or 2");
     aux.v_update = d->v_update;
+    // outputs the update reads: the six Newton concentrations (stored states
+    // Ki 1, Nai 2, Cai 3, Cass 10, CaSR 17, R' 18) in the hybrid form
+    aux.out_mask = d->v_update == 2 ? ((1u << 1) | (1u << 2) | (1u << 3) | (1u << 10) | (1u << 17) | (1u << 18))
+                                    : ((1u << SG_NY) - 1u);
+    EP_CHECK_ARG(d->hybrid_substeps >= 0 && d->hybrid_substeps <= kMaxSub, "hybrid_substeps out of range");
+    aux.hyb_sub = d->hybrid_substeps;
     return EP_OK;
 }
 

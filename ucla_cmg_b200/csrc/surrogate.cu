@@ -302,13 +302,23 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
         if (valid && raw) {
 #pragma unroll
             for (int j = 0; j < SG_NOUT; j++) a.rawY[(size_t)i * SG_NOUT + j] = __uint_as_float(yv[j]) + aux->b4[j];
-        } else if (valid && inside) {
+        } else if (valid) {
+            // de-normalise; a used output outside the range seen in training
+            // sends the node to the plain model as well
             float d[SG_NY];
+            bool out_ok = inside;
 #pragma unroll
             for (int j = 0; j < SG_NY; j++) {
                 const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+                if ((aux->out_mask >> j) & 1u) out_ok = out_ok && (u >= aux->out_lo[j]) && (u <= aux->out_hi[j]);
                 const float sc = aux->out_scale[j];
-                d[j] = sc > 0.f ? sc * sinhf(u) : u;
+                d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
+            }
+            if (!out_ok) {
+                const int slot = atomicAdd(a.fallback_count, 1);
+                a.fallback_list[slot] = i;
+                my_fb++;
+                continue;
             }
             const unsigned int lm = aux->log_mask;
             float sn[18];
@@ -317,28 +327,28 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
                 // log-scaled states are updated multiplicatively: x' = x exp(d)
                 const float xk = x[k + 1];
                 sn[k] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
-                a.S[(size_t)k * a.pitch + i] = sn[k];
             }
             const float V0 = x[0];
-            float V1 = x[0] + d[0];
+            Track tr = {-1.f, -1.f, -1.f, 1e30f};
+            bool dirty = false;
+            const bool trk = a.track != nullptr;
+            if (trk) tr = a.track[i];
             if (aux->v_update == 2) {
-                // the network replaces the Newton solve of Compute_Ion: the
+                // the network replaces the Newton solve of Compute_Ion: the six
                 // concentrations move from their start to the predicted end
                 // values over the sub-steps (geometrically for log-scaled
-                // ones); gates and V take the reference sub-steps
+                // ones); gates and V take the reference's sub-step formulas
                 float s[18];
 #pragma unroll
                 for (int k = 0; k < 18; k++) s[k] = x[k + 1];
                 const int slot[6] = {0, 1, 2, 9, 16, 17};
-                float V = V0, tsum = 0.f;
+                const int ns = aux->hyb_sub > 0 ? aux->hyb_sub : a.nsub;
+                const float hu = (float)a.t_per_step / (float)ns;
                 const float rdt = 1.f / (float)a.t_per_step;
-                Track tr = {-1.f, -1.f, -1.f, 1e30f};
-                bool dirty = false;
-                const bool trk = a.track != nullptr;
-                if (trk) tr = a.track[i];
+                float V = V0, tsum = 0.f;
                 double tsub = t0;
-                for (int k = 0; k < a.nsub; k++) {
-                    const float h = a.sub_dt[k];
+                for (int k = 0; k < ns; k++) {
+                    const float h = aux->hyb_sub > 0 ? hu : a.sub_dt[k];
                     tt_gate_step(s, V, h, c);
                     tsum += h;
                     const float w = fminf(tsum * rdt, 1.f);
@@ -356,32 +366,24 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
 #pragma unroll
                 for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = s[k];
                 a.V[i] = V;
-                if (dirty) a.track[i] = tr;
-                continue;
-            }
-            if (aux->v_update == 1) {
-                // midpoint rule on the model's own current balance: the
-                // network's dV only places the midpoint; the states there are
-                // the mean of the old and the predicted new states
-                float sm[18];
+            } else {
+                float V1 = V0 + d[0];
+                if (aux->v_update == 1) {
+                    // midpoint rule on the model's own current balance: the
+                    // network's dV only places the midpoint; the states there
+                    // are the mean of the old and the predicted new states
+                    float sm[18];
 #pragma unroll
-                for (int k = 0; k < 18; k++) sm[k] = 0.5f * (x[k + 1] + sn[k]);
-                const float dt = (float)a.t_per_step;
-                V1 = V0 + dt * tt_dvdt<float>(V0 + 0.5f * d[0], sm, c, 0.f, gks_i);
-            }
-            a.V[i] = V1;
-            if (a.track) {
-                Track tr = a.track[i];
-                if (tr.t_rep < 0.f) {
-                    bool dirty = false;
-                    track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
-                    if (dirty) a.track[i] = tr;
+                    for (int k = 0; k < 18; k++) sm[k] = 0.5f * (x[k + 1] + sn[k]);
+                    const float dt = (float)a.t_per_step;
+                    V1 = V0 + dt * tt_dvdt<float>(V0 + 0.5f * d[0], sm, c, 0.f, gks_i);
                 }
+#pragma unroll
+                for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = sn[k];
+                a.V[i] = V1;
+                if (trk && tr.t_rep < 0.f) track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
             }
-        } else if (valid) {
-            const int slot = atomicAdd(a.fallback_count, 1);
-            a.fallback_list[slot] = i;
-            my_fb++;
+            if (dirty) a.track[i] = tr;
         }
     }
     // count fallback node-steps

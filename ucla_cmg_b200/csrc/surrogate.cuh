@@ -24,6 +24,9 @@ struct SurrogateAux {
     float in_mean[SG_KIN], in_rstd[SG_KIN];
     float out_mean[SG_NOUT], out_std[SG_NOUT];
     float out_scale[SG_NOUT];   // > 0: output j is asinh(delta / out_scale[j])
+    float out_lo[SG_NOUT], out_hi[SG_NOUT];   // accepted range of the de-normalised outputs
+    unsigned int out_mask;      // outputs the state update uses
+    int hyb_sub;                // v_update 2: sub-steps per global step (0: the handle's)
     float env_lo[SG_KIN], env_hi[SG_KIN];   // in the transformed (log) space
     float nah_max;
     unsigned int log_mask;      // bit k: feature k (and state output k) is log-scaled

@@ -34,6 +34,9 @@ NAH_MAX = 2e-4
 # logarithms and are updated multiplicatively
 LOG_FEATURES = (3, 4, 6, 7, 8, 9, 10, 11, 15, 16)
 LOG_MASK = sum(1 << k for k in LOG_FEATURES)
+# outputs the hybrid form uses: the Newton concentrations Ki, Nai, Cai, Cass,
+# CaSR, R' (stored states 1, 2, 3, 10, 17, 18)
+CONC_OUTPUTS = (1, 2, 3, 10, 17, 18)
 _LOG = np.zeros(23, bool)
 _LOG[list(LOG_FEATURES)] = True
 
@@ -69,26 +72,35 @@ class Surrogate:
     log_mask: int = LOG_MASK
     v_update: int = 0
     out_scale: np.ndarray = None       # per output s_j > 0: targets are asinh(delta / s_j)
+    out_lo: np.ndarray = None          # accepted range of the de-normalised outputs
+    out_hi: np.ndarray = None
+    hybrid_substeps: int = 1
     meta: dict = field(default_factory=dict)
 
     def save(self, path=DEFAULT_PATH):
         os.makedirs(os.path.dirname(path), exist_ok=True)
         sc = np.zeros(DIMS[-1], np.float32) if self.out_scale is None else self.out_scale
+        big = np.full(DIMS[-1], 3e38, np.float32)
         np.savez_compressed(path, params=self.params, in_mean=self.in_mean, in_std=self.in_std,
                             out_mean=self.out_mean, out_std=self.out_std, env_lo=self.env_lo,
                             env_hi=self.env_hi, nah_max=self.nah_max, log_mask=self.log_mask,
                             v_update=self.v_update, out_scale=sc,
+                            out_lo=-big if self.out_lo is None else self.out_lo,
+                            out_hi=big if self.out_hi is None else self.out_hi,
+                            hybrid_substeps=self.hybrid_substeps,
                             meta=np.array(repr(self.meta)))
 
     @classmethod
     def load(cls, path=DEFAULT_PATH):
         z = np.load(path, allow_pickle=False)
         f32 = lambda k: z[k].astype(np.float32)
+        opt = lambda k: f32(k) if k in z else None
         return cls(f32("params"), f32("in_mean"), f32("in_std"), f32("out_mean"), f32("out_std"),
                    f32("env_lo"), f32("env_hi"), float(z["nah_max"]),
                    int(z["log_mask"]) if "log_mask" in z else 0,
                    int(z["v_update"]) if "v_update" in z else 0,
-                   f32("out_scale") if "out_scale" in z else None, {"meta": str(z["meta"])})
+                   opt("out_scale"), opt("out_lo"), opt("out_hi"),
+                   int(z["hybrid_substeps"]) if "hybrid_substeps" in z else 1, {"meta": str(z["meta"])})
 
     def decode(self, Yn):
         """Network outputs (normalised) -> changes over the step (log changes
@@ -111,10 +123,13 @@ class Surrogate:
         d.nah_max = float(self.nah_max)
         d.log_mask = int(self.log_mask)
         d.v_update = int(self.v_update)
-        if self.out_scale is not None:
-            sc = np.ascontiguousarray(self.out_scale, dtype=np.float32)
-            keep.append(sc)
-            d.out_scale = ptr(sc, fp)
+        for name in ("out_scale", "out_lo", "out_hi"):
+            v = getattr(self, name)
+            if v is not None:
+                arr = np.ascontiguousarray(v, dtype=np.float32)
+                keep.append(arr)
+                setattr(d, name, ptr(arr, fp))
+        d.hybrid_substeps = int(self.hybrid_substeps)
         return d, keep
 
     def deploy(self, sim):
@@ -310,12 +325,14 @@ class Trainer:
 
 
 def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, w_v=10.0,
-          asinh_q=None):
+          asinh_q=None, conc_only=False):
     """Fit the network to normalised (X, Y) on the GPU; returns a Surrogate.
 
     asinh_q: if given, output j is learned as asinh(Y_j / s_j) with s_j the
     asinh_q quantile of |Y_j|, so that the small changes of the plateau and
-    of rest are fitted to a relative, not an absolute, accuracy."""
+    of rest are fitted to a relative, not an absolute, accuracy.
+    conc_only: fit only the six Newton concentrations (the hybrid form,
+    v_update 2, reads nothing else)."""
     import torch
     X = np.asarray(X, np.float32)
     Y = np.asarray(Y, np.float32)
@@ -337,6 +354,10 @@ def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, 
     out_std = Y64.std(axis=0)
     out_std[out_std < 1e-20] = 1.0
     lo, hi = X64.min(axis=0), X64.max(axis=0)
+    # accepted output range: the targets' range widened by 25 % of its span
+    ylo, yhi = Y64.min(axis=0), Y64.max(axis=0)
+    out_lo = (ylo - 0.25 * (yhi - ylo)).astype(np.float32)
+    out_hi = (yhi + 0.25 * (yhi - ylo)).astype(np.float32)
     # training envelope: the data's box widened by 5 % of its span and by
     # 1 % of the magnitude (slow concentrations barely move in the data)
     margin = np.maximum(0.05 * (hi - lo), 0.01 * np.maximum(np.abs(lo), np.abs(hi)))
@@ -354,6 +375,9 @@ def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, 
     Xt, Yt = Xn[nval:], Yn[nval:]
     w = np.ones(DIMS[-1], np.float32)
     w[0] = w_v
+    if conc_only:
+        w[:] = 0.0
+        w[list(CONC_OUTPUTS)] = 1.0
     tr = Trainer(seed=seed, device=device)
     gen = torch.Generator(device=dev).manual_seed(seed)
     steps_per_epoch = max(1, len(Xt) // batch)
@@ -395,9 +419,10 @@ def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, 
     tr.close()
     return Surrogate(p, in_mean, in_std, out_mean, out_std, env_lo.astype(np.float32),
                      env_hi.astype(np.float32), nah_max=NAH_MAX, log_mask=LOG_MASK,
-                     out_scale=out_scale,
+                     out_scale=out_scale, out_lo=out_lo, out_hi=out_hi,
+                     v_update=2 if conc_only else 0, hybrid_substeps=1,
                      meta={"n_samples": int(n), "epochs": epochs, "lr": lr, "batch": batch,
-                           "asinh_q": asinh_q, "history": hist})
+                           "asinh_q": asinh_q, "conc_only": conc_only, "history": hist})
 
 
 def main():
@@ -412,6 +437,8 @@ def main():
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--asinh-q", type=float, default=None)
     ap.add_argument("--data", default=None, help="cache of the generated pairs (.npz)")
+    ap.add_argument("--conc-only", action="store_true",
+                    help="fit only the six Newton concentrations (hybrid form)")
     args = ap.parse_args()
     t0 = time.time()
     if args.data and os.path.exists(args.data):
@@ -424,7 +451,7 @@ def main():
     print(f"data: {X.shape} in {time.time() - t0:.1f} s", flush=True)
     t1 = time.time()
     s = train(X, Y, epochs=args.epochs, seed=args.seed, lr=args.lr, batch=args.batch,
-              asinh_q=args.asinh_q)
+              asinh_q=args.asinh_q, conc_only=args.conc_only)
     print(f"training: {time.time() - t1:.1f} s", flush=True)
     s.save(args.out)
     print("saved", args.out)
