@@ -274,6 +274,20 @@ def run_ours(args, rank, world, local):
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": int(st["launches"]),
             "clocks": clocks, "roofline": roof, "e2e": e2e}
+    if prec == capi.SURROGATE and not args.no_compare:
+        # the plain FP32 form over the same simulated window, for the ratio
+        # the metric is about (same handle set-up, same steps)
+        gp = wl.create(capi.FP32, device=local)
+        for k in range(0, pre, 500):
+            gp.step(min(500, pre - k))
+        gp.step(args.warmup)
+        torch.cuda.synchronize()
+        stp = gp.step(args.steps)
+        vp = n * args.steps * world / (stp["device_ms"] * 1e-3)
+        line["config"]["plain_fp32"] = {"value": vp, "ms_per_step": stp["device_ms"] / args.steps,
+                                        "cg_iters_per_solve": stp["cg_iters"] / max(1, 2 * args.steps)}
+        line["config"]["speedup_vs_plain_fp32"] = value / vp
+        gp.close()
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         h = float(os.environ.get("EP_CPU_SAMPLE_H", "0.12"))
@@ -331,6 +345,60 @@ def run_batch(args, rank, world, local, dist, prec):
         dist.destroy_process_group()
 
 
+def run_accuracy(args, local):
+    """The shell run for args.accuracy ms in the FP64, plain FP32 and learned
+    forms; errors of the last two against FP64: activation time, APD90, Vm
+    L-infinity over 1 ms snapshots, pseudo-ECG relative L2."""
+    import numpy as np
+    import torch
+    from ucla_cmg_b200 import capi, workloads as W
+    from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
+    torch.cuda.set_device(local)
+    wl = W.shell_c2()
+    steps = int(round(args.accuracy / wl.dt))
+    forms = (("fp64", capi.FP64), ("plain_fp32", capi.FP32), ("surrogate", capi.SURROGATE))
+    hs = {}
+    for name, prec in forms:
+        hs[name] = wl.create(prec, device=local)
+        if prec == capi.SURROGATE:
+            Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(hs[name])
+    res = {name: dict(ms=0.0, fb=0, vinf=0.0) for name, _ in forms}
+    # the three runs advance in lockstep; Vm is compared every 1 ms
+    for k in range(0, steps, 10):
+        V = {}
+        for name, _ in forms:
+            st = hs[name].step(min(10, steps - k))
+            res[name]["ms"] += st["device_ms"]
+            res[name]["fb"] += st["fallback_nodes"]
+            V[name] = hs[name].voltage()
+        for name in ("plain_fp32", "surrogate"):
+            res[name]["vinf"] = max(res[name]["vinf"], float(np.abs(V[name] - V["fp64"]).max()))
+    for name, _ in forms:
+        r = res[name]
+        r["ta"], r["apd"] = hs[name].activation()
+        r["ecg"] = hs[name].ecg()[1]
+        r["fb"] /= float(wl.mesh.n * steps)
+        hs[name].close()
+    ref = res["fp64"]
+    out = {"workload": "shell_c2", "t_ms": args.accuracy, "n_nodes": int(wl.mesh.n)}
+    for name in ("fp64", "plain_fp32", "surrogate"):
+        r = res[name]
+        e = {"node_steps_per_s": wl.mesh.n * steps / (r["ms"] * 1e-3), "fallback_fraction": r["fb"]}
+        if name != "fp64":
+            both = (ref["ta"] >= 0) & (r["ta"] >= 0)
+            da = np.abs(r["ta"] - ref["ta"])[both]
+            ab = (ref["apd"] > 0) & (r["apd"] > 0)
+            dp = np.abs(r["apd"] - ref["apd"])[ab]
+            e.update({"activated": float((r["ta"] >= 0).mean()), "activated_fp64": float((ref["ta"] >= 0).mean()),
+                      "act_err_ms": {"mean": float(da.mean()), "p99": float(np.percentile(da, 99)), "max": float(da.max())},
+                      "apd90_err_ms": {"n": int(ab.sum()), "mean": float(dp.mean()) if ab.any() else None,
+                                       "max": float(dp.max()) if ab.any() else None},
+                      "vm_linf_mv": r["vinf"],
+                      "ecg_rel_l2": float(np.linalg.norm(r["ecg"] - ref["ecg"]) / np.linalg.norm(ref["ecg"]))})
+        out[name] = e
+    print(json.dumps(out), flush=True)
+
+
 def _edge_count(m):
     import numpy as np
     e = np.concatenate([m.tets[:, [a, b]] for a in range(4) for b in range(a + 1, 4)])
@@ -348,10 +416,19 @@ def main():
     ap.add_argument("--form", default="plain_fp32", choices=["plain_fp32", "fp64", "surrogate"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3"])
+    ap.add_argument("--no-compare", action="store_true",
+                    help="surrogate form: skip the plain FP32 run over the same window")
     ap.add_argument("--t-start", type=float, default=40.0,
                     help="simulated ms advanced (untimed) before the warm-up")
+    ap.add_argument("--accuracy", type=float, default=0.0,
+                    help="instead of timing: run the shell this many ms in FP64, FP32 and the "
+                         "learned form and print the errors against FP64")
     args = ap.parse_args()
     rank, world, local = _env()
+    if args.accuracy > 0:
+        if rank == 0:
+            run_accuracy(args, local)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
     else:

@@ -235,15 +235,18 @@ int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_
  * SM (0 = as many as are co-resident); ionic_block: threads per CTA of the
  * ionic kernel (64 or 128); graph_steps: 0 launches every kernel from the
  * host, k > 0 replays the steps from an instantiated CUDA graph of k steps
- * (rounded up to a multiple of the ECG interval). */
+ * (rounded up to a multiple of the ECG interval); ionic_min_ctas: FP32
+ * ionic kernel compiled for at least 3 or 4 resident 128-thread CTAs per SM
+ * (fewer registers per thread), 0 = the compiler's register choice. */
 typedef struct ep_launch_config {
-    int32_t cg_block, cg_per_sm, ionic_block, graph_steps;
+    int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas;
 } ep_launch_config;
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);
 /* Autotuner: times trial_steps steps (after one untimed pass) for the
  * current shape, then by coordinate descent over the CG block size and CTAs
- * per SM, the ionic block size and graph replay, keeps the fastest and sets
+ * per SM, the ionic block size and register budget, and graph replay,
+ * keeps the fastest and sets
  * it.  The simulation state (V, states, trackers, step, ECG samples) is put
  * back afterwards.  best_ms / start_ms: device ms per step of the chosen and
  * of the starting shape; any output may be NULL. */

@@ -96,7 +96,7 @@ struct ep_handle {
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
-    int cg_per_sm = 0, ionic_block = 128, graph_steps = 0;
+    int cg_per_sm = 0, ionic_block = 128, ionic_min = 0, graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
@@ -373,7 +373,7 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
-    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block);
+    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block, h->ionic_min);
 }
 
 enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
@@ -408,11 +408,11 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if (h->precision == EP_SURROGATE) {
                 if ((rc = launch_learned_phase(h, ia))) return rc;
                 h->launches += 2;
-            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block))) {
+            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) {
                 return rc;
             }
         } else {
-            if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block))) return rc;
+            if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
         if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
@@ -1091,6 +1091,7 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cfg->cg_per_sm = h->cg_grid / std::max(1, nsm);
     cfg->ionic_block = h->ionic_block;
+    cfg->ionic_min_ctas = h->ionic_min;
     cfg->graph_steps = h->graph_steps;
     return EP_OK;
 }
@@ -1100,6 +1101,8 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256, "cg_block must be 128 or 256");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
+    EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
+                 "ionic_min_ctas must be 0, 3 or 4");
     EP_CHECK_ARG(cfg->graph_steps >= 0 && cfg->graph_steps <= 100000, "graph_steps out of range");
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
@@ -1114,6 +1117,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
         return rc;
     }
     h->ionic_block = cfg->ionic_block;
+    h->ionic_min = cfg->ionic_min_ctas;
     h->graph_steps = cfg->graph_steps;
     return EP_OK;
 }
@@ -1173,6 +1177,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     cur.cg_block = h->cg_block;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
+    cur.ionic_min_ctas = h->ionic_min;
     cur.graph_steps = h->graph_steps;
     int tried = 0;
     // ms per step of one configuration (negative: it could not run)
@@ -1214,6 +1219,15 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
         c.ionic_block = ib;
         const double t = trial(c);
         if (t >= 0 && t < t_best) { t_best = t; b = c; }
+    }
+    if (h->precision != EP_FP64) {
+        for (int mc : {0, 3, 4}) {
+            if (mc == b.ionic_min_ctas) continue;
+            ep_launch_config c = b;
+            c.ionic_min_ctas = mc;
+            const double t = trial(c);
+            if (t >= 0 && t < t_best) { t_best = t; b = c; }
+        }
     }
     for (int gs : {0, trial_steps}) {
         if (gs == b.graph_steps) continue;

@@ -73,8 +73,39 @@ __device__ __forceinline__ void grid_total(const double *partial, int stride, in
     __syncthreads();
 }
 
+// Row sums of one SELL slice, four slice columns at a time: the column and
+// value loads of a group are issued together, then the gathers, so each lane
+// has a dozen independent loads in flight (at one lane per row the kernel is
+// bound by memory latency, not bandwidth).  The products are still added in
+// column order, so the sums are those of the plain loop.
+template <typename R, typename F>
+__device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R *__restrict__ val, int beg, int w,
+                                           int lane, F gather) {
+    R acc = R(0);
+    int k = 0;
+    for (; k + 4 <= w; k += 4) {
+        int c[4];
+        R v[4], g[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int idx = beg + (k + u) * kSlice + lane;
+            c[u] = __ldg(col + idx);
+            v[u] = __ldg(val + idx);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) g[u] = gather(c[u]);
+#pragma unroll
+        for (int u = 0; u < 4; u++) acc += v[u] * g[u];
+    }
+    for (; k < w; k++) {
+        const int idx = beg + k * kSlice + lane;
+        acc += __ldg(val + idx) * gather(__ldg(col + idx));
+    }
+    return acc;
+}
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
+__global__ void __launch_bounds__(256, 6) k_cn_half(const CGArgs<R> a) {
     const int lane = threadIdx.x & 31;
     const int G = gridDim.x;                 // partial-array stride
     // this CTA's instance: its rows, its CTA group and its barrier
@@ -146,13 +177,10 @@ __global__ void __launch_bounds__(256) k_cn_half(const CGArgs<R> a) {
             for (int s = gwarp; s < s_hi; s += nwarps) {
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-                R q = R(0);
-                for (int k = 0; k < w; k++) {
-                    const int idx = beg + k * kSlice + lane;
-                    const int c = __ldg(a.col + idx);
-                    const R pj = pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pc + c));
-                    q += __ldg(a.Aval + idx) * pj;
-                }
+                const R *pcc = pc;
+                const R q = slice_row_sum(a.col, a.Aval, beg, w, lane, [&](int c) {
+                    return pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pcc + c));
+                });
                 if (row >= rb && row < re) {
                     const R pi = pdir(__ldg(a.dinv + row), a.r[row], bR, ldcg(pc + row));
                     pn[row] = pi;

@@ -97,8 +97,10 @@ __device__ __forceinline__ void ionic_node(const IonicArgs<R> &a, const int i, u
     if (dirty) a.track[i] = tr;
 }
 
-template <typename R, int MODEL, int NS>
-__global__ void __launch_bounds__(128) k_ionic(const IonicArgs<R> a) {
+// MINB > 1 asks the compiler for MINB resident CTAs of 128 threads per SM
+// (fewer registers, some spilled to L1); the autotuner picks it per workload
+template <typename R, int MODEL, int NS, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_ionic(const IonicArgs<R> a) {
     __shared__ unsigned long long s_newton;
     __shared__ unsigned int s_caps, s_bad;
     if (threadIdx.x == 0) { s_newton = 0; s_caps = 0; s_bad = 0; }
@@ -132,9 +134,31 @@ __global__ void __launch_bounds__(128) k_ionic(const IonicArgs<R> a) {
     }
 }
 
+template <typename R, int MINB>
+static void dispatch_ionic(int model, const IonicArgs<R> &a, int grid, int block, cudaStream_t st) {
+    switch (model) {
+    case EP_TUSSCHER:
+        k_ionic<R, EP_TUSSCHER, TT_NS, MINB><<<grid, block, 0, st>>>(a);
+        break;
+    case EP_MAHAJAN:
+    case EP_MAHAJAN_FAIL:
+        k_ionic<R, EP_MAHAJAN, MH_NS, MINB><<<grid, block, 0, st>>>(a);
+        break;
+    default:
+        k_ionic<R, EP_LUORUDY, LR_NS, 1><<<grid, block, 0, st>>>(a);
+        break;
+    }
+}
+
 template <typename R>
-int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block) {
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block, int min_ctas) {
     if (block != 64 && block != 128) { set_error("ionic block must be 64 or 128"); return EP_ERR_ARG; }
+    if (min_ctas != 0 && min_ctas != 3 && min_ctas != 4) { set_error("ionic min_ctas must be 0, 3 or 4"); return EP_ERR_ARG; }
+    if (model != EP_TUSSCHER && model != EP_MAHAJAN && model != EP_MAHAJAN_FAIL && model != EP_LUORUDY &&
+        model != EP_LUORUDYWITHGATE) {
+        set_error("unknown model %d", model);
+        return EP_ERR_ARG;
+    }
     int grid = div_up(a.n, block);
     if (a.n == 0) return EP_OK;
     if (a.node_list) {
@@ -144,27 +168,14 @@ int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block) {
         EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         grid = std::min(grid, 4 * nsm);
     }
-    switch (model) {
-    case EP_TUSSCHER:
-        k_ionic<R, EP_TUSSCHER, TT_NS><<<grid, block, 0, st>>>(a);
-        break;
-    case EP_MAHAJAN:
-    case EP_MAHAJAN_FAIL:
-        k_ionic<R, EP_MAHAJAN, MH_NS><<<grid, block, 0, st>>>(a);
-        break;
-    case EP_LUORUDY:
-    case EP_LUORUDYWITHGATE:
-        k_ionic<R, EP_LUORUDY, LR_NS><<<grid, block, 0, st>>>(a);
-        break;
-    default:
-        set_error("unknown model %d", model);
-        return EP_ERR_ARG;
-    }
+    if (sizeof(R) == 8 || min_ctas == 0) dispatch_ionic<R, 1>(model, a, grid, block, st);
+    else if (min_ctas == 3) dispatch_ionic<R, 3>(model, a, grid, block, st);
+    else dispatch_ionic<R, 4>(model, a, grid, block, st);
     EP_CUDA(cudaGetLastError());
     return EP_OK;
 }
 
-template int launch_ionic<float>(int, const IonicArgs<float> &, cudaStream_t, int);
-template int launch_ionic<double>(int, const IonicArgs<double> &, cudaStream_t, int);
+template int launch_ionic<float>(int, const IonicArgs<float> &, cudaStream_t, int, int);
+template int launch_ionic<double>(int, const IonicArgs<double> &, cudaStream_t, int, int);
 
 }  // namespace ep

@@ -79,7 +79,7 @@ template <typename R> struct IonicArgs {
 };
 
 template <typename R>
-int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t s, int block = 128);
+int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t s, int block = 128, int min_ctas = 0);
 
 // Crank-Nicolson half diffusion step: x <- A^-1 (B x) by Jacobi-PCG in one
 // persistent cooperative launch (Solvers/EP_CrankNicholson.cc:99-104).

@@ -111,13 +111,15 @@ class Monodomain:
         check(capi.lib().ep_get_launch_config(self._h, C.byref(c)))
         return c.as_dict()
 
-    def set_launch_config(self, cg_block=None, cg_per_sm=None, ionic_block=None, graph_steps=None):
+    def set_launch_config(self, cg_block=None, cg_per_sm=None, ionic_block=None, graph_steps=None,
+                          ionic_min_ctas=None):
         cur = self.launch_config()
         c = capi.LaunchConfig()
         c.cg_block = cur["cg_block"] if cg_block is None else int(cg_block)
         c.cg_per_sm = cur["cg_per_sm"] if cg_per_sm is None else int(cg_per_sm)
         c.ionic_block = cur["ionic_block"] if ionic_block is None else int(ionic_block)
         c.graph_steps = cur["graph_steps"] if graph_steps is None else int(graph_steps)
+        c.ionic_min_ctas = cur["ionic_min_ctas"] if ionic_min_ctas is None else int(ionic_min_ctas)
         check(capi.lib().ep_set_launch_config(self._h, C.byref(c)))
 
     def autotune(self, trial_steps=20):

@@ -178,15 +178,22 @@ def _random_slab(rng):
     g0, g1 = rng.uniform(0.6, 1.4, 2)
     gks = g0 + (g1 - g0) * (m.xyz[:, 1 - ax] / 0.8)
     tc = tt_type_consts()
-    # stimulus: a random corner or edge block, sometimes a second one later
+    # stimulus: a random corner or edge block, sometimes a second one later.
+    # The first beat starts after a random rest of up to 150 ms: in a large
+    # tissue most nodes wait that long for the wave, and their gates keep
+    # relaxing from the initial state meanwhile (slow Xr1 in particular).
     ids = []
     t_on = []
+    t_first = rng.uniform(0.0, 150.0) if rng.random() < 0.7 else 0.0
     for k in range(1 + (rng.random() < 0.5)):
+        t_k = t_first if k == 0 else rng.uniform(max(340.0, t_first + 300.0), 480.0)
+        if k == 1 and t_k >= 480.0:
+            break
         cx, cy = rng.integers(0, 2, 2) * (nx - 4)
         blk = ((m.xyz[:, 0] - cx * 0.02) ** 2 + (m.xyz[:, 1] - cy * 0.02) ** 2 < 0.1 ** 2)
         idx = np.where(blk)[0]
         ids.append(idx)
-        t_on.append(np.full(len(idx), 0.0 if k == 0 else rng.uniform(340.0, 440.0)))
+        t_on.append(np.full(len(idx), t_k))
     ids = np.concatenate(ids).astype(np.int32)
     t_on = np.concatenate(t_on)
     amp = rng.uniform(40.0, 60.0) * TT_XI
@@ -221,12 +228,12 @@ def generate(n_target=10_000_000, seed=0, T=500.0, every=5, device=0, verbose=Tr
             keep = in_domain(st, istim)
             # keep every state on the way to threshold (the foot of the action
             # potential decides activation times), 20% of the plateau and
-            # repolarisation, 2% of rest
+            # repolarisation, 4% of rest
             V = st[:, 0]
             u = rng.random(m.n)
             rest = np.abs(V + 85.4) < 1.0
             foot = (V > -84.4) & (V < -45.0) & (st[:, 8] > 0.05)      # h not yet inactivated
-            keep &= foot | (rest & (u < 0.02)) | (~rest & ~foot & (u < 0.2))
+            keep &= foot | (rest & (u < 0.04)) | (~rest & ~foot & (u < 0.2))
             idx = np.where(keep)[0]
             if len(idx) == 0:
                 continue
