@@ -413,7 +413,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain_fp32", choices=["plain_fp32", "fp64", "surrogate"])
+    ap.add_argument("--form", default="surrogate", choices=["plain_fp32", "fp64", "surrogate"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3"])
     ap.add_argument("--no-compare", action="store_true",
