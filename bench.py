@@ -28,6 +28,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "node-steps/s at 2M-node shell: surrogate vs plain FP32, act-time err ≤0.5 ms"
+WORKLOAD_TEXT = {
+    "shell_c2": "shell_c2: truncated prolate-ellipsoid shell, {n} nodes, {m} tets, ten Tusscher endo/M/epi "
+                "40/30/30, G_Ks 0.8->1.2 apex->base, 200 PMJ stimuli t~U(0,30) ms, 10 electrodes",
+    "slab_c0": "slab_c0: 1.0x1.0x0.2 cm slab, {n} nodes, {m} tets, ten Tusscher epi, corner stimulus, dt 0.02 ms",
+    "slab_c1": "slab_c1: 4.0x4.0x0.4 cm slab, {n} nodes, {m} tets, Mahajan, edge-strip stimulus, dt 0.01 ms",
+}
 UNIT = "node-steps/s"
 
 
@@ -99,13 +105,20 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic(kernel):
-    """DRAM bytes per launch from the committed ncu summary, if any."""
+def _traffic(kernel, form, cg_iters):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json); the CG launch's bytes grow with its
+    iteration count, so they are stored as prologue + per iteration."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f).get(kernel)
+            t = json.load(f)
     except Exception:
         return None
+    if kernel == "cg" and "cg" in t:
+        return t["cg"]["prologue_bytes"] + cg_iters * t["cg"]["per_iteration_bytes"]
+    if kernel == "ionic":
+        return t.get("surrogate" if form == "surrogate" else "ionic_plain_fp32" if form == "plain_fp32" else "-")
+    return None
 
 
 def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_every=10):
@@ -199,7 +212,7 @@ def run_ours(args, rank, world, local):
     prec = {"fp64": capi.FP64, "plain_fp32": capi.FP32, "surrogate": capi.SURROGATE}[args.form]
     if args.workload == "batch_c3":
         return run_batch(args, rank, world, local, dist, prec)
-    wl = W.shell_c2()
+    wl = {"shell_c2": W.shell_c2, "slab_c0": W.slab_c0, "slab_c1": W.slab_c1}[args.workload]()
     g = wl.create(prec, device=local)
     if prec == capi.SURROGATE:
         from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
@@ -211,6 +224,8 @@ def run_ours(args, rank, world, local):
     pre = int(round(args.t_start / wl.dt))
     for k in range(0, pre, 500):
         g.step(min(500, pre - k))
+    # the project's autotuner picks the launch shape (state is restored)
+    tuned = g.autotune(20) if not args.no_tune else None
     g.set_profiling(True)
     g.step(args.warmup)
     torch.cuda.synchronize()
@@ -248,28 +263,30 @@ def run_ours(args, rank, world, local):
     nnz = int(wl.mesh.n + 2 * _edge_count(wl.mesh))
     cg_per_solve = st["cg_iters"] / max(1, 2 * args.steps)
     kms = {"cg": st["cg_ms"], "ionic": st["ionic_ms"], "ecg": st["ecg_ms"]}
-    launches = {"cg": 2 * args.steps, "ionic": args.steps, "ecg": args.steps // 10}
+    ecg_every = max(1, int(round(1.0 / wl.dt)))
+    launches = {"cg": 2 * args.steps, "ionic": args.steps, "ecg": max(1, args.steps // ecg_every)}
     dom = max(kms, key=kms.get)
     per_launch_ms = kms[dom] / max(1, launches[dom])
-    alg = algorithmic_bytes(dom, n, nnz, cg_per_solve, rb)
+    nstate = capi.model_nstate(wl.model)
+    alg = algorithmic_bytes(dom, n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes),
+                            ecg_every=ecg_every)
     peak, peak_kind = _peaks()
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom),
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom, args.form, cg_per_solve) if wl.name == "shell_c2" else None,
             "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
             "kernel_ms": kms}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else ("bf16+f32" if prec == capi.SURROGATE else "f32"),
             "data": "synthetic",
-            "config": {"workload": f"shell_c2: truncated prolate-ellipsoid shell, {n} nodes, "
-                                   f"{wl.mesh.m} tets, ten Tusscher endo/M/epi 40/30/30, G_Ks 0.8->1.2 "
-                                   "apex->base, 200 PMJ stimuli t~U(0,30) ms, 10 electrodes",
+            "config": {"workload": WORKLOAD_TEXT[wl.name].format(n=n, m=wl.mesh.m),
                        "form": args.form, "dt_ms": wl.dt, "ionic_dt_ms": wl.ionic_dt,
                        "t_window_ms": [round((pre + args.warmup) * wl.dt, 3),
                                        round((pre + args.warmup + args.steps) * wl.dt, 3)],
                        "l2": "inputs > L2 (operators + states ~ 0.5 GB), no flush",
                        "cg_iters_per_solve": cg_per_solve, "newton_iters": st["newton_iters"],
+                       "launch_config": tuned[0] if tuned else g.launch_config(),
                        "fallback_fraction": st["fallback_nodes"] / float(n * args.steps),
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": int(st["launches"]),
@@ -280,11 +297,14 @@ def run_ours(args, rank, world, local):
         gp = wl.create(capi.FP32, device=local)
         for k in range(0, pre, 500):
             gp.step(min(500, pre - k))
+        if not args.no_tune:
+            gp.autotune(20)
         gp.step(args.warmup)
         torch.cuda.synchronize()
         stp = gp.step(args.steps)
         vp = n * args.steps * world / (stp["device_ms"] * 1e-3)
         line["config"]["plain_fp32"] = {"value": vp, "ms_per_step": stp["device_ms"] / args.steps,
+                                        "launch_config": gp.launch_config(),
                                         "cg_iters_per_solve": stp["cg_iters"] / max(1, 2 * args.steps)}
         line["config"]["speedup_vs_plain_fp32"] = value / vp
         gp.close()
@@ -346,17 +366,21 @@ def run_batch(args, rank, world, local, dist, prec):
 
 
 def run_accuracy(args, local):
-    """The shell run for args.accuracy ms in the FP64, plain FP32 and learned
-    forms; errors of the last two against FP64: activation time, APD90, Vm
-    L-infinity over 1 ms snapshots, pseudo-ECG relative L2."""
+    """The workload run for args.accuracy ms in the FP64, plain FP32 and (ten
+    Tusscher at dt = 0.1 ms, the step the network was trained for) learned
+    forms; errors against FP64: activation time, APD90, Vm L-infinity over
+    1 ms snapshots, pseudo-ECG relative L2."""
     import numpy as np
     import torch
     from ucla_cmg_b200 import capi, workloads as W
     from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
     torch.cuda.set_device(local)
-    wl = W.shell_c2()
+    wl = {"shell_c2": W.shell_c2, "slab_c0": W.slab_c0, "slab_c1": W.slab_c1}[args.workload]()
     steps = int(round(args.accuracy / wl.dt))
-    forms = (("fp64", capi.FP64), ("plain_fp32", capi.FP32), ("surrogate", capi.SURROGATE))
+    per_ms = max(1, int(round(1.0 / wl.dt)))
+    forms = [("fp64", capi.FP64), ("plain_fp32", capi.FP32)]
+    if wl.model == capi.TUSSCHER and abs(wl.dt - 0.1) < 1e-12:
+        forms.append(("surrogate", capi.SURROGATE))
     hs = {}
     for name, prec in forms:
         hs[name] = wl.create(prec, device=local)
@@ -364,14 +388,14 @@ def run_accuracy(args, local):
             Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(hs[name])
     res = {name: dict(ms=0.0, fb=0, vinf=0.0) for name, _ in forms}
     # the three runs advance in lockstep; Vm is compared every 1 ms
-    for k in range(0, steps, 10):
+    for k in range(0, steps, per_ms):
         V = {}
         for name, _ in forms:
-            st = hs[name].step(min(10, steps - k))
+            st = hs[name].step(min(per_ms, steps - k))
             res[name]["ms"] += st["device_ms"]
             res[name]["fb"] += st["fallback_nodes"]
             V[name] = hs[name].voltage()
-        for name in ("plain_fp32", "surrogate"):
+        for name, _ in forms[1:]:
             res[name]["vinf"] = max(res[name]["vinf"], float(np.abs(V[name] - V["fp64"]).max()))
     for name, _ in forms:
         r = res[name]
@@ -380,8 +404,8 @@ def run_accuracy(args, local):
         r["fb"] /= float(wl.mesh.n * steps)
         hs[name].close()
     ref = res["fp64"]
-    out = {"workload": "shell_c2", "t_ms": args.accuracy, "n_nodes": int(wl.mesh.n)}
-    for name in ("fp64", "plain_fp32", "surrogate"):
+    out = {"workload": wl.name, "t_ms": args.accuracy, "n_nodes": int(wl.mesh.n), "dt_ms": wl.dt}
+    for name, _ in forms:
         r = res[name]
         e = {"node_steps_per_s": wl.mesh.n * steps / (r["ms"] * 1e-3), "fallback_fraction": r["fb"]}
         if name != "fp64":
@@ -392,7 +416,10 @@ def run_accuracy(args, local):
             e.update({"activated": float((r["ta"] >= 0).mean()), "activated_fp64": float((ref["ta"] >= 0).mean()),
                       "act_err_ms": {"mean": float(da.mean()), "p99": float(np.percentile(da, 99)), "max": float(da.max())},
                       "apd90_err_ms": {"n": int(ab.sum()), "mean": float(dp.mean()) if ab.any() else None,
-                                       "max": float(dp.max()) if ab.any() else None},
+                                       "p99": float(np.percentile(dp, 99)) if ab.any() else None,
+                                       "max": float(dp.max()) if ab.any() else None,
+                                       "repolarised": float((r["apd"] > 0).mean()),
+                                       "repolarised_fp64": float((ref["apd"] > 0).mean())},
                       "vm_linf_mv": r["vinf"],
                       "ecg_rel_l2": float(np.linalg.norm(r["ecg"] - ref["ecg"]) / np.linalg.norm(ref["ecg"]))})
         out[name] = e
@@ -415,7 +442,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="surrogate", choices=["plain_fp32", "fp64", "surrogate"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3"])
+    ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3", "slab_c0", "slab_c1"])
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-compare", action="store_true",
                     help="surrogate form: skip the plain FP32 run over the same window")
     ap.add_argument("--t-start", type=float, default=40.0,
