@@ -231,15 +231,17 @@ int  ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres);
 int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_t *inst_blk);
 
 /* Launch shape of ep_step (no reference counterpart).  cg_block: threads
- * per CTA of the persistent CG launch (128 or 256); cg_per_sm: its CTAs per
+ * per CTA of the persistent CG launch (128, 256, 512 or 768); cg_per_sm: its CTAs per
  * SM (0 = as many as are co-resident); ionic_block: threads per CTA of the
  * ionic kernel (64 or 128); graph_steps: 0 launches every kernel from the
  * host, k > 0 replays the steps from an instantiated CUDA graph of k steps
  * (rounded up to a multiple of the ECG interval); ionic_min_ctas: FP32
  * ionic kernel compiled for at least 3 or 4 resident 128-thread CTAs per SM
- * (fewer registers per thread), 0 = the compiler's register choice. */
+ * (fewer registers per thread), 0 = the compiler's register choice;
+ * cg_batch: SELL columns whose gathers the CG kernel issues together (4 or
+ * 8; 8 keeps more loads in flight at a larger register budget). */
 typedef struct ep_launch_config {
-    int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas;
+    int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas, cg_batch;
 } ep_launch_config;
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);
@@ -325,10 +327,7 @@ typedef struct ep_surrogate_desc {
                                        it runs the plain model */
     int32_t hybrid_substeps;        /* v_update 2: gate/V sub-steps per global
                                        step (0: the handle's ionic sub-steps) */
-    int32_t v_update;               /* 0: V' = V + dV from the network;
-                                       1: V' = V + dt dV/dt(V + dV/2, (s + s')/2),
-                                       the cell model's own current balance at
-                                       the step midpoint;
+    int32_t v_update;               /* 0: V and every state from the network;
                                        2: only the six Newton concentrations
                                        (Ki, Nai, Cai, Cass, CaSR, R') come from
                                        the network (interpolated over the

@@ -88,15 +88,15 @@ struct ep_handle {
     std::vector<int> pkind;              // kernel class started at each event
     long long launches = 0;
     // learned ionic step (EP_SURROGATE)
-    DBuf sg_wimg, sg_aux, sg_list, sg_count, sg_err;
-    int has_surrogate = 0;
+    DBuf sg_wimg, sg_aux, sg_list, sg_count, sg_err, sg_pred, sg_take;
+    int has_surrogate = 0, sg_vupdate = 0;
     // independent instances sharing the launches (ep_batch_create)
     int ninst = 1;
     std::vector<int> inst_row;           // ninst + 1 node offsets
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
-    int cg_per_sm = 0, ionic_block = 128, ionic_min = 0, graph_steps = 0;
+    int cg_per_sm = 0, cg_batch = 4, ionic_block = 128, ionic_min = 0, graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
@@ -289,8 +289,8 @@ extern "C" int ep_batch_plan(int32_t ninst, const int32_t *inst_row, int32_t gri
 // (re)size the CG launch for the handle's launch shape: grid, CTA groups,
 // partials, barriers and per-instance results
 static int plan_cg(ep_handle *h) {
-    int rc = h->precision == EP_FP64 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm)
-                                     : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm);
+    int rc = h->precision == EP_FP64 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch)
+                                     : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch);
     if (rc) return rc;
     if (h->ninst > h->cg_grid) {
         set_error("%d instances but only %d CTAs in the persistent launch", h->ninst, h->cg_grid);
@@ -356,6 +356,8 @@ static void fill_surrogate_args(ep_handle *h, const IonicArgs<float> &ia, Surrog
     sa.fallback_count = h->sg_count.as<int>();
     sa.status = h->status.as<DevStatus>();
     sa.err = h->sg_err.as<unsigned int>();
+    sa.pred = h->sg_pred.as<float>();
+    sa.take = h->sg_take.as<uint8_t>();
 }
 
 // the learned ionic phase: tensor-core MLP for the nodes inside the training
@@ -370,6 +372,7 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     fill_surrogate_args(h, ia, sa);
     int rc = launch_surrogate(sa, h->stream);
     if (rc) return rc;
+    if (h->sg_vupdate == 2 && (rc = launch_hybrid(sa, h->stream))) return rc;
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
@@ -402,12 +405,12 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     int rc;
     for (int s = 0; s < nsteps; s++) {
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch))) return rc;
         if ((rc = mark(h, ne, K_IONIC))) return rc;
         if constexpr (sizeof(R) == 4) {
             if (h->precision == EP_SURROGATE) {
                 if ((rc = launch_learned_phase(h, ia))) return rc;
-                h->launches += 2;
+                h->launches += h->sg_vupdate == 2 ? 3 : 2;
             } else if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) {
                 return rc;
             }
@@ -415,7 +418,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch))) return rc;
         if ((rc = mark(h, ne, K_OTHER))) return rc;
         launch_step_inc(h->d_step.as<long long>(), h->stream);
         h->launches += 4;
@@ -942,11 +945,11 @@ int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
     if (h->precision == EP_FP64) {
         CGArgs<double> ca;
         fill_cg_args<double>(h, ca);
-        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream);
+        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch);
     } else {
         CGArgs<float> ca;
         fill_cg_args<float>(h, ca);
-        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream);
+        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch);
     }
     if (rc) return rc;
     double last[2];
@@ -1013,7 +1016,7 @@ static int pack_surrogate(const ep_surrogate_desc *d, std::vector<unsigned short
     }
     aux.nah_max = d->nah_max;
     aux.log_mask = d->log_mask & ((1u << SG_NF) - 1u) & ~1u;   // V stays linear
-    EP_CHECK_ARG(d->v_update >= 0 && d->v_update <= 2, "v_update must be 0, 1 or 2");
+    EP_CHECK_ARG(d->v_update == 0 || d->v_update == 2, "v_update must be 0 or 2");
     aux.v_update = d->v_update;
     // outputs the update reads: the six Newton concentrations (stored states
     // Ki 1, Nai 2, Cai 3, Cass 10, CaSR 17, R' 18) in the hybrid form
@@ -1041,8 +1044,13 @@ int ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d) {
         if ((rc = h->sg_count.alloc(sizeof(int)))) return rc;
         if ((rc = h->sg_err.alloc(sizeof(unsigned int)))) return rc;
     }
+    if (aux.v_update == 2 && !h->sg_pred.p) {
+        if ((rc = h->sg_pred.alloc(sizeof(float) * 6 * (size_t)h->pitch))) return rc;
+        if ((rc = h->sg_take.alloc((size_t)h->pitch))) return rc;
+    }
     EP_CUDA(cudaMemset(h->sg_err.p, 0, sizeof(unsigned int)));
     h->has_surrogate = 1;
+    h->sg_vupdate = aux.v_update;
     return EP_OK;
 }
 
@@ -1086,6 +1094,7 @@ int ep_set_profiling(ep_handle *h, int on) {
 int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     EP_CHECK_ARG(h && cfg, "null argument");
     cfg->cg_block = h->cg_block;
+    cfg->cg_batch = h->cg_batch;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1098,7 +1107,9 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
 
 int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(h && cfg, "null argument");
-    EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256, "cg_block must be 128 or 256");
+    EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256 || cfg->cg_block == 512 || cfg->cg_block == 768,
+                 "cg_block must be 128, 256, 512 or 768");
+    EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8, "cg_batch must be 4 or 8");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
     EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
@@ -1107,12 +1118,13 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     drop_graph(h);
-    const int ob = h->cg_block, op = h->cg_per_sm;
+    const int ob = h->cg_block, op = h->cg_per_sm, obt = h->cg_batch;
     h->cg_block = cfg->cg_block;
     h->cg_per_sm = cfg->cg_per_sm;
+    h->cg_batch = cfg->cg_batch;
     int rc = plan_cg(h);
     if (rc) {
-        h->cg_block = ob; h->cg_per_sm = op;
+        h->cg_block = ob; h->cg_per_sm = op; h->cg_batch = obt;
         plan_cg(h);
         return rc;
     }
@@ -1175,6 +1187,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     ep_launch_config cur;
     cur.cg_block = h->cg_block;
+    cur.cg_batch = h->cg_batch;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
     cur.ionic_min_ctas = h->ionic_min;
@@ -1200,17 +1213,24 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
         return EP_ERR_CUDA;
     }
     // coordinate descent: CG shape, then ionic block, then graphs
-    for (int blk : {128, 256}) {
-        int maxper = 1;
-        if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper) : cg_max_per_sm<float>(blk, &maxper)))
-            continue;
-        for (int per = 1; per <= std::min(maxper, 8); per++) {
-            ep_launch_config c = b;
-            c.cg_block = blk; c.cg_per_sm = per;
-            if (c.cg_block == b.cg_block && c.cg_per_sm == b.cg_per_sm) continue;
-            if (per * nsm < h->ninst) continue;
-            const double t = trial(c);
-            if (t >= 0 && t < t_best) { t_best = t; b = c; }
+    // CG: gather width x CTA size x CTAs per SM (all that fit, or half:
+    // fewer CTAs make the grid barrier cheaper)
+    const ep_launch_config cg0 = b;
+    for (int nb : {4, 8}) {
+        for (int blk : {128, 256, 512, 768}) {
+            int maxper = 0;
+            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb)
+                                         : cg_max_per_sm<float>(blk, &maxper, nb)))
+                continue;
+            maxper = std::min(maxper, 8);
+            for (int per : {maxper, maxper / 2}) {
+                if (per < 1 || per * nsm < h->ninst) continue;
+                ep_launch_config c = cg0;
+                c.cg_block = blk; c.cg_per_sm = per; c.cg_batch = nb;
+                if (c.cg_block == cg0.cg_block && c.cg_per_sm == cg0.cg_per_sm && c.cg_batch == cg0.cg_batch) continue;
+                const double t = trial(c);
+                if (t >= 0 && t < t_best) { t_best = t; b = c; }
+            }
         }
     }
     for (int ib : {64, 128}) {

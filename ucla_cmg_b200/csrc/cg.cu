@@ -73,29 +73,29 @@ __device__ __forceinline__ void grid_total(const double *partial, int stride, in
     __syncthreads();
 }
 
-// Row sums of one SELL slice, four slice columns at a time: the column and
+// Row sums of one SELL slice, NB slice columns at a time: the column and
 // value loads of a group are issued together, then the gathers, so each lane
-// has a dozen independent loads in flight (at one lane per row the kernel is
+// has 3 NB independent loads in flight (at one lane per row the kernel is
 // bound by memory latency, not bandwidth).  The products are still added in
-// column order, so the sums are those of the plain loop.
-template <typename R, typename F>
+// column order, so the sums are those of the plain loop whatever NB is.
+template <int NB, typename R, typename F>
 __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R *__restrict__ val, int beg, int w,
                                            int lane, F gather) {
     R acc = R(0);
     int k = 0;
-    for (; k + 4 <= w; k += 4) {
-        int c[4];
-        R v[4], g[4];
+    for (; k + NB <= w; k += NB) {
+        int c[NB];
+        R v[NB], g[NB];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < NB; u++) {
             const int idx = beg + (k + u) * kSlice + lane;
             c[u] = __ldg(col + idx);
             v[u] = __ldg(val + idx);
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) g[u] = gather(c[u]);
+        for (int u = 0; u < NB; u++) g[u] = gather(c[u]);
 #pragma unroll
-        for (int u = 0; u < 4; u++) acc += v[u] * g[u];
+        for (int u = 0; u < NB; u++) acc += v[u] * g[u];
     }
     for (; k < w; k++) {
         const int idx = beg + k * kSlice + lane;
@@ -104,8 +104,10 @@ __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R 
     return acc;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256, 6) k_cn_half(const CGArgs<R> a) {
+// register budget: NB = 4 takes 42 (six 256-thread CTAs, or two of 768, per
+// SM); NB = 8 takes 64 (four 256-thread CTAs) for twice the loads in flight
+template <typename R, int NB>
+__global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_half(const CGArgs<R> a) {
     const int lane = threadIdx.x & 31;
     const int G = gridDim.x;                 // partial-array stride
     // this CTA's instance: its rows, its CTA group and its barrier
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(256, 6) k_cn_half(const CGArgs<R> a) {
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
                 const R *pcc = pc;
-                const R q = slice_row_sum(a.col, a.Aval, beg, w, lane, [&](int c) {
+                const R q = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, [&](int c) {
                     return pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pcc + c));
                 });
                 if (row >= rb && row < re) {
@@ -238,18 +240,19 @@ __global__ void __launch_bounds__(256, 6) k_cn_half(const CGArgs<R> a) {
 }
 
 template <typename R>
-int cg_max_per_sm(int block, int *per) {
-    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R>, block, 0));
-    if (*per < 1) { set_error("CG kernel cannot be resident"); return EP_ERR_CUDA; }
+int cg_max_per_sm(int block, int *per, int batch) {
+    if (batch == 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 8>, block, 0));
+    else EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 4>, block, 0));
+    if (*per < 1) { set_error("CG kernel cannot be resident with %d threads per CTA", block); return EP_ERR_CUDA; }
     return EP_OK;
 }
 
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm) {
+int cg_grid_size(int block, int *grid, int per_sm, int batch) {
     int dev = 0, nsm = 0, per = 0;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int rc = cg_max_per_sm<R>(block, &per);
+    int rc = cg_max_per_sm<R>(block, &per, batch);
     if (rc) return rc;
     if (per_sm > 0 && per_sm < per) per = per_sm;
     *grid = nsm * per;
@@ -257,7 +260,7 @@ int cg_grid_size(int block, int *grid, int per_sm) {
 }
 
 template <typename R>
-int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s) {
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -268,16 +271,17 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R>, a));
+    if (batch == 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 8>, a));
+    else EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 4>, a));
     return EP_OK;
 }
 
-template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t);
-template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t);
-template int cg_grid_size<float>(int, int *, int);
-template int cg_grid_size<double>(int, int *, int);
-template int cg_max_per_sm<float>(int, int *);
-template int cg_max_per_sm<double>(int, int *);
+template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t, int);
+template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t, int);
+template int cg_grid_size<float>(int, int *, int, int);
+template int cg_grid_size<double>(int, int *, int, int);
+template int cg_max_per_sm<float>(int, int *, int);
+template int cg_max_per_sm<double>(int, int *, int);
 
 // ---------------------------------------------------------------------------
 // pseudo-ECG: out[k] = sum_i W[k * wpitch + i] V[i], FP64 accumulation.

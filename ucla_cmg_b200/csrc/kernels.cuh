@@ -105,13 +105,14 @@ template <typename R> struct CGArgs {
     const int *inst_row, *inst_blk;
 };
 
+// batch: SELL columns gathered per group (4 or 8; two register budgets)
 template <typename R>
-int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s);
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch = 4);
 // CTAs of the persistent launch: per_sm (0 = as many as fit) x SM count
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm = 0);
+int cg_grid_size(int block, int *grid, int per_sm = 0, int batch = 4);
 template <typename R>
-int cg_max_per_sm(int block, int *per);
+int cg_max_per_sm(int block, int *per, int batch = 4);
 
 // ECG_k = sum_i W[k n + i] V[i] (ComputeECG.h:172-189 in per-node form),
 // deterministic two-level reduction, written to out[k].

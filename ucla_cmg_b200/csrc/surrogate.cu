@@ -157,11 +157,14 @@ __device__ __forceinline__ bool wait_commit(uint64_t *bar, uint32_t &phase, unsi
     return true;
 }
 
-// hidden-layer epilogue: TMEM -> +bias -> tanh -> BF16 A row (K = 128 layout)
-__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *__restrict__ bias, unsigned char *A) {
-    const int r = threadIdx.x;
+// hidden-layer epilogue: TMEM -> +bias -> tanh -> BF16 A row (K = 128
+// layout).  Row r's 128 columns are split between the two warps that share
+// its TMEM lane quarter: half h takes columns [64 h, 64 h + 64).
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *__restrict__ bias, unsigned char *A,
+                                                int r, int half) {
 #pragma unroll 1
-    for (int q = 0; q < SG_H / 32; q++) {
+    for (int qq = 0; qq < 2; qq++) {
+        const int q = 2 * half + qq;
         uint32_t v[32];
         tmem_ld32(tmem_row + 32u * q, v);
         uint32_t w[16];
@@ -180,9 +183,15 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *
     }
 }
 
-__global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
+// The network over tiles of 128 nodes, 256 threads per CTA.  Threads
+// 0..127 own one node each (features, the output layer, the envelope
+// decision); all eight warps share the hidden-layer epilogues (warp w reads
+// TMEM lane quarter w % 4, column half w / 4).
+__global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = tid & (SG_M - 1), half = tid >> 7;
+    const bool owner = half == 0;                 // warp-uniform
     uint64_t *bar = (uint64_t *)(smem + OFF_MISC);
     uint32_t *holder = (uint32_t *)(smem + OFF_MISC + 16);
     unsigned char *A = smem + OFF_A;
@@ -201,7 +210,7 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *holder;
-    const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+    const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
     const uint32_t d_hid = tmem, d_out = tmem + 128u;
     const uint32_t sW1 = smem_u32(smem + OFF_W1), sW2 = smem_u32(smem + OFF_W2);
     const uint32_t sW3 = smem_u32(smem + OFF_W3), sW4 = smem_u32(smem + OFF_W4);
@@ -214,59 +223,56 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
     const int ntiles = (a.n + SG_M - 1) / SG_M;
 
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int i = tile * SG_M + tid;
-        const bool valid = i < a.n;
+        const int i = tile * SG_M + row;
+        const bool valid = owner && i < a.n;
         float x[SG_NF];
-        float xn[SG_KIN];
         bool inside = false;
-        float istim = 0.f;
-        const float *c = a.consts;
-        float gks_i = 1.f;
+        if (owner) {
+            float xn[SG_KIN];
 #pragma unroll
-        for (int k = 0; k < SG_KIN; k++) xn[k] = 0.f;
-        if (valid && raw) {
+            for (int k = 0; k < SG_KIN; k++) xn[k] = 0.f;
+            if (valid && raw) {
 #pragma unroll
-            for (int k = 0; k < SG_KIN; k++) xn[k] = a.rawX[(size_t)i * SG_KIN + k];
-        } else if (valid) {
-            x[0] = a.V[i];
+                for (int k = 0; k < SG_KIN; k++) xn[k] = a.rawX[(size_t)i * SG_KIN + k];
+            } else if (valid) {
+                x[0] = a.V[i];
 #pragma unroll
-            for (int k = 0; k < 18; k++) x[k + 1] = a.S[(size_t)k * a.pitch + i];
-            const int ty = a.type ? a.type[i] : 0;
-            c = a.consts + (size_t)ty * a.nconst;
-            gks_i = a.gks ? a.gks[i] : 1.f;
-            if (a.stim_head) {
-                int k = a.stim_head[i];
-                long long best = -1;
-                while (k >= 0) {
-                    const long long on = a.stim_on[k], off = a.stim_off[k];
-                    if (step >= on && step < off && on > best) { best = on; istim = a.stim_amp[k]; }
-                    k = a.stim_next[k];
+                for (int k = 0; k < 18; k++) x[k + 1] = a.S[(size_t)k * a.pitch + i];
+                const int ty = a.type ? a.type[i] : 0;
+                const float *c = a.consts + (size_t)ty * a.nconst;
+                float istim = 0.f;
+                if (a.stim_head) {
+                    int k = a.stim_head[i];
+                    long long best = -1;
+                    while (k >= 0) {
+                        const long long on = a.stim_on[k], off = a.stim_off[k];
+                        if (step >= on && step < off && on > best) { best = on; istim = a.stim_amp[k]; }
+                        k = a.stim_next[k];
+                    }
+                }
+                x[19] = istim / (a.Cm * a.Xi);
+                x[20] = c[15] * (a.gks ? a.gks[i] : 1.f);
+                x[21] = c[20];
+                x[22] = c[53];
+                inside = (istim == 0.f);
+                const float m = x[7], h = x[8];
+                inside = inside && (m * m * m * h <= aux->nah_max);
+                const unsigned int lm = aux->log_mask;
+#pragma unroll
+                for (int k = 0; k < SG_NF; k++) {
+                    // quantities spanning decades enter as logarithms
+                    const float xt = ((lm >> k) & 1u) ? __logf(fmaxf(x[k], 1e-30f)) : x[k];
+                    inside = inside && (xt >= aux->env_lo[k]) && (xt <= aux->env_hi[k]);
+                    xn[k] = (xt - aux->in_mean[k]) * aux->in_rstd[k];
                 }
             }
-            x[19] = istim / (a.Cm * a.Xi);
-            x[20] = c[15] * gks_i;
-            x[21] = c[20];
-            x[22] = c[53];
-            inside = (istim == 0.f);
-            const float m = x[7], h = x[8];
-            inside = inside && (m * m * m * h <= aux->nah_max);
-            const unsigned int lm = aux->log_mask;
-#pragma unroll
-            for (int k = 0; k < SG_NF; k++) {
-                // quantities spanning decades enter as logarithms
-                const float xt = ((lm >> k) & 1u) ? __logf(fmaxf(x[k], 1e-30f)) : x[k];
-                inside = inside && (xt >= aux->env_lo[k]) && (xt <= aux->env_hi[k]);
-                xn[k] = (xt - aux->in_mean[k]) * aux->in_rstd[k];
-            }
-        }
-        // input row (K = 32 layout)
-        {
+            // input row (K = 32 layout)
             uint32_t w[16];
 #pragma unroll
             for (int j = 0; j < 16; j++) w[j] = pack_bf16(xn[2 * j], xn[2 * j + 1]);
 #pragma unroll
             for (int cch = 0; cch < 4; cch++) {
-                uint4 *dst = (uint4 *)(A + ((tid >> 3) * (SG_KIN / 8) + cch) * 128 + (tid & 7) * 16);
+                uint4 *dst = (uint4 *)(A + ((row >> 3) * (SG_KIN / 8) + cch) * 128 + (row & 7) * 16);
                 *dst = make_uint4(w[4 * cch], w[4 * cch + 1], w[4 * cch + 2], w[4 * cch + 3]);
             }
         }
@@ -284,7 +290,7 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
                 issue_layer(d_hid, sA, sW[l], l == 0 ? SG_KIN : SG_H, SG_H, bar);
             }
             ok = wait_commit(bar, phase, a.err);
-            if (ok) hidden_epilogue(d_hid + lane_off, bias[l], A);
+            if (ok) hidden_epilogue(d_hid + lane_off, bias[l], A, row, half);
         }
         if (!ok) break;
         // output layer (K = 128, N = 32)
@@ -296,6 +302,7 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
             issue_layer(d_out, sA, sW4, SG_H, SG_NOUT, bar);
         }
         if (!wait_commit(bar, phase, a.err)) break;
+        if (!owner) continue;
         uint32_t yv[32];
         tmem_ld32(d_out + lane_off, yv);
         tc_fence_before();
@@ -314,76 +321,40 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
                 const float sc = aux->out_scale[j];
                 d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
             }
+            const unsigned int lm = aux->log_mask;
+            if (aux->v_update == 2) a.take[i] = out_ok ? 1 : 0;
             if (!out_ok) {
                 const int slot = atomicAdd(a.fallback_count, 1);
                 a.fallback_list[slot] = i;
                 my_fb++;
-                continue;
-            }
-            const unsigned int lm = aux->log_mask;
-            float sn[18];
+            } else if (aux->v_update == 2) {
+                // the new concentrations; k_hybrid advances gates and V
+                const int cslot[6] = {0, 1, 2, 9, 16, 17};
 #pragma unroll
-            for (int k = 0; k < 18; k++) {
-                // log-scaled states are updated multiplicatively: x' = x exp(d)
-                const float xk = x[k + 1];
-                sn[k] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
-            }
-            const float V0 = x[0];
-            Track tr = {-1.f, -1.f, -1.f, 1e30f};
-            bool dirty = false;
-            const bool trk = a.track != nullptr;
-            if (trk) tr = a.track[i];
-            if (aux->v_update == 2) {
-                // the network replaces the Newton solve of Compute_Ion: the six
-                // concentrations move from their start to the predicted end
-                // values over the sub-steps (geometrically for log-scaled
-                // ones); gates and V take the reference's sub-step formulas
-                float s[18];
-#pragma unroll
-                for (int k = 0; k < 18; k++) s[k] = x[k + 1];
-                const int slot[6] = {0, 1, 2, 9, 16, 17};
-                const int ns = aux->hyb_sub > 0 ? aux->hyb_sub : a.nsub;
-                const float hu = (float)a.t_per_step / (float)ns;
-                const float rdt = 1.f / (float)a.t_per_step;
-                float V = V0, tsum = 0.f;
-                double tsub = t0;
-                for (int k = 0; k < ns; k++) {
-                    const float h = aux->hyb_sub > 0 ? hu : a.sub_dt[k];
-                    tt_gate_step(s, V, h, c);
-                    tsum += h;
-                    const float w = fminf(tsum * rdt, 1.f);
-#pragma unroll
-                    for (int j = 0; j < 6; j++) {
-                        const int q = slot[j];
-                        const float a0 = x[q + 1], a1 = sn[q];
-                        s[q] = ((lm >> (q + 1)) & 1u) ? a0 * __powf(a1 / a0, w) : a0 + w * (a1 - a0);
-                    }
-                    const float v1 = V + h * tt_dvdt<float>(V, s, c, 0.f, gks_i);
-                    if (trk && tr.t_rep < 0.f) track_interval(tr, dirty, V, v1, tsub, h, a.act_thr);
-                    V = v1;
-                    tsub += (double)h;
+                for (int j = 0; j < 6; j++) {
+                    const int q = cslot[j];
+                    const float xk = x[q + 1];
+                    a.pred[(size_t)j * a.pitch + i] = ((lm >> (q + 1)) & 1u) ? xk * __expf(d[q + 1]) : xk + d[q + 1];
                 }
-#pragma unroll
-                for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = s[k];
-                a.V[i] = V;
             } else {
-                float V1 = V0 + d[0];
-                if (aux->v_update == 1) {
-                    // midpoint rule on the model's own current balance: the
-                    // network's dV only places the midpoint; the states there
-                    // are the mean of the old and the predicted new states
-                    float sm[18];
+                // every quantity from the network
 #pragma unroll
-                    for (int k = 0; k < 18; k++) sm[k] = 0.5f * (x[k + 1] + sn[k]);
-                    const float dt = (float)a.t_per_step;
-                    V1 = V0 + dt * tt_dvdt<float>(V0 + 0.5f * d[0], sm, c, 0.f, gks_i);
+                for (int k = 0; k < 18; k++) {
+                    // log-scaled states are updated multiplicatively: x' = x exp(d)
+                    const float xk = x[k + 1];
+                    a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
                 }
-#pragma unroll
-                for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = sn[k];
+                const float V0 = x[0], V1 = x[0] + d[0];
                 a.V[i] = V1;
-                if (trk && tr.t_rep < 0.f) track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
+                if (a.track) {
+                    Track tr = a.track[i];
+                    if (tr.t_rep < 0.f) {
+                        bool dirty = false;
+                        track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
+                        if (dirty) a.track[i] = tr;
+                    }
+                }
             }
-            if (dirty) a.track[i] = tr;
         }
     }
     // count fallback node-steps
@@ -393,6 +364,60 @@ __global__ void __launch_bounds__(128, 2) k_surrogate(const SurrogateArgs a) {
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, SG_TMEM_COLS);
+}
+
+// The hybrid form's physics for the nodes the network took: the reference's
+// gate update and current balance over the sub-steps, with the six
+// concentrations moving from their start to the network's end values
+// (geometrically for the log-scaled Cai and Cass).  One thread per node.
+__global__ void __launch_bounds__(128, 4) k_hybrid(const SurrogateArgs a) {
+    const SurrogateAux *aux = a.aux;
+    const long long step = *a.step_ptr;
+    const double t0 = (double)step * a.t_per_step;
+    const unsigned int lm = aux->log_mask;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        if (!a.take[i]) continue;
+        float s[18], c0[6], c1[6];
+#pragma unroll
+        for (int k = 0; k < 18; k++) s[k] = a.S[(size_t)k * a.pitch + i];
+        const int cslot[6] = {0, 1, 2, 9, 16, 17};
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            c0[j] = s[cslot[j]];
+            c1[j] = a.pred[(size_t)j * a.pitch + i];
+        }
+        const int ty = a.type ? a.type[i] : 0;
+        const float *c = a.consts + (size_t)ty * a.nconst;
+        const float gks_i = a.gks ? a.gks[i] : 1.f;
+        Track tr = {-1.f, -1.f, -1.f, 1e30f};
+        bool dirty = false;
+        const bool trk = a.track != nullptr;
+        if (trk) tr = a.track[i];
+        const int ns = aux->hyb_sub > 0 ? aux->hyb_sub : a.nsub;
+        const float hu = (float)a.t_per_step / (float)ns;
+        const float rdt = 1.f / (float)a.t_per_step;
+        float V = a.V[i], tsum = 0.f;
+        double tsub = t0;
+        for (int k = 0; k < ns; k++) {
+            const float h = aux->hyb_sub > 0 ? hu : a.sub_dt[k];
+            tt_gate_step(s, V, h, c);
+            tsum += h;
+            const float w = fminf(tsum * rdt, 1.f);
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                const int q = cslot[j];
+                s[q] = ((lm >> (q + 1)) & 1u) ? c0[j] * __powf(c1[j] / c0[j], w) : c0[j] + w * (c1[j] - c0[j]);
+            }
+            const float v1 = V + h * tt_dvdt<float>(V, s, c, 0.f, gks_i);
+            if (trk && tr.t_rep < 0.f) track_interval(tr, dirty, V, v1, tsub, h, a.act_thr);
+            V = v1;
+            tsub += (double)h;
+        }
+#pragma unroll
+        for (int k = 0; k < 18; k++) a.S[(size_t)k * a.pitch + i] = s[k];
+        a.V[i] = V;
+        if (dirty) a.track[i] = tr;
+    }
 }
 
 int launch_surrogate(const SurrogateArgs &a, cudaStream_t s) {
@@ -407,7 +432,14 @@ int launch_surrogate(const SurrogateArgs &a, cudaStream_t s) {
     const int ntiles = (a.n + SG_M - 1) / SG_M;
     const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
     if (grid <= 0) return EP_OK;
-    k_surrogate<<<grid, 128, SG_SMEM, s>>>(a);
+    k_surrogate<<<grid, SG_THREADS, SG_SMEM, s>>>(a);
+    EP_CUDA(cudaGetLastError());
+    return EP_OK;
+}
+
+int launch_hybrid(const SurrogateArgs &a, cudaStream_t s) {
+    if (a.n <= 0) return EP_OK;
+    k_hybrid<<<(a.n + 127) / 128, 128, 0, s>>>(a);
     EP_CUDA(cudaGetLastError());
     return EP_OK;
 }

@@ -6,6 +6,7 @@
 namespace ep {
 
 constexpr int SG_M = 128;        // nodes per tile = MMA M = TMEM lanes
+constexpr int SG_THREADS = 256;  // threads per CTA of the network kernel
 constexpr int SG_H = 128;        // hidden width
 constexpr int SG_KIN = 32;       // padded input width
 constexpr int SG_NOUT = 32;      // padded output width
@@ -30,7 +31,7 @@ struct SurrogateAux {
     float env_lo[SG_KIN], env_hi[SG_KIN];   // in the transformed (log) space
     float nah_max;
     unsigned int log_mask;      // bit k: feature k (and state output k) is log-scaled
-    int v_update;               // 0: V += network dV; 1: midpoint current balance;
+    int v_update;               // 0: every quantity from the network;
                                 // 2: network concentrations, reference gates and V
 };
 
@@ -65,9 +66,14 @@ struct SurrogateArgs {
     // raw mode (tests): X [n x 32] normalised inputs -> Y [n x 32] raw outputs
     const float *rawX;
     float *rawY;
+    // hybrid form: the network's new concentrations [6][pitch] and which
+    // nodes it took (1) or handed to the plain model (0)
+    float *pred;
+    uint8_t *take;
 };
 
 int launch_surrogate(const SurrogateArgs &a, cudaStream_t s);
+int launch_hybrid(const SurrogateArgs &a, cudaStream_t s);
 size_t surrogate_smem_bytes();
 
 }  // namespace ep
