@@ -156,3 +156,23 @@ def test_autotune_restores_state(gpu):
     b.step(50)
     assert np.all(np.isfinite(b.voltage()))
     b.close()
+
+
+def test_graph_survives_state_upload(gpu):
+    """Setting the voltage and the states between replays writes into the
+    same device buffers, so the instantiated graph stays valid and the run
+    matches one without graphs."""
+    insts = _instances()
+    blks = _stims(insts)
+    out = []
+    for gs in (0, 20):
+        b = _batch(insts, blks, capi.FP32)
+        b.set_launch_config(graph_steps=gs)
+        b.step(60)
+        S, V = b.states(), b.voltage()
+        b.set_states(S)
+        b.set_voltage(V)
+        b.step(60)
+        out.append(b.voltage())
+        b.close()
+    assert np.array_equal(out[0], out[1])

@@ -101,6 +101,8 @@ struct ep_handle {
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
     DBuf ecg_slot;                       // next ECG sample slot (device counter)
+    void *pin = nullptr;                 // pinned host staging for state transfers
+    size_t pin_bytes = 0;
 };
 
 namespace {
@@ -542,6 +544,7 @@ void ep_destroy(ep_handle *h) {
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->pin) cudaFreeHost(h->pin);
     delete h;
     cudaSetDevice(cur);
 }
@@ -740,23 +743,106 @@ int ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres) {
 int ep_num_nodes(const ep_handle *h) { return h ? h->n : EP_ERR_ARG; }
 int ep_num_states(const ep_handle *h) { return h ? h->nstate : EP_ERR_ARG; }
 
+}  // extern "C"
+
+// Host <-> device state transfers go through one pinned staging buffer of
+// the handle (grown on demand) and copy into the existing device buffers:
+// the buffers never move after ep_create, which captured graphs rely on.
+static void *stage(ep_handle *h, size_t bytes) {
+    if (bytes > h->pin_bytes) {
+        if (h->pin) cudaFreeHost(h->pin);
+        h->pin = nullptr;
+        h->pin_bytes = 0;
+        if (cudaMallocHost(&h->pin, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMallocHost(%zu) failed", bytes);
+            return nullptr;
+        }
+        h->pin_bytes = bytes;
+    }
+    return h->pin;
+}
+
+template <typename R>
+static int put_voltage(ep_handle *h, const double *V) {
+    R *st = (R *)stage(h, sizeof(R) * h->n);
+    if (!st) return EP_ERR_NOMEM;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < h->n; i++) st[i] = (R)V[i];
+    EP_CUDA(cudaMemcpyAsync(h->V.p, st, sizeof(R) * h->n, cudaMemcpyHostToDevice, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    return EP_OK;
+}
+
+template <typename R>
+static int get_voltage(ep_handle *h, double *V) {
+    R *st = (R *)stage(h, sizeof(R) * h->n);
+    if (!st) return EP_ERR_NOMEM;
+    EP_CUDA(cudaMemcpyAsync(st, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < h->n; i++) V[i] = (double)st[i];
+    return EP_OK;
+}
+
+// stored states <-> node-major rows (State[0] = V except LR, which keeps V
+// in slot 7)
+template <typename R>
+static int put_states(ep_handle *h, const double *in) {
+    const size_t tot = (size_t)h->ns * h->pitch;
+    R *st = (R *)stage(h, sizeof(R) * tot);
+    if (!st) return EP_ERR_NOMEM;
+    const int off = is_lr(h->model) ? 0 : 1;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < h->pitch; i++) {
+        if (i < h->n) {
+            const double *s = in + (size_t)i * h->nstate;
+            for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = (R)s[k + off];
+        } else {
+            for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = R(0);
+        }
+    }
+    EP_CUDA(cudaMemcpyAsync(h->S.p, st, sizeof(R) * tot, cudaMemcpyHostToDevice, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    return EP_OK;
+}
+
+template <typename R>
+static int get_states(ep_handle *h, double *out) {
+    const size_t tot = (size_t)h->ns * h->pitch;
+    R *st = (R *)stage(h, sizeof(R) * (tot + h->pitch));
+    if (!st) return EP_ERR_NOMEM;
+    R *sv = st + tot;
+    EP_CUDA(cudaMemcpyAsync(st, h->S.p, sizeof(R) * tot, cudaMemcpyDeviceToHost, h->stream));
+    EP_CUDA(cudaMemcpyAsync(sv, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    const bool lr = is_lr(h->model);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < h->n; i++) {
+        double *o = out + (size_t)i * h->nstate;
+        if (lr) {
+            for (int k = 0; k < 7; k++) o[k] = (double)st[(size_t)k * h->pitch + i];
+            o[7] = (double)sv[i];
+        } else {
+            o[0] = (double)sv[i];
+            for (int k = 0; k < h->ns; k++) o[k + 1] = (double)st[(size_t)k * h->pitch + i];
+        }
+    }
+    return EP_OK;
+}
+
+extern "C" {
+
 int ep_set_voltage(ep_handle *h, const double *V) {
     EP_CHECK_ARG(h && V, "null argument");
     EP_CUDA(cudaSetDevice(h->device));
-    std::vector<double> v(V, V + h->n);
-    int rc = h->precision == EP_FP64 ? upload<double>(h->V, v, h->pitch) : upload<float>(h->V, v, h->pitch);
-    return rc;
+    return h->precision == EP_FP64 ? put_voltage<double>(h, V) : put_voltage<float>(h, V);
 }
 
 int ep_get_voltage(ep_handle *h, double *V) {
     EP_CHECK_ARG(h && V, "null argument");
     EP_CUDA(cudaSetDevice(h->device));
-    std::vector<double> v;
-    int rc = h->precision == EP_FP64 ? download<double>(h->V, v, h->n, h->stream)
-                                     : download<float>(h->V, v, h->n, h->stream);
-    if (rc) return rc;
-    std::memcpy(V, v.data(), sizeof(double) * h->n);
-    return EP_OK;
+    return h->precision == EP_FP64 ? get_voltage<double>(h, V) : get_voltage<float>(h, V);
 }
 
 int ep_get_model_voltage(ep_handle *h, double *V) {
@@ -768,36 +854,13 @@ int ep_get_model_voltage(ep_handle *h, double *V) {
 int ep_get_states(ep_handle *h, double *out) {
     EP_CHECK_ARG(h && out, "null argument");
     EP_CUDA(cudaSetDevice(h->device));
-    std::vector<double> S, V;
-    const size_t tot = (size_t)h->ns * h->pitch;
-    int rc = h->precision == EP_FP64 ? download<double>(h->S, S, tot, h->stream)
-                                     : download<float>(h->S, S, tot, h->stream);
-    if (rc) return rc;
-    std::vector<double> v(h->n);
-    if ((rc = ep_get_voltage(h, v.data()))) return rc;
-    for (int i = 0; i < h->n; i++) {
-        double *o = out + (size_t)i * h->nstate;
-        if (is_lr(h->model)) {
-            for (int k = 0; k < 7; k++) o[k] = S[(size_t)k * h->pitch + i];
-            o[7] = v[i];
-        } else {
-            o[0] = v[i];
-            for (int k = 0; k < h->ns; k++) o[k + 1] = S[(size_t)k * h->pitch + i];
-        }
-    }
-    return EP_OK;
+    return h->precision == EP_FP64 ? get_states<double>(h, out) : get_states<float>(h, out);
 }
 
 int ep_set_states(ep_handle *h, const double *in) {
     EP_CHECK_ARG(h && in, "null argument");
     EP_CUDA(cudaSetDevice(h->device));
-    std::vector<double> S((size_t)h->ns * h->pitch, 0.0);
-    for (int i = 0; i < h->n; i++) {
-        const double *s = in + (size_t)i * h->nstate;
-        if (is_lr(h->model)) for (int k = 0; k < 7; k++) S[(size_t)k * h->pitch + i] = s[k];
-        else for (int k = 0; k < h->ns; k++) S[(size_t)k * h->pitch + i] = s[k + 1];
-    }
-    return h->precision == EP_FP64 ? upload<double>(h->S, S) : upload<float>(h->S, S);
+    return h->precision == EP_FP64 ? put_states<double>(h, in) : put_states<float>(h, in);
 }
 
 int ep_set_stimulus(ep_handle *h, int32_t n, const int32_t *ids, const double *t_on,
