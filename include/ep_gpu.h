@@ -239,9 +239,13 @@ int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_
  * ionic kernel compiled for at least 3 or 4 resident 128-thread CTAs per SM
  * (fewer registers per thread), 0 = the compiler's register choice;
  * cg_batch: SELL columns whose gathers the CG kernel issues together (4 or
- * 8; 8 keeps more loads in flight at a larger register budget). */
+ * 8; 8 keeps more loads in flight at a larger register budget);
+ * cg_variant: 0 the CG recurrences of the reference (two reductions per
+ * iteration), 1 the Chronopoulos-Gear recurrences (one reduction per
+ * iteration; same iterates in exact arithmetic, rounding-level differences;
+ * five more vectors on the device). */
 typedef struct ep_launch_config {
-    int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas, cg_batch;
+    int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas, cg_batch, cg_variant;
 } ep_launch_config;
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);

@@ -71,6 +71,7 @@ struct ep_handle {
     int nslices = 0;
     // device memory
     DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, consts, gks, lr_table, type, slice_ptr, col;
+    DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
     DBuf partial, bar, status, cg_stats, cg_last, d_step, track;
     DBuf stim_head, stim_next, stim_on, stim_off, stim_amp;
     int nstim = 0;
@@ -96,7 +97,7 @@ struct ep_handle {
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
-    int cg_per_sm = 0, cg_batch = 4, ionic_block = 128, ionic_min = 0, graph_steps = 0;
+    int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, ionic_block = 128, ionic_min = 0, graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
@@ -200,6 +201,8 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.ninst = h->ninst;
     a.inst_row = h->d_inst_row.as<int>();
     a.inst_blk = h->d_inst_blk.as<int>();
+    a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
+    a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
 }
 
 template <typename R>
@@ -291,9 +294,17 @@ extern "C" int ep_batch_plan(int32_t ninst, const int32_t *inst_row, int32_t gri
 // (re)size the CG launch for the handle's launch shape: grid, CTA groups,
 // partials, barriers and per-instance results
 static int plan_cg(ep_handle *h) {
-    int rc = h->precision == EP_FP64 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch)
-                                     : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch);
+    int rc = h->precision == EP_FP64
+                 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant)
+                 : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant);
     if (rc) return rc;
+    if (h->cg_variant == 1 && !h->w0.p) {
+        const size_t vb = (size_t)h->pitch * h->rsize;
+        for (DBuf *b : {&h->r1, &h->w0, &h->w1, &h->s0, &h->s1}) {
+            if ((rc = b->alloc(vb))) return rc;
+            EP_CUDA(cudaMemset(b->p, 0, vb));
+        }
+    }
     if (h->ninst > h->cg_grid) {
         set_error("%d instances but only %d CTAs in the persistent launch", h->ninst, h->cg_grid);
         return EP_ERR_ARG;
@@ -305,7 +316,7 @@ static int plan_cg(ep_handle *h) {
     }
     if ((rc = upload_raw(h->d_inst_row, h->inst_row.data(), h->inst_row.size()))) return rc;
     if ((rc = upload_raw(h->d_inst_blk, h->inst_blk.data(), h->inst_blk.size()))) return rc;
-    if ((rc = h->partial.alloc(sizeof(double) * 4 * (size_t)h->cg_grid))) return rc;
+    if ((rc = h->partial.alloc(sizeof(double) * 12 * (size_t)h->cg_grid))) return rc;
     if (h->bar.bytes != sizeof(GridBarrier) * (size_t)h->ninst) {
         if ((rc = h->bar.alloc(sizeof(GridBarrier) * (size_t)h->ninst))) return rc;
         EP_CUDA(cudaMemset(h->bar.p, 0, sizeof(GridBarrier) * (size_t)h->ninst));
@@ -407,7 +418,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     int rc;
     for (int s = 0; s < nsteps; s++) {
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant))) return rc;
         if ((rc = mark(h, ne, K_IONIC))) return rc;
         if constexpr (sizeof(R) == 4) {
             if (h->precision == EP_SURROGATE) {
@@ -420,7 +431,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch))) return rc;
+        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant))) return rc;
         if ((rc = mark(h, ne, K_OTHER))) return rc;
         launch_step_inc(h->d_step.as<long long>(), h->stream);
         h->launches += 4;
@@ -1008,11 +1019,11 @@ int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
     if (h->precision == EP_FP64) {
         CGArgs<double> ca;
         fill_cg_args<double>(h, ca);
-        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch);
+        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
     } else {
         CGArgs<float> ca;
         fill_cg_args<float>(h, ca);
-        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch);
+        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
     }
     if (rc) return rc;
     double last[2];
@@ -1158,6 +1169,7 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     EP_CHECK_ARG(h && cfg, "null argument");
     cfg->cg_block = h->cg_block;
     cfg->cg_batch = h->cg_batch;
+    cfg->cg_variant = h->cg_variant;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1173,6 +1185,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256 || cfg->cg_block == 512 || cfg->cg_block == 768,
                  "cg_block must be 128, 256, 512 or 768");
     EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8, "cg_batch must be 4 or 8");
+    EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
     EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
@@ -1181,13 +1194,14 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     drop_graph(h);
-    const int ob = h->cg_block, op = h->cg_per_sm, obt = h->cg_batch;
+    const int ob = h->cg_block, op = h->cg_per_sm, obt = h->cg_batch, ov = h->cg_variant;
     h->cg_block = cfg->cg_block;
     h->cg_per_sm = cfg->cg_per_sm;
     h->cg_batch = cfg->cg_batch;
+    h->cg_variant = cfg->cg_variant;
     int rc = plan_cg(h);
     if (rc) {
-        h->cg_block = ob; h->cg_per_sm = op; h->cg_batch = obt;
+        h->cg_block = ob; h->cg_per_sm = op; h->cg_batch = obt; h->cg_variant = ov;
         plan_cg(h);
         return rc;
     }
@@ -1251,6 +1265,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     ep_launch_config cur;
     cur.cg_block = h->cg_block;
     cur.cg_batch = h->cg_batch;
+    cur.cg_variant = h->cg_variant;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
     cur.ionic_min_ctas = h->ionic_min;
@@ -1282,8 +1297,8 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     for (int nb : {4, 8}) {
         for (int blk : {128, 256, 512, 768}) {
             int maxper = 0;
-            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb)
-                                         : cg_max_per_sm<float>(blk, &maxper, nb)))
+            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant)
+                                         : cg_max_per_sm<float>(blk, &maxper, nb, cg0.cg_variant)))
                 continue;
             maxper = std::min(maxper, 8);
             for (int per : {maxper, maxper / 2}) {
@@ -1295,6 +1310,12 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
                 if (t >= 0 && t < t_best) { t_best = t; b = c; }
             }
         }
+    }
+    {
+        ep_launch_config c = b;
+        c.cg_variant = 1 - b.cg_variant;
+        const double t = trial(c);
+        if (t >= 0 && t < t_best) { t_best = t; b = c; }
     }
     for (int ib : {64, 128}) {
         if (ib == b.ionic_block) continue;

@@ -239,20 +239,184 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same solve by the Chronopoulos-Gear recurrences: one grid barrier per
+// iteration instead of two.  With z = dinv r and w = A z,
+//   gamma = (r, z), delta = (z, w)                 (one reduction)
+//   beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma / alpha_old)
+//   p = z + beta p, s = w + beta s, x += alpha p, r -= alpha s
+// and the next w = A z is formed in the same pass: each neighbour's new z is
+// recomputed from its old r, w, s (read from the other half of r, w, s's
+// double buffers), with the owner's explicit fma sequence so both round alike.
+// In exact arithmetic the iterates are those of k_cn_half; in floating point
+// they differ at the rounding level (an option of the autotuner, not the
+// default).
 template <typename R>
-int cg_max_per_sm(int block, int *per, int batch) {
-    if (batch == 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 8>, block, 0));
-    else EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 4>, block, 0));
+__device__ __forceinline__ R cg1_snew(R w, R beta, R s) { return fma(beta, s, w); }
+template <typename R>
+__device__ __forceinline__ R cg1_rnew(R r, R alpha, R snew) { return fma(-alpha, snew, r); }
+
+template <typename R, int NB>
+__global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_half_cg1(const CGArgs<R> a) {
+    const int lane = threadIdx.x & 31;
+    const int G = gridDim.x;
+    int inst = 0, b0 = 0, nb = G, rb = 0, re = a.n;
+    if (a.ninst > 1) {
+        int lo = 0, hi = a.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.inst_blk[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        }
+        inst = lo;
+        b0 = a.inst_blk[inst]; nb = a.inst_blk[inst + 1] - b0;
+        rb = a.inst_row[inst]; re = a.inst_row[inst + 1];
+    }
+    GridBarrier *bar = a.bar + inst;
+    const unsigned int nblk = nb;
+    const int s_lo = rb / kSlice, s_hi = (re + kSlice - 1) / kSlice;
+    const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
+    const int nwarps = (nb * (int)blockDim.x) >> 5;
+
+    // ---- P1: r0 = B x - A x; p = 0, s_{-1} = 0 ----
+    {
+        double v[2] = {0.0, 0.0};
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+            R ax = R(0), bx = R(0);
+            for (int k = 0; k < w; k++) {
+                const int idx = beg + k * kSlice + lane;
+                const R xv = a.x[__ldg(a.col + idx)];
+                ax += __ldg(a.Aval + idx) * xv;
+                bx += __ldg(a.Bval + idx) * xv;
+            }
+            if (row >= rb && row < re) {
+                const R r = bx - ax;
+                a.r[row] = r;
+                a.p0[row] = R(0);
+                a.s1[row] = R(0);
+                v[0] += (double)r * (double)r;
+                v[1] += (double)bx * (double)bx;
+            }
+        }
+        block_reduce_store<2>(v, a.partial, G);
+    }
+    if (!grid_sync(bar, nblk)) return;
+    double rr0, bb;
+    {
+        double t[2];
+        grid_total<2>(a.partial, G, b0, nb, t);
+        rr0 = t[0]; bb = t[1];
+    }
+    const double stop2 = fmax(a.tol * a.tol * rr0, a.floor_rel * a.floor_rel * bb);
+    bool converged = (rr0 <= stop2);
+    double rr_last = rr0;
+    int it = 0;
+    double gamma = 0.0, delta = 0.0;
+    // ---- P2: w0 = A z0, gamma0 = (r0, z0), delta0 = (z0, w0) ----
+    if (!converged) {
+        double v[2] = {0.0, 0.0};
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+            const R wv = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane,
+                                           [&](int c) { return __ldg(a.dinv + c) * ldcg(a.r + c); });
+            if (row >= rb && row < re) {
+                const R z = __ldg(a.dinv + row) * a.r[row];
+                a.w0[row] = wv;
+                v[0] += (double)a.r[row] * (double)z;
+                v[1] += (double)z * (double)wv;
+            }
+        }
+        // partial slots: P1 [0, 2G), P2 [9G, 11G), iterations alternate
+        // [3G, 6G) and [6G, 9G): consecutive phases never share a slot
+        block_reduce_store<2>(v, a.partial + 9 * G, G);
+        if (!grid_sync(bar, nblk)) return;
+        double t[2];
+        grid_total<2>(a.partial + 9 * G, G, b0, nb, t);
+        gamma = t[0]; delta = t[1];
+    }
+    double alpha = (delta > 0.0) ? gamma / delta : 0.0, beta = 0.0;
+    if (!(delta > 0.0)) converged = true;       // A z0 = 0: nothing left to solve
+    int cur = 0;
+    while (!converged && it < a.maxit) {
+        const R aR = (R)alpha, bR = (R)beta;
+        // the double buffers by selects (no local-memory pointer arrays)
+        const R *rc = cur ? a.r1 : a.r, *wc = cur ? a.w1 : a.w0, *sp = cur ? a.s0 : a.s1;
+        R *rn = cur ? a.r : a.r1, *wn = cur ? a.w0 : a.w1, *sc = cur ? a.s1 : a.s0;
+        double v[3] = {0.0, 0.0, 0.0};
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+            // w_{k+1} = A z_{k+1}, z_{k+1} of the neighbours rebuilt from old r, w, s
+            const R wv = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, [&](int c) {
+                const R snew = cg1_snew(ldcg(wc + c), bR, ldcg(sp + c));
+                return __ldg(a.dinv + c) * cg1_rnew(ldcg(rc + c), aR, snew);
+            });
+            if (row >= rb && row < re) {
+                const R d = __ldg(a.dinv + row);
+                const R rk = rc[row];
+                const R p = fma(bR, a.p0[row], d * rk);
+                const R snew = cg1_snew(wc[row], bR, sp[row]);
+                const R rnew = cg1_rnew(rk, aR, snew);
+                const R znew = d * rnew;
+                a.p0[row] = p;
+                sc[row] = snew;
+                a.x[row] += aR * p;
+                rn[row] = rnew;
+                wn[row] = wv;
+                v[0] += (double)rnew * (double)znew;
+                v[1] += (double)znew * (double)wv;
+                v[2] += (double)rnew * (double)rnew;
+            }
+        }
+        block_reduce_store<3>(v, a.partial + 3 * (cur + 1) * G, G);   // alternate slots
+        if (!grid_sync(bar, nblk)) return;
+        double t[3];
+        grid_total<3>(a.partial + 3 * (cur + 1) * G, G, b0, nb, t);
+        it++;
+        rr_last = t[2];
+        converged = (t[2] <= stop2);
+        const double gnew = t[0];
+        beta = gnew / gamma;
+        const double den = t[1] - beta * gnew / alpha;
+        if (!(den > 0.0)) converged = true;        // breakdown at the rounding floor
+        alpha = gnew / den;
+        gamma = gnew;
+        cur = 1 - cur;
+    }
+    // the solution is in x; r's current buffer is left wherever it is
+    if ((int)blockIdx.x == b0 && threadIdx.x == 0) {
+        atomicAdd(a.iters_total, (unsigned long long)it);
+        atomicMax(a.iters_max, (unsigned int)it);
+        if (!converged) atomicAdd(a.fails, 1u);
+        if (a.last) {
+            a.last[2 * inst] = (double)it;
+            a.last[2 * inst + 1] = rr0 > 0.0 ? sqrt(rr_last / rr0) : 0.0;
+        }
+    }
+}
+
+template <typename R>
+int cg_max_per_sm(int block, int *per, int batch, int variant) {
+    if (variant == 1) {
+        if (batch == 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 8>, block, 0));
+        else EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 4>, block, 0));
+    } else if (batch == 8) {
+        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 8>, block, 0));
+    } else {
+        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 4>, block, 0));
+    }
     if (*per < 1) { set_error("CG kernel cannot be resident with %d threads per CTA", block); return EP_ERR_CUDA; }
     return EP_OK;
 }
 
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm, int batch) {
+int cg_grid_size(int block, int *grid, int per_sm, int batch, int variant) {
     int dev = 0, nsm = 0, per = 0;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int rc = cg_max_per_sm<R>(block, &per, batch);
+    int rc = cg_max_per_sm<R>(block, &per, batch, variant);
     if (rc) return rc;
     if (per_sm > 0 && per_sm < per) per = per_sm;
     *grid = nsm * per;
@@ -260,7 +424,7 @@ int cg_grid_size(int block, int *grid, int per_sm, int batch) {
 }
 
 template <typename R>
-int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch) {
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch, int variant) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -271,17 +435,24 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (batch == 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 8>, a));
-    else EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 4>, a));
+    if (variant == 1) {
+        if (!a.r1 || !a.w0 || !a.w1 || !a.s0 || !a.s1) { set_error("single-reduction CG needs its vectors"); return EP_ERR_ARG; }
+        if (batch == 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 8>, a));
+        else EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 4>, a));
+    } else if (batch == 8) {
+        EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 8>, a));
+    } else {
+        EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 4>, a));
+    }
     return EP_OK;
 }
 
-template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t, int);
-template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t, int);
-template int cg_grid_size<float>(int, int *, int, int);
-template int cg_grid_size<double>(int, int *, int, int);
-template int cg_max_per_sm<float>(int, int *, int);
-template int cg_max_per_sm<double>(int, int *, int);
+template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t, int, int);
+template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t, int, int);
+template int cg_grid_size<float>(int, int *, int, int, int);
+template int cg_grid_size<double>(int, int *, int, int, int);
+template int cg_max_per_sm<float>(int, int *, int, int);
+template int cg_max_per_sm<double>(int, int *, int, int);
 
 // ---------------------------------------------------------------------------
 // pseudo-ECG: out[k] = sum_i W[k * wpitch + i] V[i], FP64 accumulation.

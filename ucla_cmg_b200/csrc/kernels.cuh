@@ -89,7 +89,7 @@ template <typename R> struct CGArgs {
     const int *col;
     const R *Aval, *Bval, *dinv;
     R *x, *r, *q, *p0, *p1;
-    double *partial;             // 4 * grid: consecutive phases use disjoint slots
+    double *partial;             // 12 * grid: consecutive phases use disjoint slots
     GridBarrier *bar;
     double tol;
     double floor_rel;            // stop also when ||r|| <= floor_rel ||B x||
@@ -103,16 +103,21 @@ template <typename R> struct CGArgs {
     // one instance owning every row and CTA.
     int ninst;
     const int *inst_row, *inst_blk;
+    // single-reduction variant only: second r buffer, w = A z and s = A p
+    // (two buffers each); p lives in p0
+    R *r1, *w0, *w1, *s0, *s1;
 };
 
-// batch: SELL columns gathered per group (4 or 8; two register budgets)
+// batch: SELL columns gathered per group (4 or 8; two register budgets);
+// variant 0: the two-reduction CG of the reference, 1: Chronopoulos-Gear
+// (one reduction per iteration; needs r1, w0, w1, s0, s1)
 template <typename R>
-int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch = 4);
+int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch = 4, int variant = 0);
 // CTAs of the persistent launch: per_sm (0 = as many as fit) x SM count
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm = 0, int batch = 4);
+int cg_grid_size(int block, int *grid, int per_sm = 0, int batch = 4, int variant = 0);
 template <typename R>
-int cg_max_per_sm(int block, int *per, int batch = 4);
+int cg_max_per_sm(int block, int *per, int batch = 4, int variant = 0);
 
 // ECG_k = sum_i W[k n + i] V[i] (ComputeECG.h:172-189 in per-node form),
 // deterministic two-level reduction, written to out[k].
