@@ -1,0 +1,93 @@
+"""The EPSimulator-compatible driver: input parsing, the reference's
+stimulus schedule and region types, and the mesh file formats (CPU)."""
+import numpy as np
+
+from ucla_cmg_b200 import capi, mesh as M
+from ucla_cmg_b200 import driver as D
+from ucla_cmg_b200 import voomep_io as IO
+
+
+def test_parse_input(tmp_path):
+    f = tmp_path / "case.input"
+    f.write_text("""# comment line
+MODEL  Mesh/slab
+OutputDir out/
+CellModel Tusscher
+dt 0.02
+IonicDt 0.01
+SimulationTime 12.5   # any '#' in a line drops the whole line (the reference's test)
+SimulationTime 10
+frequency 0.5
+TissueDiffusion 1e-3 2e-4 2e-4
+Smoothing
+Stimulus Nodal set.txt 0. 1.0
+Stimulus Circ 0.1 0.2 0.0 0.05 5.0 6.0 30000
+Stimulus Zonal y 0.1 7 8
+Stimulus Plane 0 0 0 1 0 0 9 10 100
+MechDt 999
+""")
+    c = D.parse_input(str(f))
+    assert c["model"] == "Mesh/slab" and c["output_dir"] == "out/" and c["cell_model"] == "Tusscher"
+    assert c["dt"] == 0.02 and c["ionic_dt"] == 0.01 and c["simulation_time"] == 10.0
+    assert c["frequency"] == 0.5 and c["D"] == [1e-3, 2e-4, 2e-4] and c["smoothing"] == 0.1
+    assert c["write_restart"] == 99999.0 and c["read_restart"] is None
+    s = c["stimuli"]
+    assert [x["type"] for x in s] == [0, 1, 2, 3]
+    assert s[0]["i_stim"] == 50000.0 and s[1]["i_stim"] == 30000.0 and s[3]["i_stim"] == 100.0
+    assert s[1]["radius"] == 0.05 and s[1]["center"] == [0.1, 0.2, 0.0]
+    assert s[2]["axis"] == 1 and s[2]["limit"] == 0.1
+    assert s[3]["normal"] == [1.0, 0.0, 0.0] and s[3]["t_start"] == 9.0
+    assert "MECHDT" in c["ignored"]
+
+
+def test_stimulus_pointer_schedule():
+    st = [dict(t_start=0.0, t_stop=1.0), dict(t_start=5.0, t_stop=6.0)]
+    ev = D.stimulus_events(st, 0.1, 100)
+    assert ev == [(0, 0, True), (10, 0, False), (50, 1, True), (60, 1, False)]
+    # out of order: the second start precedes the first stop; the reference's
+    # start pointer has moved past it when the count gets there, so it never fires
+    st = [dict(t_start=5.0, t_stop=6.0), dict(t_start=1.0, t_stop=2.0)]
+    ev = D.stimulus_events(st, 0.1, 100)
+    assert (10, 1, True) not in ev and (50, 0, True) in ev
+
+
+def test_stimulus_regions_and_windows():
+    xyz = np.array([[0.0, 0, 0], [0.05, 0, 0], [0.2, 0, 0], [0.5, 0, 0]])
+    circ = dict(type=1, center=[0.0, 0.0, 0.0], radius=0.1, i_stim=7.0, t_start=0.0, t_stop=1.0)
+    zonal = dict(type=2, axis=0, limit=0.3, i_stim=3.0, t_start=2.0, t_stop=3.0)
+    plane = dict(type=3, center=[0.3, 0, 0], normal=[-1.0, 0, 0], i_stim=5.0, t_start=4.0, t_stop=5.0)
+    istim = np.full(4, 9.0)
+    D.apply_region(istim, circ, True, xyz, None, ".")
+    assert list(istim) == [7.0, 7.0, 0.0, 0.0]            # CIRC switches the others off
+    D.apply_region(istim, zonal, True, xyz, None, ".")
+    assert list(istim) == [3.0, 3.0, 3.0, 0.0]
+    # PLANE: nodes with (x - c).n < 0, here x > 0.3; node 4 (1-based) is a
+    # Purkinje node and keeps its value; every other node is switched off
+    D.apply_region(istim, plane, True, xyz, np.array([4]), ".")
+    assert list(istim) == [0.0, 0.0, 0.0, 0.0]
+    ids, on, off, amp = D.stimulus_windows([circ, zonal, plane], 0.5, 20, xyz, None, ".")
+    w = set(zip(ids.tolist(), on.tolist(), off.tolist(), amp.tolist()))
+    assert w == {(0, 0, 2, 7.0), (1, 0, 2, 7.0), (0, 4, 6, 3.0), (1, 4, 6, 3.0), (2, 4, 6, 3.0),
+                 (3, 8, 10, 5.0)}
+
+
+def test_mesh_files_round_trip(tmp_path):
+    m = M.slab(5, 4, 3, 0.4, 0.3, 0.2)
+    t = (np.arange(m.n) % 3).astype(np.uint8)
+    base = str(tmp_path / "slab")
+    IO.write_mesh(base, m, t)
+    m2, t2, purk, other = IO.read_mesh(base)
+    assert other == 0 and purk is None
+    assert np.array_equal(m2.tets, m.tets)
+    assert np.allclose(m2.xyz, m.xyz, rtol=0, atol=0)
+    assert np.array_equal(m2.fibers, m.fibers)
+    assert np.array_equal(t2, t)
+
+
+def test_mesh_reader_skips_cables(tmp_path):
+    base = str(tmp_path / "mix")
+    (tmp_path / "mix.node").write_text("5 3 0 0\n1 0 0 0\n2 1 0 0\n3 0 1 0\n4 0 0 1\n5 2 2 2\n")
+    (tmp_path / "mix.ele").write_text("2 4 0\n1 4 1 2 3 4\n2 2 4 5\n")
+    (tmp_path / "mix.purk").write_text("2\n4 5\n")
+    m, t, purk, other = IO.read_mesh(base)
+    assert m.m == 1 and other == 1 and list(purk) == [4, 5]

@@ -1,0 +1,111 @@
+"""voomEP mesh files: readers (and writers, for fixtures and converted meshes).
+
+Formats as the reference reads them (voomEP/src/Mesh/Mesh.cc):
+
+* ``<base>.node``: header ``nNodes dim x x``, then ``id x y [z]`` per node
+  (Mesh.cc:201, 316-323);
+* ``<base>.ele``: header ``nElems x x``, then ``id nPerElem n1 .. nk`` with
+  1-based node ids (Mesh.cc:279-290, 330-335); a 3D EP mesh holds 4-node
+  tets, plus 2-node Purkinje cables in mixed (MIX3D) meshes;
+* ``<base>.fibers``: per element, in ``.ele`` order, the 9 numbers
+  f, s, n (Mesh.cc:337-341, CardiacBody.cc:158-167);
+* ``<base>.cell``: lines ``nodeID typeID`` (1-based node ids), the tissue
+  type of each node, default 0 (Mesh.cc:391-401);
+* ``<base>.purk``: ``n`` then n 1-based node ids of Purkinje nodes
+  (Mesh.cc:377-388).
+"""
+import os
+
+import numpy as np
+
+from .mesh import TetMesh
+
+
+def read_node(path):
+    with open(path) as f:
+        tok = f.read().split()
+    n, dim = int(tok[0]), int(tok[1])
+    a = np.array(tok[4:4 + n * (dim + 1)], dtype=np.float64).reshape(n, dim + 1)
+    xyz = np.zeros((n, 3))
+    xyz[:, :dim] = a[:, 1:]
+    return xyz
+
+
+def read_ele(path):
+    """(tets [m x 4] zero-based, element index of each tet, number of
+    elements that are not 4-node tets)."""
+    with open(path) as f:
+        tok = f.read().split()
+    ne = int(tok[0])
+    pos = 3
+    tets, which, other = [], [], 0
+    for e in range(ne):
+        k = int(tok[pos + 1])
+        conn = tok[pos + 2:pos + 2 + k]
+        pos += 2 + k
+        if k == 4:
+            tets.append([int(c) - 1 for c in conn])
+            which.append(e)
+        else:
+            other += 1
+    return np.array(tets, dtype=np.int32).reshape(-1, 4), np.array(which, dtype=np.int64), other
+
+
+def read_fibers(path, n_elems):
+    a = np.loadtxt(path, dtype=np.float64).reshape(-1)
+    if a.size < 9 * n_elems:
+        raise ValueError(f"{path}: {a.size} numbers for {n_elems} elements")
+    return a[:9 * n_elems].reshape(n_elems, 9)
+
+
+def read_cell(path, n):
+    t = np.zeros(n, dtype=np.uint8)
+    with open(path) as f:
+        tok = f.read().split()
+    a = np.array(tok[:len(tok) // 2 * 2], dtype=np.int64).reshape(-1, 2)
+    t[a[:, 0] - 1] = a[:, 1]
+    return t
+
+
+def read_purk(path):
+    with open(path) as f:
+        tok = f.read().split()
+    k = int(tok[0])
+    return np.array(tok[1:1 + k], dtype=np.int64)
+
+
+def read_mesh(base):
+    """The tet mesh of ``base`` (.node/.ele, optional .fibers/.cell/.purk).
+    Returns (TetMesh, node_type or None, purkinje node ids (1-based) or None,
+    number of non-tet elements)."""
+    xyz = read_node(base + ".node")
+    tets, which, other = read_ele(base + ".ele")
+    fib = None
+    if os.path.exists(base + ".fibers"):
+        with open(base + ".ele") as f:
+            n_elems = int(f.readline().split()[0])
+        fib = read_fibers(base + ".fibers", n_elems)[which]
+    ntype = read_cell(base + ".cell", len(xyz)) if os.path.exists(base + ".cell") else None
+    purk = read_purk(base + ".purk") if os.path.exists(base + ".purk") else None
+    return TetMesh(xyz, tets, fib, {}), ntype, purk, other
+
+
+def write_mesh(base, mesh, node_type=None):
+    """Write ``mesh`` in the reference's formats (1-based ids)."""
+    n, m = mesh.n, mesh.m
+    with open(base + ".node", "w") as f:
+        f.write(f"{n} 3 0 0\n")
+        for i in range(n):
+            x, y, z = mesh.xyz[i]
+            f.write(f"{i + 1} {x:.17g} {y:.17g} {z:.17g}\n")
+    with open(base + ".ele", "w") as f:
+        f.write(f"{m} 4 0\n")
+        for e in range(m):
+            a, b, c, d = mesh.tets[e] + 1
+            f.write(f"{e + 1} 4 {a} {b} {c} {d}\n")
+    if mesh.fibers is not None:
+        np.savetxt(base + ".fibers", mesh.fibers, fmt="%.17g")
+    if node_type is not None:
+        with open(base + ".cell", "w") as f:
+            for i in range(n):
+                f.write(f"{i + 1} {int(node_type[i])}\n")
