@@ -19,18 +19,15 @@ def test_driver_matches_direct_run(gpu, tmp_path):
     IO.write_mesh(str(tmp_path / "slab"), m)
     blk = M.corner_block(m, 3, 3)
     np.savetxt(tmp_path / "stim.txt", blk + 1, fmt="%d")
-    (tmp_path / "case.input").write_text(f"""MODEL slab
-OutputDir out/
-CellModel TUSSCHER
-DT 0.02
-IonicDT 0.02
-SimulationTime 5
-Frequency 1
-TissueDiffusion {D_[0]} {D_[1]} {D_[2]}
-Stimulus Nodal stim.txt 0. 1.0 100000
-""".replace("{D_[0]} {D_[1]} {D_[2]}", " ".join(repr(v) for v in M.sigma_to_D(1.2, 0.2))))
+    dtxt = " ".join(repr(float(v)) for v in M.sigma_to_D(1.2, 0.2))
+    (tmp_path / "case.input").write_text("MODEL slab\nOutputDir out/\nCellModel TUSSCHER\nDT 0.02\n"
+                                         "IonicDT 0.02\nSimulationTime 5\nFrequency 1\n"
+                                         f"TissueDiffusion {dtxt}\n"
+                                         "Stimulus Nodal stim.txt 0. 1.0 100000\n")
     cfg, nsteps = D.run(str(tmp_path / "case.input"), capi.FP64, rest_voltage=True, verbose=False)
-    assert nsteps == 250
+    # simtime accumulates 0.02 per step and is still below 5 after 250 steps,
+    # so the loop (as the reference's) takes 251; the last output is at 250
+    assert nsteps == 251
     out = tmp_path / "out"
     files = sorted(f for f in os.listdir(out) if f.startswith("Voltage_time_"))
     assert len(files) == 6 and files[0] == "Voltage_time_00000.00.00" and files[-1] == "Voltage_time_00005.00.00"
