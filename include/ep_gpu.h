@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EP_ABI_VERSION 1
+#define EP_ABI_VERSION 2
 
 /* ---- status codes ---- */
 #define EP_OK               0
@@ -101,7 +101,21 @@ typedef struct ep_solver_desc {
                                    tolerance; FP32 scales it by max(|x|,1)) */
     int32_t ecg_every;          /* steps between pseudo-ECG samples (0 off) */
     double act_threshold;       /* mV; activation = upward crossing (0: -40) */
+    int32_t scheme;             /* EP_SCHEME_*: the EPSolver Method (EPSolver.h:
+                                   Method; the reference driver always takes
+                                   CRANKNICKOLSON) */
+    double diffusion_dt;        /* explicit scheme: diffusion sub-step (0: 0.05,
+                                   EP_ExplicitSolver.h:68) */
 } ep_solver_desc;
+
+/* ---- operator-splitting schemes (EPSolver::New, Solvers/EPSolver.cc) ---- */
+#define EP_SCHEME_CN        0  /* EP_CrankNicholson: D/2 by CN (CG to 1e-7),
+                                  ionic sub-steps of IONICDT */
+#define EP_SCHEME_BE        1  /* EP_BackwardEuler: (C_L + dt/2 K) V' = C_L V
+                                  (CG to 1e-10), adaptive ionic strides, again */
+#define EP_SCHEME_EXPLICIT  2  /* EP_ExplicitSolver: forward-Euler diffusion
+                                  sub-steps V += h (-K V) / C_L over dt/2,
+                                  adaptive ionic strides, again */
 
 typedef struct ep_step_stats {
     int64_t steps;              /* steps done by this call */

@@ -33,7 +33,8 @@ def test_driver_matches_direct_run(gpu, tmp_path):
     assert len(files) == 6 and files[0] == "Voltage_time_00000.00.00" and files[-1] == "Voltage_time_00005.00.00"
     Vd = np.fromfile(out / files[-1], dtype=np.float64)
     m2, _, _, _ = IO.read_mesh(str(tmp_path / "slab"))
-    g = Monodomain(m2, capi.TUSSCHER, capi.FP64, dt=0.02, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2))
+    g = Monodomain(m2, capi.TUSSCHER, capi.FP64, dt=0.02, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
+                   tt_jacobian=capi.TT_JAC_TRUE)
     g.set_voltage(g.states()[:, 0])
     g.set_stimulus(blk, 0.0, 1.0, 100000.0)
     g.step(250)

@@ -20,6 +20,7 @@ ERRORS = {-1: "EP_ERR_ARG", -2: "EP_ERR_CUDA", -3: "EP_ERR_NOMEM", -4: "EP_ERR_M
 LUORUDY, LUORUDYWITHGATE, TUSSCHER, MAHAJAN, MAHAJAN_FAIL = 0, 1, 2, 3, 4
 FP64, FP32, SURROGATE = 0, 1, 2
 TT_JAC_REFERENCE, TT_JAC_TRUE = 0, 1
+SCHEME_CN, SCHEME_BE, SCHEME_EXPLICIT = 0, 1, 2
 
 dp = C.POINTER(C.c_double)
 
@@ -47,7 +48,7 @@ class SolverDesc(C.Structure):
     _fields_ = [("dt", C.c_double), ("ionic_dt", C.c_double), ("cg_tol", C.c_double),
                 ("cg_maxit", C.c_int32), ("smoothing_alpha", C.c_double),
                 ("precision", C.c_int32), ("newton_tol", C.c_double), ("ecg_every", C.c_int32),
-                ("act_threshold", C.c_double)]
+                ("act_threshold", C.c_double), ("scheme", C.c_int32), ("diffusion_dt", C.c_double)]
 
 
 class StepStats(C.Structure):

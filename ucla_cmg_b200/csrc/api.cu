@@ -61,6 +61,9 @@ struct ep_handle {
     int nsub = 1;
     double sub_dt[kMaxSub];
     double cg_tol = 1e-7;
+    int scheme = 0;                      // EP_SCHEME_*
+    std::vector<double> ex_h;            // explicit scheme: diffusion sub-steps of one half
+    DBuf cl;                             // explicit scheme: lumped capacitance C_L
     int cg_maxit = 1000;
     int cg_grid = 0, cg_block = 256;
     int ecg_every = 0;
@@ -180,6 +183,8 @@ void fill_ionic_args(ep_handle *h, IonicArgs<R> &a) {
     a.tt = h->tt;
     a.mh_abs = h->mh_abs;
     a.lr_table = h->lr_table.as<R>();
+    a.stride = h->scheme != EP_SCHEME_CN ? 1 : 0;
+    a.stride_dt = (R)h->ionic_dt;
 }
 
 template <typename R>
@@ -409,6 +414,21 @@ static int mark(ep_handle *h, size_t &ne, int kind) {
     return EP_OK;
 }
 
+// one half diffusion step of the handle's scheme
+template <typename R>
+static int half_diffusion(ep_handle *h, const CGArgs<R> &ca) {
+    if (h->scheme == EP_SCHEME_EXPLICIT) {
+        for (double hh : h->ex_h) {
+            int rc = launch_explicit<R>(h->n, h->nslices, h->slice_ptr.as<int>(), h->col.as<int>(), h->Aval.as<R>(),
+                                        h->cl.as<R>(), h->V.as<R>(), h->q.as<R>(), hh, h->stream);
+            if (rc) return rc;
+        }
+        h->launches += (long long)h->ex_h.size() - 1;
+        return EP_OK;
+    }
+    return launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
+}
+
 template <typename R>
 static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     IonicArgs<R> ia;
@@ -418,7 +438,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     int rc;
     for (int s = 0; s < nsteps; s++) {
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant))) return rc;
+        if ((rc = half_diffusion<R>(h, ca))) return rc;
         if ((rc = mark(h, ne, K_IONIC))) return rc;
         if constexpr (sizeof(R) == 4) {
             if (h->precision == EP_SURROGATE) {
@@ -431,7 +451,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant))) return rc;
+        if ((rc = half_diffusion<R>(h, ca))) return rc;
         if ((rc = mark(h, ne, K_OTHER))) return rc;
         launch_step_inc(h->d_step.as<long long>(), h->stream);
         h->launches += 4;
@@ -577,6 +597,13 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
                      (sd->precision == EP_SURROGATE && md->model == EP_TUSSCHER),
                  "unsupported precision (EP_SURROGATE needs the ten Tusscher model)");
     EP_CHECK_ARG(sd->dt > 0 && sd->ionic_dt > 0, "dt and ionic_dt must be positive");
+    EP_CHECK_ARG(sd->scheme >= EP_SCHEME_CN && sd->scheme <= EP_SCHEME_EXPLICIT, "unknown scheme");
+    if (sd->scheme != EP_SCHEME_CN && sd->smoothing_alpha > 0.0) {
+        set_error("diffusive smoothing is defined for the Crank-Nicolson scheme only");
+        return EP_ERR_UNSUPPORTED;
+    }
+    EP_CHECK_ARG(sd->scheme == EP_SCHEME_CN || sd->precision != EP_SURROGATE,
+                 "the learned ionic step is trained for the Crank-Nicolson sub-steps");
     long long ntot = 0, mtot = 0;
     int ntypes = 0;
     bool any_type = false, any_gks = false, all_fib = true;
@@ -612,7 +639,22 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
     h->nsub = substeps(sd->dt, sd->ionic_dt, h->sub_dt);
     EP_CHECK_ARG(h->nsub > 0, "more than 64 ionic sub-steps per step");
     h->Cm = meshes[0].Cm > 0 ? meshes[0].Cm : 1.0;
-    h->cg_tol = sd->cg_tol > 0 ? sd->cg_tol : 1e-7;
+    h->scheme = sd->scheme;
+    // the reference's fixed tolerances: CN 1e-7 (EP_CrankNicholson.cc:104),
+    // BE 1e-10 (EP_BackwardEuler.cc:67)
+    h->cg_tol = sd->cg_tol > 0 ? sd->cg_tol : (sd->scheme == EP_SCHEME_BE ? 1e-10 : 1e-7);
+    if (sd->scheme == EP_SCHEME_EXPLICIT) {
+        // EP_ExplicitSolver::Solve: sub-steps of min(dtDiff, dt/2) until less
+        // than 1e-6 of the half step is left, the last one shortened
+        const double dtd = sd->diffusion_dt > 0 ? sd->diffusion_dt : 0.05;
+        double solve = 0.5 * sd->dt, stepT = dtd < 0.5 * sd->dt ? dtd : 0.5 * sd->dt;
+        while (solve > 1e-6) {
+            h->ex_h.push_back(stepT);
+            solve -= stepT;
+            stepT = stepT < solve ? stepT : solve;
+            EP_CHECK_ARG(h->ex_h.size() <= 100000, "too many explicit diffusion sub-steps");
+        }
+    }
     h->cg_maxit = sd->cg_maxit > 0 ? sd->cg_maxit : 1000;
     h->ecg_every = sd->ecg_every > 0 ? sd->ecg_every : 0;
     h->act_thr = sd->act_threshold != 0.0 ? sd->act_threshold : -40.0;
@@ -654,7 +696,7 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
         // FEM operators of this instance in FP64, appended block-diagonally
         HostCSR ci;
         if (assemble_cn(ni, mesh->xyz, mi, tl.data(), mesh->fibers, mesh->D, h->Cm, h->dt,
-                        sd->smoothing_alpha, ci) != 0) {
+                        sd->smoothing_alpha, ci, sd->scheme) != 0) {
             set_error("mesh %d has an element with non-positive volume", k);
             return EP_ERR_MESH;
         }
@@ -698,6 +740,12 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
     if (h->precision == EP_FP64) rc = create_typed<double>(h.get(), csr, st, consts, gks);
     else rc = create_typed<float>(h.get(), csr, st, consts, gks);
     if (rc) return rc;
+    if (h->scheme == EP_SCHEME_EXPLICIT) {
+        std::vector<double> cl(csr.CL);
+        cl.resize(h->pitch, 1.0);
+        rc = h->precision == EP_FP64 ? upload<double>(h->cl, cl) : upload<float>(h->cl, cl);
+        if (rc) return rc;
+    }
     // solver scratch and status
     if ((rc = plan_cg(h.get()))) return rc;
     if ((rc = h->status.alloc(sizeof(DevStatus)))) return rc;
@@ -1019,11 +1067,11 @@ int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
     if (h->precision == EP_FP64) {
         CGArgs<double> ca;
         fill_cg_args<double>(h, ca);
-        rc = launch_cg<double>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
+        rc = half_diffusion<double>(h, ca);
     } else {
         CGArgs<float> ca;
         fill_cg_args<float>(h, ca);
-        rc = launch_cg<float>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
+        rc = half_diffusion<float>(h, ca);
     }
     if (rc) return rc;
     double last[2];

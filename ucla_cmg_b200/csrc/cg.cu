@@ -18,6 +18,8 @@
 // visibility; only r and p are read across blocks (through L2, ld.cg).
 // Dot products accumulate in FP64 whatever the vector type.  Reductions
 // sum the per-block partials in block order, so results are deterministic.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace ep {
@@ -453,6 +455,43 @@ template int cg_grid_size<float>(int, int *, int, int, int);
 template int cg_grid_size<double>(int, int *, int, int, int);
 template int cg_max_per_sm<float>(int, int *, int, int);
 template int cg_max_per_sm<double>(int, int *, int, int);
+
+// ---------------------------------------------------------------------------
+// One forward-Euler diffusion sub-step of the explicit scheme
+// (EP_ExplicitSolver::Solve, Solvers/EP_ExplicitSolver.cc:54-83):
+// out_i = V_i + h (D V)_i / C_L,i with D = -K in the SELL operator.
+template <typename R>
+__global__ void __launch_bounds__(256) k_explicit(int n, int nslices, const int *__restrict__ slice_ptr,
+                                                  const int *__restrict__ col, const R *__restrict__ Dval,
+                                                  const R *__restrict__ cl, const R *__restrict__ V, R *out, R h) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = gwarp; s < nslices; s += nwarps) {
+        const int row = s * kSlice + lane;
+        const int beg = slice_ptr[s], w = (slice_ptr[s + 1] - beg) / kSlice;
+        const R d = slice_row_sum<4>(col, Dval, beg, w, lane, [&](int c) { return __ldg(V + c); });
+        if (row < n) out[row] = V[row] + h * d / cl[row];
+    }
+}
+
+template <typename R>
+int launch_explicit(int n, int nslices, const int *slice_ptr, const int *col, const R *Dval, const R *cl, R *V,
+                    R *tmp, double h, cudaStream_t s) {
+    int dev = 0, nsm = 148;
+    EP_CUDA(cudaGetDevice(&dev));
+    EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = std::max(1, std::min(8 * nsm, (nslices + 7) / 8));
+    k_explicit<R><<<grid, 256, 0, s>>>(n, nslices, slice_ptr, col, Dval, cl, V, tmp, (R)h);
+    EP_CUDA(cudaGetLastError());
+    EP_CUDA(cudaMemcpyAsync(V, tmp, sizeof(R) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    return EP_OK;
+}
+
+template int launch_explicit<float>(int, int, const int *, const int *, const float *, const float *, float *,
+                                     float *, double, cudaStream_t);
+template int launch_explicit<double>(int, int, const int *, const int *, const double *, const double *, double *,
+                                      double *, double, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // pseudo-ECG: out[k] = sum_i W[k * wpitch + i] V[i], FP64 accumulation.

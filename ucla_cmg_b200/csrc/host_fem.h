@@ -15,8 +15,11 @@ struct HostCSR {
 
 // Returns 0, or -1 if an element has a non-positive Jacobian.
 // tets are zero-based.  s = dt/4 (+ smoothing 4 alpha / dt).
+// scheme 0: Crank-Nicolson (A = Cm M + s K, B = Cm M - s K); 1: backward
+// Euler (A = C_L + dt/2 K, B = diag C_L); 2: explicit (A = -K, B zero).
 int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *fibers,
-                const double D[3], double Cm, double dt, double smoothing_alpha, HostCSR &out);
+                const double D[3], double Cm, double dt, double smoothing_alpha, HostCSR &out,
+                int scheme = 0);
 
 // W[k * n + i] with ECG_k = sum_i W V_i (ComputeECG.h:30-189 with grad V
 // constant on a P1 tet).

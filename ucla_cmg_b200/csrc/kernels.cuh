@@ -76,6 +76,11 @@ template <typename R> struct IonicArgs {
     TTOpts tt;
     int mh_abs;
     const R *lr_table;           // nullable
+    // stride: the per-node adaptive sub-steps of the backward-Euler and
+    // explicit schemes (CardiacBody::getVoltageFromIonicCurrent) with base
+    // sub-step stride_dt, instead of the fixed sub_dt sequence
+    int stride;
+    R stride_dt;
 };
 
 template <typename R>
@@ -127,5 +132,10 @@ int launch_ecg(int n, int ne, const R *W, int wpitch, const R *V, double *partia
                unsigned int *slot = nullptr, int cap = 0);
 
 void launch_step_inc(long long *step, cudaStream_t s);
+// explicit scheme: V <- V + h (D V) / C_L over the SELL operator D = -K
+// (tmp: a scratch vector of n)
+template <typename R>
+int launch_explicit(int n, int nslices, const int *slice_ptr, const int *col, const R *Dval, const R *cl, R *V,
+                    R *tmp, double h, cudaStream_t s);
 
 }  // namespace ep

@@ -26,6 +26,9 @@ Same as the reference:
   State[0] for Mahajan, 0 mV for ten Tusscher and Luo-Rudy, hazard H1);
   ``--rest-voltage`` starts every model from its resting State[0] instead;
 * INITIALSTATES: the ``CELL`` block's values become every node's state;
+* ten Tusscher's Newton uses the true Jacobian by default: the reference's
+  transposed one (Tusscher.cc:173,181) diverges at dt >= 0.02 ms, with the
+  reference's own objects; ``--tt-reference-jacobian`` selects it;
 * CN solver with CG tolerance 1e-7 and 1000 iterations (EP_CrankNicholson.cc:
   104, 150); SMOOTHING alpha; output at t = 0 (unless READRESTART) and every
   ``int(FREQUENCY/DT)`` steps; restart files every ``long(WRITERESTART/DT)``
@@ -221,7 +224,8 @@ def read_initial_states(path):
     return np.array(cell), np.array(purk)
 
 
-def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate_path=None, verbose=True):
+def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate_path=None, verbose=True,
+        tt_jacobian=capi.TT_JAC_TRUE):
     cfg = parse_input(input_file)
     base_dir = cfg["input_dir"]
     model = CELL_MODELS[cfg["cell_model"].upper()]
@@ -243,7 +247,7 @@ def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate
     dt = cfg["dt"]
     g = Monodomain(mesh, model, precision, dt=dt, ionic_dt=cfg["ionic_dt"], D=cfg["D"], cg_tol=1e-7,
                    cg_maxit=1000, node_type=node_type, n_types=n_types, initial_states=init,
-                   smoothing_alpha=cfg["smoothing"] or 0.0, device=device)
+                   smoothing_alpha=cfg["smoothing"] or 0.0, tt_jacobian=tt_jacobian, device=device)
     if precision == capi.SURROGATE:
         from .surrogate import Surrogate, DEFAULT_PATH
         Surrogate.load(surrogate_path or DEFAULT_PATH).deploy(g)
@@ -303,9 +307,12 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"])
     ap.add_argument("--rest-voltage", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--tt-reference-jacobian", action="store_true",
+                    help="ten Tusscher Newton with the reference's transposed Jacobian (diverges at dt >= 0.02 ms)")
     a = ap.parse_args()
     prec = {"fp64": capi.FP64, "fp32": capi.FP32, "surrogate": capi.SURROGATE}[a.precision]
-    cfg, nsteps = run(a.input, prec, a.rest_voltage, a.device)
+    cfg, nsteps = run(a.input, prec, a.rest_voltage, a.device,
+                      tt_jacobian=capi.TT_JAC_REFERENCE if a.tt_reference_jacobian else capi.TT_JAC_TRUE)
     print(f"** {nsteps} steps done; output in {cfg['output_dir']}")
 
 
