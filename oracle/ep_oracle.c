@@ -1149,6 +1149,116 @@ void epo_sim_init(epo_sim *s, epo_csr *csr, double dt, double ionic_dt,
 void epo_sim_free(epo_sim *s)
 {
     free(s->V); free(s->istim); free(s->dvdt); free(s->b); free(s->ici);
+    free(s->A_be); free(s->B_be);
+}
+
+double epo_cells_ionic_node_cb(void *ctx, int i, double Cm, double dt, double V, double istim)
+{
+    epo_cells *c = (epo_cells *)ctx;
+    double *st = c->state + (size_t)i * c->nstate;
+    const int t = c->type ? c->type[i] : 0;
+    const double *k = c->consts + (size_t)t * c->nconst;
+    const double Xi = c->user_xi ? c->user_Xi : c->Xi;
+    if (c->model == EPO_TUSSCHER) {
+        int it = 0;
+        double kk[EPO_TT_NCONST];
+        const double *kp = k;
+        if (c->gks_scale) {
+            memcpy(kk, k, sizeof kk);
+            kk[15] *= c->gks_scale[i];
+            kp = kk;
+        }
+        return epo_tt_compute_ion(st, kp, Xi, Cm, dt, V, istim, c->newton_cap, c->tt_jac_true, &it);
+    }
+    if (c->model == EPO_MAHAJAN || c->model == EPO_MAHAJAN_FAIL) {
+        int sub = 0;
+        return epo_mh_compute_ion(st, k, Xi, Cm, dt, V, istim, c->mh_abs_mode, &sub);
+    }
+    return epo_lr_compute_ion(st, c->lr_table, Xi, Cm, dt, V, istim);
+}
+
+void epo_sim_set_scheme(epo_sim *s, int scheme, double dt_diff, epo_ionic_node_fn fn, void *ctx)
+{
+    const epo_csr *a = s->csr;
+    s->scheme = scheme;
+    s->ionic_node = fn;
+    s->ionic_ctx = ctx;
+    free(s->A_be); free(s->B_be);
+    s->A_be = s->B_be = NULL;
+    if (scheme == EPO_SCHEME_BE) {
+        /* the stiffness times dt/2 plus the lumped capacitance on the diagonal
+         * (EP_BackwardEuler.cc:13-30); the right side C_L V */
+        s->A_be = (double *)calloc((size_t)a->nnz, sizeof(double));
+        s->B_be = (double *)calloc((size_t)a->nnz, sizeof(double));
+        for (int i = 0; i < a->n; i++)
+            for (int k = a->rowptr[i]; k < a->rowptr[i + 1]; k++) {
+                s->A_be[k] = a->K[k] * (s->dt / 2.0);
+                if (a->col[k] == i) { s->A_be[k] += a->CL[i]; s->B_be[k] = a->CL[i]; }
+            }
+    } else if (scheme == EPO_SCHEME_EXPLICIT) {
+        /* EP_ExplicitSolver::Solve: steps of min(dtDiff, dt/2) while more
+         * than 1e-6 of the half step is left */
+        double solve = 0.5 * s->dt, st = dt_diff < 0.5 * s->dt ? dt_diff : 0.5 * s->dt;
+        s->nex = 0;
+        while (solve > 1e-6 && s->nex < 4096) {
+            s->ex_h[s->nex++] = st;
+            solve -= st;
+            st = st < solve ? st : solve;
+        }
+    }
+}
+
+/* CardiacBody::getVoltageFromIonicCurrent (CardiacBody.cc:819-904), per node:
+ * a first sub-step of dt_ion; when its rate, stored in an int, is 0 the
+ * stride becomes 5 dt_ion; then strides until dT, the last one shortened. */
+static void ionic_strides(epo_sim *s)
+{
+    const double dT = s->dt;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < s->n; i++) {
+        double dt = s->ionic_dt;
+        double V = s->V[i];
+        const double ist = s->istim[i];
+        if (dT / dt > 1.0) {
+            double iion = s->ionic_node(s->ionic_ctx, i, s->Cm, dt, V, ist);
+            V += dt * iion;
+            double totT = dt, delT;
+            const int slope = (int)iion;
+            if (!slope) dt *= 5;
+            int flag = 1;
+            while (flag) {
+                if (totT + dt > dT) { delT = dT - totT; flag = 0; }
+                else delT = dt;
+                iion = s->ionic_node(s->ionic_ctx, i, s->Cm, delT, V, ist);
+                V += delT * iion;
+                totT += delT;
+            }
+        } else {
+            const double iion = s->ionic_node(s->ionic_ctx, i, s->Cm, dt, V, ist);
+            V += dt * iion;
+        }
+        s->V[i] = V;
+    }
+}
+
+static void half_be(epo_sim *s)
+{
+    double rr;
+    epo_spmv(s->csr, s->B_be, s->V, s->b);
+    const int it = epo_pcg(s->csr, s->A_be, s->b, s->V, s->cg_tol, s->cg_maxit, s->jacobi_steps, &rr);
+    if (it < 0) { s->cg_fail++; s->cg_iters_total += s->cg_maxit; }
+    else s->cg_iters_total += it;
+}
+
+static void half_explicit(epo_sim *s)
+{
+    const int n = s->n;
+    for (int k = 0; k < s->nex; k++) {
+        const double h = s->ex_h[k];
+        epo_spmv(s->csr, s->csr->K, s->V, s->b);          /* K V; D = -K */
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) s->V[i] += h * (-s->b[i]) / s->csr->CL[i];
+    }
 }
 
 static void half_step(epo_sim *s)
@@ -1164,6 +1274,13 @@ void epo_sim_step(epo_sim *s)
 {
     const int n = s->n;
     const double *CL = s->csr->CL;
+    if (s->scheme == EPO_SCHEME_BE || s->scheme == EPO_SCHEME_EXPLICIT) {
+        if (s->scheme == EPO_SCHEME_BE) half_be(s); else half_explicit(s);
+        ionic_strides(s);
+        if (s->scheme == EPO_SCHEME_BE) half_be(s); else half_explicit(s);
+        s->step++;
+        return;
+    }
     half_step(s);
     for (int k = 0; k < s->nsub; k++) {
         const double h = s->sub_dt[k];

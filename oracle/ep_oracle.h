@@ -129,6 +129,13 @@ void epo_ecg_weights(int n, const double *xyz, int m, const int *tets,
 typedef void (*epo_ionic_fn)(void *ctx, double Cm, double dt, const double *V,
                              const double *istim, double *dvdt);
 
+/* one node's Compute_Ion (returns dV/dt, advances that node's state) */
+typedef double (*epo_ionic_node_fn)(void *ctx, int i, double Cm, double dt, double V, double istim);
+
+#define EPO_SCHEME_CN 0
+#define EPO_SCHEME_BE 1
+#define EPO_SCHEME_EXPLICIT 2
+
 typedef struct epo_sim {
     epo_csr *csr;
     int n;
@@ -140,14 +147,26 @@ typedef struct epo_sim {
     int nsub; double sub_dt[64];
     long long cg_iters_total; int cg_fail;
     long step;
+    /* scheme (EPSolver Method) and what the non-CN schemes need */
+    int scheme;
+    epo_ionic_node_fn ionic_node;
+    double *A_be, *B_be;    /* BE: C_L + dt/2 K and diag C_L on the csr pattern */
+    int nex; double ex_h[4096];   /* explicit: diffusion sub-steps of one half */
 } epo_sim;
 
 void epo_sim_init(epo_sim *s, epo_csr *csr, double dt, double ionic_dt,
                   double Cm, double cg_tol, int cg_maxit, int jacobi_steps,
                   epo_ionic_fn fn, void *ctx);
 void epo_sim_free(epo_sim *s);
-/* EP_CrankNicholson::Solve: D/2 - ionic sub-steps - D/2 */
+/* EP_CrankNicholson::Solve: D/2 - ionic sub-steps - D/2 (or the scheme set
+ * below) */
 void epo_sim_step(epo_sim *s);
+/* switch to EP_BackwardEuler (EP_BackwardEuler.cc:5-91) or EP_ExplicitSolver
+ * (EP_ExplicitSolver.cc:4-118, diffusion sub-step dt_diff); both advance the
+ * cells by CardiacBody::getVoltageFromIonicCurrent (CardiacBody.cc:819-904)
+ * through the per-node callback */
+void epo_sim_set_scheme(epo_sim *s, int scheme, double dt_diff, epo_ionic_node_fn fn, void *ctx);
+double epo_cells_ionic_node_cb(void *ctx, int i, double Cm, double dt, double V, double istim);
 void epo_cells_ionic_cb(void *ctx, double Cm, double dt, const double *V,
                         const double *istim, double *dvdt);
 

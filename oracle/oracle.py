@@ -54,7 +54,9 @@ class _Sim(C.Structure):
                 ("V", dp), ("istim", dp), ("dvdt", dp), ("b", dp), ("ici", dp),
                 ("ionic", C.c_void_p), ("ionic_ctx", C.c_void_p),
                 ("nsub", C.c_int), ("sub_dt", C.c_double * 64),
-                ("cg_iters_total", C.c_longlong), ("cg_fail", C.c_int), ("step", C.c_long)]
+                ("cg_iters_total", C.c_longlong), ("cg_fail", C.c_int), ("step", C.c_long),
+                ("scheme", C.c_int), ("ionic_node", C.c_void_p), ("A_be", dp), ("B_be", dp),
+                ("nex", C.c_int), ("ex_h", C.c_double * 4096)]
 
 
 def build():
@@ -87,6 +89,7 @@ def lib():
                                    C.c_void_p]
         L.epo_sim_free.argtypes = [C.POINTER(_Sim)]
         L.epo_sim_step.argtypes = [C.POINTER(_Sim)]
+        L.epo_sim_set_scheme.argtypes = [C.POINTER(_Sim), C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.epo_stim_schedule.argtypes = [C.c_int, dp, dp, C.c_double, C.c_long,
                                         C.POINTER(C.c_long), C.POINTER(C.c_long)]
         L.epo_num_steps.restype = C.c_long
@@ -126,6 +129,7 @@ def ref_lib():
                                    C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
                                    C.c_void_p]
         L.epo_sim_step.argtypes = [C.POINTER(_Sim)]
+        L.epo_sim_set_scheme.argtypes = [C.POINTER(_Sim), C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.epo_sim_free.argtypes = [C.POINTER(_Sim)]
         L.epo_set_threads.argtypes = [C.c_int]
         _REF = L
@@ -371,6 +375,17 @@ class Sim:
         self._L.epo_sim_init(C.byref(self.s), C.byref(csr.c), dt, ionic_dt, Cm, cg_tol,
                              cg_maxit, jacobi_steps, fn, ctx)
         self.n = csr.n
+
+    def set_scheme(self, scheme, dt_diff=0.05):
+        """EPO_SCHEME_BE (1) or EPO_SCHEME_EXPLICIT (2); the cells then move by
+        the reference's per-node ionic strides."""
+        if isinstance(self.cells, RefCells):
+            fn = C.cast(ref_lib().ref_cells_ionic_node_cb, C.c_void_p)
+            ctx = C.c_void_p(self.cells.h)
+        else:
+            fn = C.cast(lib().epo_cells_ionic_node_cb, C.c_void_p)
+            ctx = C.cast(self.cells.h, C.c_void_p)
+        self._L.epo_sim_set_scheme(C.byref(self.s), int(scheme), float(dt_diff), fn, ctx)
 
     @property
     def V(self):

@@ -153,6 +153,13 @@ void ref_cells_compute_ion(void *h, double Cm, double dt, const double *V,
         dvdt[i] = r->cells[i]->Compute_Ion(r->userXi, r->userXiSet, Cm, dt, V[i], istim[i]);
 }
 
+// one node's Compute_Ion, for the per-node strides of the non-CN schemes
+double ref_cells_ionic_node_cb(void *h, int i, double Cm, double dt, double V, double istim)
+{
+    RefCells *r = (RefCells *)h;
+    return r->cells[i]->Compute_Ion(r->userXi, r->userXiSet, Cm, dt, V, istim);
+}
+
 // adapter for the oracle's split-step driver
 void ref_cells_ionic_cb(void *h, double Cm, double dt, const double *V,
                         const double *istim, double *dvdt)

@@ -64,7 +64,7 @@ def _instance_descs(mesh, model, D, Cm, node_type, type_consts, n_types, gks_sca
 
 
 def _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, ecg_every,
-                 act_threshold):
+                 act_threshold, scheme=capi.SCHEME_CN, diffusion_dt=0.0):
     sd = capi.SolverDesc()
     sd.dt, sd.ionic_dt = float(dt), float(ionic_dt)
     sd.cg_tol, sd.cg_maxit = float(cg_tol), int(cg_maxit)
@@ -73,6 +73,8 @@ def _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, new
     sd.newton_tol = float(newton_tol)
     sd.ecg_every = int(ecg_every)
     sd.act_threshold = float(act_threshold)
+    sd.scheme = int(scheme)
+    sd.diffusion_dt = float(diffusion_dt)
     return sd
 
 
@@ -88,7 +90,12 @@ class Monodomain:
                  D=(1e-3, 5e-4, 2.5e-4), Cm=1.0, cg_tol=1e-7, cg_maxit=1000, node_type=None,
                  type_consts=None, n_types=None, gks_scale=None, user_xi=0.0, newton_cap=0,
                  tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0, initial_states=None,
-                 smoothing_alpha=0.0, newton_tol=0.0, ecg_every=0, act_threshold=-40.0, device=0):
+                 smoothing_alpha=0.0, newton_tol=0.0, ecg_every=0, act_threshold=-40.0, device=0,
+                 scheme=capi.SCHEME_CN, diffusion_dt=0.0):
+        """scheme: capi.SCHEME_CN (EP_CrankNicholson, the reference driver's),
+        SCHEME_BE (EP_BackwardEuler) or SCHEME_EXPLICIT (EP_ExplicitSolver,
+        diffusion sub-step diffusion_dt, 0: 0.05 ms).  cg_tol 0 takes the
+        scheme's own (1e-7 CN, 1e-10 BE)."""
         L = capi.lib()
         self.mesh = mesh
         self.model = model
@@ -98,7 +105,7 @@ class Monodomain:
         md, mo, self._keep = _instance_descs(mesh, model, D, Cm, node_type, type_consts, n_types, gks_scale,
                                              user_xi, newton_cap, tt_jacobian, mh_abs_mode, initial_states)
         sd = _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, ecg_every,
-                          act_threshold)
+                          act_threshold, scheme, diffusion_dt)
         h = C.c_void_p()
         check(L.ep_create(C.byref(md), C.byref(mo), C.byref(sd), int(device), C.byref(h)))
         self._h = h
