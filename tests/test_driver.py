@@ -91,3 +91,21 @@ def test_mesh_reader_skips_cables(tmp_path):
     (tmp_path / "mix.purk").write_text("2\n4 5\n")
     m, t, purk, other = IO.read_mesh(base)
     assert m.m == 1 and other == 1 and list(purk) == [4, 5]
+
+
+def test_schedule_matches_oracle_restatement():
+    """The driver's two-pointer schedule against the oracle's C restatement
+    of the same EPSimulator logic, on sorted and unsorted lists."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(1)
+    for trial in range(20):
+        k = int(rng.integers(1, 6))
+        t0 = np.round(rng.uniform(0, 20, k), 2)
+        if trial % 2 == 0:
+            t0 = np.sort(t0)
+        t1 = t0 + np.round(rng.uniform(0.5, 3, k), 2)
+        st = [dict(t_start=a, t_stop=b) for a, b in zip(t0, t1)]
+        ev = D.stimulus_events(st, 0.1, 300)
+        on, off = O.stim_schedule(t0, t1, 0.1, 300)
+        assert sorted((s, i) for s, i, f in ev if f) == sorted((int(s), i) for i, s in enumerate(on) if s >= 0)
+        assert sorted((s, i) for s, i, f in ev if not f) == sorted((int(s), i) for i, s in enumerate(off) if s >= 0)
