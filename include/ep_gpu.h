@@ -253,7 +253,8 @@ int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_
  * ionic kernel compiled for at least 3 or 4 resident 128-thread CTAs per SM
  * (fewer registers per thread), 0 = the compiler's register choice;
  * cg_batch: SELL columns whose gathers the CG kernel issues together (4 or
- * 8; 8 keeps more loads in flight at a larger register budget);
+ * 8; 8 keeps more loads in flight at a larger register budget; 16: groups of
+ * 8 with the next group's index loads issued before the current gathers);
  * cg_variant: 0 the CG recurrences of the reference (two reductions per
  * iteration), 1 the Chronopoulos-Gear recurrences (one reduction per
  * iteration; same iterates in exact arithmetic, rounding-level differences;

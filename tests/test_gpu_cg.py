@@ -86,3 +86,21 @@ def test_single_reduction_variant_in_tissue(gpu):
         g.close()
     assert np.max(out[0]) > 0.0
     assert np.max(np.abs(out[0] - out[1])) < 1e-6 * np.max(np.abs(out[0]))
+
+
+@pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
+def test_gather_widths_are_bit_identical(gpu, shell, prec):
+    """The gather width (4, 8, or 8 pipelined) changes which loads are in
+    flight together, not the order of the additions: same bits."""
+    wl, V, c = shell
+    out = []
+    for nb in (4, 8, 16):
+        g = Monodomain(wl.mesh, capi.TUSSCHER, prec, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
+        g.set_launch_config(cg_batch=nb, cg_per_sm=4)
+        g.set_voltage(V)
+        it, rr = g.diffusion_half_step()
+        out.append((g.voltage(), it))
+        g.close()
+    for x, it in out[1:]:
+        assert it == out[0][1]
+        assert np.array_equal(x, out[0][0])

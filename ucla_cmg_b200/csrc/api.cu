@@ -1232,7 +1232,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(h && cfg, "null argument");
     EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256 || cfg->cg_block == 512 || cfg->cg_block == 768,
                  "cg_block must be 128, 256, 512 or 768");
-    EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8, "cg_batch must be 4 or 8");
+    EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8 || cfg->cg_batch == 16, "cg_batch must be 4, 8 or 16");
     EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
@@ -1342,7 +1342,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     // CG: gather width x CTA size x CTAs per SM (all that fit, or half:
     // fewer CTAs make the grid barrier cheaper)
     const ep_launch_config cg0 = b;
-    for (int nb : {4, 8}) {
+    for (int nb : {4, 8, 16}) {
         for (int blk : {128, 256, 512, 768}) {
             int maxper = 0;
             if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant)

@@ -106,8 +106,50 @@ __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R 
     return acc;
 }
 
+// The same sum with the next group's column and value loads issued before
+// the current group's gathers (software pipelining: the index loads of
+// group k + 1 overlap the gathers of group k).  Same order of additions.
+template <int NB, typename R, typename F>
+__device__ __forceinline__ R slice_row_sum_pipe(const int *__restrict__ col, const R *__restrict__ val, int beg, int w,
+                                                int lane, F gather) {
+    R acc = R(0);
+    const int full = w / NB;
+    int c[NB], cn[NB];
+    R v[NB], vn[NB];
+    if (full > 0) {
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            const int idx = beg + u * kSlice + lane;
+            c[u] = __ldg(col + idx);
+            v[u] = __ldg(val + idx);
+        }
+    }
+    for (int b = 0; b < full; b++) {
+        const bool more = b + 1 < full;
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            const int idx = beg + ((b + 1) * NB + u) * kSlice + lane;
+            cn[u] = more ? __ldg(col + idx) : 0;
+            vn[u] = more ? __ldg(val + idx) : R(0);
+        }
+        R g[NB];
+#pragma unroll
+        for (int u = 0; u < NB; u++) g[u] = gather(c[u]);
+#pragma unroll
+        for (int u = 0; u < NB; u++) acc += v[u] * g[u];
+#pragma unroll
+        for (int u = 0; u < NB; u++) { c[u] = cn[u]; v[u] = vn[u]; }
+    }
+    for (int k = full * NB; k < w; k++) {
+        const int idx = beg + k * kSlice + lane;
+        acc += __ldg(val + idx) * gather(__ldg(col + idx));
+    }
+    return acc;
+}
+
 // register budget: NB = 4 takes 42 (six 256-thread CTAs, or two of 768, per
-// SM); NB = 8 takes 64 (four 256-thread CTAs) for twice the loads in flight
+// SM); NB = 8 takes 64 (four 256-thread CTAs) for twice the loads in flight;
+// NB = 16 is NB = 8 software-pipelined (64 registers)
 template <typename R, int NB>
 __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_half(const CGArgs<R> a) {
     const int lane = threadIdx.x & 31;
@@ -182,9 +224,10 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
                 const R *pcc = pc;
-                const R q = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, [&](int c) {
-                    return pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pcc + c));
-                });
+                auto gat = [&](int c) { return pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pcc + c)); };
+                R q;
+                if constexpr (NB == 16) q = slice_row_sum_pipe<8>(a.col, a.Aval, beg, w, lane, gat);
+                else q = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, gat);
                 if (row >= rb && row < re) {
                     const R pi = pdir(__ldg(a.dinv + row), a.r[row], bR, ldcg(pc + row));
                     pn[row] = pi;
@@ -402,10 +445,12 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
 template <typename R>
 int cg_max_per_sm(int block, int *per, int batch, int variant) {
     if (variant == 1) {
-        if (batch == 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 8>, block, 0));
+        if (batch >= 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 8>, block, 0));
         else EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 4>, block, 0));
     } else if (batch == 8) {
         EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 8>, block, 0));
+    } else if (batch == 16) {
+        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 16>, block, 0));
     } else {
         EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 4>, block, 0));
     }
@@ -439,10 +484,12 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch
     cfg.numAttrs = 1;
     if (variant == 1) {
         if (!a.r1 || !a.w0 || !a.w1 || !a.s0 || !a.s1) { set_error("single-reduction CG needs its vectors"); return EP_ERR_ARG; }
-        if (batch == 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 8>, a));
+        if (batch >= 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 8>, a));
         else EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 4>, a));
     } else if (batch == 8) {
         EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 8>, a));
+    } else if (batch == 16) {
+        EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 16>, a));
     } else {
         EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half<R, 4>, a));
     }
