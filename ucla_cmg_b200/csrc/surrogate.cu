@@ -32,7 +32,8 @@ constexpr int OFF_W3 = OFF_W2 + SG_W2 * 2;
 constexpr int OFF_W4 = OFF_W3 + SG_W3 * 2;
 constexpr int OFF_A = OFF_W4 + SG_W4 * 2;                 // 128 x 128 bf16
 constexpr int OFF_MISC = OFF_A + SG_M * SG_H * 2;
-constexpr int SG_SMEM = OFF_MISC + 64;
+constexpr int OFF_FLAGS = OFF_MISC + 64;                 // 2 x 128 envelope flags
+constexpr int SG_SMEM = OFF_FLAGS + 2 * SG_M;
 constexpr uint32_t SG_TMEM_COLS = 256;
 
 size_t surrogate_smem_bytes() { return SG_SMEM; }
@@ -183,6 +184,62 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *
     }
 }
 
+// One node's input row: features (V, 18 states, I_stim, G_Ks, G_to, s-gate),
+// logarithms of the wide-range ones, normalisation, BF16 row of A (K = 32
+// layout); returns whether the node is inside the training envelope.
+__device__ __forceinline__ bool build_row(const SurrogateArgs &a, const SurrogateAux *aux, long long step, bool raw,
+                                          int i, bool valid, int row, unsigned char *A) {
+    float xn[SG_KIN];
+#pragma unroll
+    for (int k = 0; k < SG_KIN; k++) xn[k] = 0.f;
+    bool inside = false;
+    if (valid && raw) {
+#pragma unroll
+        for (int k = 0; k < SG_KIN; k++) xn[k] = a.rawX[(size_t)i * SG_KIN + k];
+    } else if (valid) {
+        float x[SG_NF];
+        x[0] = a.V[i];
+#pragma unroll
+        for (int k = 0; k < 18; k++) x[k + 1] = a.S[(size_t)k * a.pitch + i];
+        const int ty = a.type ? a.type[i] : 0;
+        const float *c = a.consts + (size_t)ty * a.nconst;
+        float istim = 0.f;
+        if (a.stim_head) {
+            int k = a.stim_head[i];
+            long long best = -1;
+            while (k >= 0) {
+                const long long on = a.stim_on[k], off = a.stim_off[k];
+                if (step >= on && step < off && on > best) { best = on; istim = a.stim_amp[k]; }
+                k = a.stim_next[k];
+            }
+        }
+        x[19] = istim / (a.Cm * a.Xi);
+        x[20] = c[15] * (a.gks ? a.gks[i] : 1.f);
+        x[21] = c[20];
+        x[22] = c[53];
+        inside = (istim == 0.f);
+        const float m = x[7], h = x[8];
+        inside = inside && (m * m * m * h <= aux->nah_max);
+        const unsigned int lm = aux->log_mask;
+#pragma unroll
+        for (int k = 0; k < SG_NF; k++) {
+            // quantities spanning decades enter as logarithms
+            const float xt = ((lm >> k) & 1u) ? __logf(fmaxf(x[k], 1e-30f)) : x[k];
+            inside = inside && (xt >= aux->env_lo[k]) && (xt <= aux->env_hi[k]);
+            xn[k] = (xt - aux->in_mean[k]) * aux->in_rstd[k];
+        }
+    }
+    uint32_t w[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) w[j] = pack_bf16(xn[2 * j], xn[2 * j + 1]);
+#pragma unroll
+    for (int cch = 0; cch < 4; cch++) {
+        uint4 *dst = (uint4 *)(A + ((row >> 3) * (SG_KIN / 8) + cch) * 128 + (row & 7) * 16);
+        *dst = make_uint4(w[4 * cch], w[4 * cch + 1], w[4 * cch + 2], w[4 * cch + 3]);
+    }
+    return inside;
+}
+
 // The network over tiles of 128 nodes, 256 threads per CTA.  Threads
 // 0..127 own one node each (features, the output layer, the envelope
 // decision); all eight warps share the hidden-layer epilogues (warp w reads
@@ -222,60 +279,18 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
     const double t0 = (double)step * a.t_per_step;
     const int ntiles = (a.n + SG_M - 1) / SG_M;
 
+    // The rows of a tile are built by the owner threads for the first tile,
+    // then by the other half of the CTA while the owners finish the previous
+    // tile's output (A is free once the output layer's MMA has completed).
+    uint8_t *flags = smem + OFF_FLAGS;            // [2][SG_M]: inside the envelope
+    int buf = 0;
+    if (owner && (int)blockIdx.x < ntiles) {
+        const int i0 = (int)blockIdx.x * SG_M + row;
+        flags[row] = build_row(a, aux, step, raw, i0, i0 < a.n, row, A) ? 1 : 0;
+    }
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int i = tile * SG_M + row;
         const bool valid = owner && i < a.n;
-        float x[SG_NF];
-        bool inside = false;
-        if (owner) {
-            float xn[SG_KIN];
-#pragma unroll
-            for (int k = 0; k < SG_KIN; k++) xn[k] = 0.f;
-            if (valid && raw) {
-#pragma unroll
-                for (int k = 0; k < SG_KIN; k++) xn[k] = a.rawX[(size_t)i * SG_KIN + k];
-            } else if (valid) {
-                x[0] = a.V[i];
-#pragma unroll
-                for (int k = 0; k < 18; k++) x[k + 1] = a.S[(size_t)k * a.pitch + i];
-                const int ty = a.type ? a.type[i] : 0;
-                const float *c = a.consts + (size_t)ty * a.nconst;
-                float istim = 0.f;
-                if (a.stim_head) {
-                    int k = a.stim_head[i];
-                    long long best = -1;
-                    while (k >= 0) {
-                        const long long on = a.stim_on[k], off = a.stim_off[k];
-                        if (step >= on && step < off && on > best) { best = on; istim = a.stim_amp[k]; }
-                        k = a.stim_next[k];
-                    }
-                }
-                x[19] = istim / (a.Cm * a.Xi);
-                x[20] = c[15] * (a.gks ? a.gks[i] : 1.f);
-                x[21] = c[20];
-                x[22] = c[53];
-                inside = (istim == 0.f);
-                const float m = x[7], h = x[8];
-                inside = inside && (m * m * m * h <= aux->nah_max);
-                const unsigned int lm = aux->log_mask;
-#pragma unroll
-                for (int k = 0; k < SG_NF; k++) {
-                    // quantities spanning decades enter as logarithms
-                    const float xt = ((lm >> k) & 1u) ? __logf(fmaxf(x[k], 1e-30f)) : x[k];
-                    inside = inside && (xt >= aux->env_lo[k]) && (xt <= aux->env_hi[k]);
-                    xn[k] = (xt - aux->in_mean[k]) * aux->in_rstd[k];
-                }
-            }
-            // input row (K = 32 layout)
-            uint32_t w[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) w[j] = pack_bf16(xn[2 * j], xn[2 * j + 1]);
-#pragma unroll
-            for (int cch = 0; cch < 4; cch++) {
-                uint4 *dst = (uint4 *)(A + ((row >> 3) * (SG_KIN / 8) + cch) * 128 + (row & 7) * 16);
-                *dst = make_uint4(w[4 * cch], w[4 * cch + 1], w[4 * cch + 2], w[4 * cch + 3]);
-            }
-        }
         // layer 1 (K = 32), 2, 3 (K = 128): hidden, tanh
         const uint32_t sW[3] = {sW1, sW2, sW3};
         const float *bias[3] = {aux->b1, aux->b2, aux->b3};
@@ -302,7 +317,19 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
             issue_layer(d_out, sA, sW4, SG_H, SG_NOUT, bar);
         }
         if (!wait_commit(bar, phase, a.err)) break;
-        if (!owner) continue;
+        if (!owner) {
+            // the next tile's rows (its layer-1 MMA waits for the barrier at
+            // the top of the next iteration)
+            const int nt = tile + (int)gridDim.x;
+            if (nt < ntiles) {
+                const int i1 = nt * SG_M + row;
+                flags[(buf ^ 1) * SG_M + row] = build_row(a, aux, step, raw, i1, i1 < a.n, row, A) ? 1 : 0;
+            }
+            buf ^= 1;
+            continue;
+        }
+        const bool inside = flags[buf * SG_M + row] != 0;
+        buf ^= 1;
         uint32_t yv[32];
         tmem_ld32(d_out + lane_off, yv);
         tc_fence_before();
@@ -333,7 +360,7 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
 #pragma unroll
                 for (int j = 0; j < 6; j++) {
                     const int q = cslot[j];
-                    const float xk = x[q + 1];
+                    const float xk = a.S[(size_t)q * a.pitch + i];
                     a.pred[(size_t)j * a.pitch + i] = ((lm >> (q + 1)) & 1u) ? xk * __expf(d[q + 1]) : xk + d[q + 1];
                 }
             } else {
@@ -341,10 +368,10 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
 #pragma unroll
                 for (int k = 0; k < 18; k++) {
                     // log-scaled states are updated multiplicatively: x' = x exp(d)
-                    const float xk = x[k + 1];
+                    const float xk = a.S[(size_t)k * a.pitch + i];
                     a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
                 }
-                const float V0 = x[0], V1 = x[0] + d[0];
+                const float V0 = a.V[i], V1 = V0 + d[0];
                 a.V[i] = V1;
                 if (a.track) {
                     Track tr = a.track[i];
