@@ -174,7 +174,7 @@ int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block, i
         int dev = 0, nsm = 148;
         EP_CUDA(cudaGetDevice(&dev));
         EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        grid = std::min(grid, 4 * nsm);
+        grid = std::min(grid, 16 * nsm);   // one node per thread up to ~300K listed nodes
     }
     if constexpr (sizeof(R) == 8) {
         dispatch_ionic<R, 1>(model, a, grid, block, st);       // FP64: the compiler's register choice
