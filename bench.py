@@ -382,10 +382,13 @@ def run_accuracy(args, local):
     if wl.model == capi.TUSSCHER and abs(wl.dt - 0.1) < 1e-12:
         forms.append(("surrogate", capi.SURROGATE))
     hs = {}
+    tuned = {}
     for name, prec in forms:
         hs[name] = wl.create(prec, device=local)
         if prec == capi.SURROGATE:
             Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(hs[name])
+        if not args.no_tune:
+            tuned[name] = hs[name].autotune(20)[0]      # the state is put back afterwards
     res = {name: dict(ms=0.0, fb=0, vinf=0.0) for name, _ in forms}
     # the three runs advance in lockstep; Vm is compared every 1 ms
     for k in range(0, steps, per_ms):
@@ -407,7 +410,8 @@ def run_accuracy(args, local):
     out = {"workload": wl.name, "t_ms": args.accuracy, "n_nodes": int(wl.mesh.n), "dt_ms": wl.dt}
     for name, _ in forms:
         r = res[name]
-        e = {"node_steps_per_s": wl.mesh.n * steps / (r["ms"] * 1e-3), "fallback_fraction": r["fb"]}
+        e = {"node_steps_per_s": wl.mesh.n * steps / (r["ms"] * 1e-3), "fallback_fraction": r["fb"],
+             "launch_config": tuned.get(name)}
         if name != "fp64":
             both = (ref["ta"] >= 0) & (r["ta"] >= 0)
             da = np.abs(r["ta"] - ref["ta"])[both]
