@@ -1,15 +1,23 @@
 """Benchmark: node-steps/s of the monodomain split step on the ~2M-node shell.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain_fp32|fp64]
-                    [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--form surrogate|plain_fp32|fp64] [--impl ours|reference]
+                    [--workload shell_c2|slab_c0|slab_c1|batch_c3] [--t-start MS]
+                    [--no-tune] [--no-compare] [--no-cpu] [--accuracy MS]
 
 One step = one global dt (0.1 ms) of EP_CrankNicholson::Solve over the whole
-shell: half diffusion step (SpMV + Jacobi-PCG to 1e-7), 5 ionic sub-steps
-(ten Tusscher, endo/M/epi, PMJ stimuli), half diffusion step, and the
-pseudo-ECG every 10 steps.  Inputs (the operators and all cell states) are
-resident in HBM; they total > 126 MB, so no L2 flush is needed between
+shell: half diffusion step (SpMV + Jacobi-PCG to 1e-7), the ionic phase (ten
+Tusscher, endo/M/epi, PMJ stimuli; by default the learned form, with the
+plain FP32 form timed over the same window for the ratio), half diffusion
+step, and the pseudo-ECG every 10 steps.  The timed window starts at
+--t-start (40 ms) after an untimed advance, and each form's launch shape is
+picked by the autotuner first.  Inputs (the operators and all cell states)
+are resident in HBM; they total > 126 MB, so no L2 flush is needed between
 steps.  Multi-GPU: independent replicas (the path does not shard), weak
 scaling, timing = max over ranks of the device (CUDA-event) time.
+
+--accuracy MS runs the workload that long in FP64, FP32 and the learned form
+in lockstep and prints the errors against FP64 instead of timing.
 
 --impl reference times the reference's own CPU implementation on the host
 cores: the reference cell-model sources compiled unmodified (oracle/_ref)
