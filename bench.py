@@ -324,6 +324,11 @@ def run_ours(args, rank, world, local):
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"5 steps (after 1 untimed) of a {ncpu}-node shell "
                                           f"(h={h} cm) from t=0, same model, dt and stimuli"}
+        # the same path on one host thread (the reference runs one MPI rank
+        # per core; this is one rank's speed), on a coarser sample
+        n1, t1, _ = cpu_sample("reference", 0.2, 3, 1)
+        line["cpu_baseline"]["value_1_thread"] = n1 * 2 / sum(t1[1:])
+        line["cpu_baseline"]["sample_1_thread"] = f"2 steps (after 1 untimed) of a {n1}-node shell (h=0.2 cm)"
     g.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
