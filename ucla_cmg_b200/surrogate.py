@@ -160,9 +160,9 @@ def features(states, istim_pApF, gks_abs, gto, sflag):
     return X
 
 
-def in_domain(states, istim):
+def in_domain(states, istim, nah_max=NAH_MAX):
     m, h = states[:, 7], states[:, 8]
-    return (m ** 3 * h <= NAH_MAX) & (istim == 0.0)
+    return (m ** 3 * h <= nah_max) & (istim == 0.0)
 
 
 def _random_slab(rng):
@@ -200,7 +200,8 @@ def _random_slab(rng):
     return m, node_type, tc, gks, ids, t_on, amp
 
 
-def generate(n_target=10_000_000, seed=0, T=500.0, every=5, device=0, verbose=True, max_runs=64):
+def generate(n_target=10_000_000, seed=0, T=500.0, every=5, device=0, verbose=True, max_runs=64,
+             nah_max=NAH_MAX):
     """Training pairs (X, Y) from randomised plain-model slab runs.
     X: (N, 23) inputs; Y: (N, 19) changes of V and the 18 states over one
     0.1 ms step's ionic phase (plain FP64 model from the same start)."""
@@ -225,7 +226,7 @@ def generate(n_target=10_000_000, seed=0, T=500.0, every=5, device=0, verbose=Tr
             istim = np.zeros(m.n)
             act = (t_on <= t) & (t < t_on + 2.0)
             istim[ids[act]] = amp
-            keep = in_domain(st, istim)
+            keep = in_domain(st, istim, nah_max)
             # keep every state on the way to threshold (the foot of the action
             # potential decides activation times), 20% of the plateau and
             # repolarisation, 4% of rest
@@ -331,7 +332,7 @@ class Trainer:
             pass
 
 
-def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, w_v=10.0,
+def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, w_v=10.0, nah_max=NAH_MAX,
           asinh_q=None, conc_only=False):
     """Fit the network to normalised (X, Y) on the GPU; returns a Surrogate.
 
@@ -425,7 +426,7 @@ def train(X, Y, epochs=20, batch=8192, lr=2e-3, seed=0, device=0, verbose=True, 
     p = tr.params()
     tr.close()
     return Surrogate(p, in_mean, in_std, out_mean, out_std, env_lo.astype(np.float32),
-                     env_hi.astype(np.float32), nah_max=NAH_MAX, log_mask=LOG_MASK,
+                     env_hi.astype(np.float32), nah_max=nah_max, log_mask=LOG_MASK,
                      out_scale=out_scale, out_lo=out_lo, out_hi=out_hi,
                      v_update=2 if conc_only else 0, hybrid_substeps=1,
                      meta={"n_samples": int(n), "epochs": epochs, "lr": lr, "batch": batch,
@@ -444,6 +445,8 @@ def main():
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--asinh-q", type=float, default=None)
     ap.add_argument("--data", default=None, help="cache of the generated pairs (.npz)")
+    ap.add_argument("--nah-max", type=float, default=NAH_MAX,
+                    help="largest fast sodium gate product m^3 h the network takes (the upstroke bound)")
     ap.add_argument("--conc-only", action="store_true",
                     help="fit only the six Newton concentrations (hybrid form)")
     args = ap.parse_args()
@@ -452,12 +455,12 @@ def main():
         z = np.load(args.data)
         X, Y = z["X"], z["Y"]
     else:
-        X, Y = generate(args.samples, seed=args.seed)
+        X, Y = generate(args.samples, seed=args.seed, nah_max=args.nah_max)
         if args.data:
             np.savez(args.data, X=X, Y=Y)
     print(f"data: {X.shape} in {time.time() - t0:.1f} s", flush=True)
     t1 = time.time()
-    s = train(X, Y, epochs=args.epochs, seed=args.seed, lr=args.lr, batch=args.batch,
+    s = train(X, Y, epochs=args.epochs, seed=args.seed, lr=args.lr, batch=args.batch, nah_max=args.nah_max,
               asinh_q=args.asinh_q, conc_only=args.conc_only)
     print(f"training: {time.time() - t1:.1f} s", flush=True)
     s.save(args.out)
