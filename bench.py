@@ -45,6 +45,23 @@ WORKLOAD_TEXT = {
 UNIT = "node-steps/s"
 
 
+def max_over_ranks(ms, dist):
+    """The slowest rank's device time (replicas: the job ends with it)."""
+    if dist is None:
+        return ms
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(ms)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_nodes, steps, world, ms):
+    """Whole-job node-steps/s: every rank advances its own copy of the
+    workload, so the job does world x n x steps node-steps in max-rank time."""
+    return n_nodes * steps * world / (ms * 1e-3)
+
+
 def _env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
@@ -244,13 +261,10 @@ def run_ours(args, rank, world, local):
     st = g.step(args.steps)
     clocks = clk.stop()
     torch.cuda.synchronize()
-    ms = st["device_ms"]
+    ms = max_over_ranks(st["device_ms"], dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = n * args.steps * world / (ms * 1e-3)
+    value = replica_value(n, args.steps, world, ms)
     # ---- end to end through the public API with host buffers ----
     states = g.states()
     V = g.voltage()
@@ -310,7 +324,7 @@ def run_ours(args, rank, world, local):
         gp.step(args.warmup)
         torch.cuda.synchronize()
         stp = gp.step(args.steps)
-        vp = n * args.steps * world / (stp["device_ms"] * 1e-3)
+        vp = replica_value(n, args.steps, world, max_over_ranks(stp["device_ms"], dist))
         line["config"]["plain_fp32"] = {"value": vp, "ms_per_step": stp["device_ms"] / args.steps,
                                         "launch_config": gp.launch_config(),
                                         "cg_iters_per_solve": stp["cg_iters"] / max(1, 2 * args.steps)}
@@ -354,13 +368,10 @@ def run_batch(args, rank, world, local, dist, prec):
     st = b.step(args.steps)
     clocks = clk.stop()
     torch.cuda.synchronize()
-    ms = st["device_ms"]
+    ms = max_over_ranks(st["device_ms"], dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    line = {"metric": "node-steps/s, 64 independent slabs in one batch", "value": n * args.steps * world / (ms * 1e-3),
+    line = {"metric": "node-steps/s, 64 independent slabs in one batch", "value": replica_value(n, args.steps, world, ms),
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == capi.FP64 else "f32", "data": "synthetic",

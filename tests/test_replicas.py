@@ -1,0 +1,51 @@
+"""The bench's multi-GPU logic on CPU: two gloo ranks (replicas, no data
+collective), max-over-ranks timing, whole-job value; the reference arm does
+its work on rank 0 only."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import bench
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    ms = bench.max_over_ranks(10.0 + 5.0 * rank, dist)
+    v = bench.replica_value(1000, 20, world, ms)
+    out.put((rank, ms, v))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_replicas_max_over_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == [15.0, 15.0]                 # both ranks see the slowest
+    assert res[0][2] == res[1][2] == pytest.approx(2 * 1000 * 20 / 15e-3)
+
+
+def test_reference_arm_only_on_rank0(capsys):
+    class A:
+        gpus, steps, warmup = 2, 1, 1
+    assert bench.run_reference(A, 1, 2) is None
+    assert capsys.readouterr().out == ""
