@@ -104,3 +104,62 @@ def test_gather_widths_are_bit_identical(gpu, shell, prec):
     for x, it in out[1:]:
         assert it == out[0][1]
         assert np.array_equal(x, out[0][0])
+
+
+def _slab_run(var=0, predict=0, prec=capi.FP64, steps=400, graph_steps=0):
+    from ucla_cmg_b200 import mesh as M
+    m = M.slab(21, 21, 5, 0.4, 0.4, 0.08)
+    blk = M.corner_block(m, 3, 3)
+    g = Monodomain(m, capi.TUSSCHER, prec, dt=0.02, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
+                   cg_tol=1e-10 if prec == capi.FP64 else 1e-7, tt_jacobian=capi.TT_JAC_TRUE)
+    g.set_launch_config(cg_variant=var, cg_predict=predict, graph_steps=graph_steps)
+    g.set_voltage(-85.423)
+    g.set_stimulus(blk, 0.0, 1.0, 50.0 * 2000.0)
+    st = g.step(steps)
+    V = g.voltage()
+    return g, V, st
+
+
+@pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
+def test_predictor_in_tissue(gpu, prec):
+    """Starting each solve from V + the previous correction of the same half
+    step: the stop test is the reference's (relative to B V - A V), so the
+    field agrees with the plain start to the CG tolerance's level, in fewer
+    iterations, and no solve fails."""
+    g0, V0, st0 = _slab_run(0, 0, prec)
+    g0.close()
+    g1, V1, st1 = _slab_run(0, 1, prec)
+    assert g1.launch_config()["cg_predict"] == 1
+    g1.close()
+    assert np.max(V0) > 0.0
+    assert st1["cg_failures"] == 0 and st1["nonfinite"] == 0
+    tol = 1e-6 if prec == capi.FP64 else 2e-4
+    assert np.max(np.abs(V0 - V1)) < tol * np.max(np.abs(V0)), np.max(np.abs(V0 - V1))
+    assert st1["cg_iters"] < st0["cg_iters"], (st1["cg_iters"], st0["cg_iters"])
+
+
+def test_predictor_restarts_on_voltage_upload(gpu):
+    """A voltage upload restarts the predictor from zero, so a run from an
+    uploaded state repeats bit for bit (also under graph replay)."""
+    for gs in (0, 50):
+        g, V, st = _slab_run(0, 1, steps=100, graph_steps=gs)
+        S = g.states()
+        out = []
+        for rep in range(2):
+            g.set_states(S)
+            g.set_voltage(V)
+            g.step(100)
+            out.append(g.voltage())
+        g.close()
+        assert np.max(out[0]) > 0.0
+        assert np.array_equal(out[0], out[1])
+
+
+def test_predictor_needs_two_reduction_variant(gpu):
+    from ucla_cmg_b200 import mesh as M
+    m = M.slab(6, 6, 3, 0.4, 0.4, 0.08)
+    g = Monodomain(m, capi.TUSSCHER, capi.FP64, dt=0.02, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2))
+    with pytest.raises(capi.EPError):
+        g.set_launch_config(cg_variant=1, cg_predict=1)
+    assert g.launch_config()["cg_predict"] == 0
+    g.close()

@@ -75,6 +75,7 @@ struct ep_handle {
     // device memory
     DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
+    DBuf pd0, pd1, pvin;                 // CG predictor: x - V of the first / second half step, scratch
     DBuf partial, bar, status, cg_stats, cg_last, d_step, track;
     DBuf stim_head, stim_next, stim_on, stim_off, stim_amp;
     int nstim = 0;
@@ -100,7 +101,8 @@ struct ep_handle {
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
-    int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, ionic_block = 128, ionic_min = 0, graph_steps = 0;
+    int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, cg_predict = 0, ionic_block = 128, ionic_min = 0,
+        graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
@@ -208,6 +210,15 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.inst_blk = h->d_inst_blk.as<int>();
     a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
+    a.delta = nullptr; a.vin = nullptr;      // the time step sets the predictor per half step
+}
+
+// start the CG predictor from x0 = V again (after a state upload or when it
+// is switched on)
+static int reset_predictor(ep_handle *h) {
+    for (DBuf *b : {&h->pd0, &h->pd1})
+        if (b->p) EP_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, h->stream));
+    return EP_OK;
 }
 
 template <typename R>
@@ -433,8 +444,13 @@ template <typename R>
 static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     IonicArgs<R> ia;
     fill_ionic_args<R>(h, ia);
-    CGArgs<R> ca;
+    CGArgs<R> ca, ca2;
     fill_cg_args<R>(h, ca);
+    ca2 = ca;
+    if (h->cg_predict) {
+        ca.delta = h->pd0.as<R>(); ca2.delta = h->pd1.as<R>();
+        ca.vin = ca2.vin = h->pvin.as<R>();
+    }
     int rc;
     for (int s = 0; s < nsteps; s++) {
         if ((rc = mark(h, ne, K_CG))) return rc;
@@ -451,7 +467,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
-        if ((rc = half_diffusion<R>(h, ca))) return rc;
+        if ((rc = half_diffusion<R>(h, ca2))) return rc;
         if ((rc = mark(h, ne, K_OTHER))) return rc;
         launch_step_inc(h->d_step.as<long long>(), h->stream);
         h->launches += 4;
@@ -829,6 +845,8 @@ static int put_voltage(ep_handle *h, const double *V) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < h->n; i++) st[i] = (R)V[i];
     EP_CUDA(cudaMemcpyAsync(h->V.p, st, sizeof(R) * h->n, cudaMemcpyHostToDevice, h->stream));
+    int rc = reset_predictor(h);
+    if (rc) return rc;
     EP_CUDA(cudaStreamSynchronize(h->stream));
     return EP_OK;
 }
@@ -1218,6 +1236,7 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     cfg->cg_block = h->cg_block;
     cfg->cg_batch = h->cg_batch;
     cfg->cg_variant = h->cg_variant;
+    cfg->cg_predict = h->cg_predict;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1234,6 +1253,8 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
                  "cg_block must be 128, 256, 512 or 768");
     EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8 || cfg->cg_batch == 16, "cg_batch must be 4, 8 or 16");
     EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
+    EP_CHECK_ARG(cfg->cg_predict == 0 || cfg->cg_predict == 1, "cg_predict must be 0 or 1");
+    EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
     EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
@@ -1253,6 +1274,18 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
         plan_cg(h);
         return rc;
     }
+    if (cfg->cg_predict && !h->pd0.p) {
+        const size_t vb = (size_t)h->pitch * h->rsize;
+        for (DBuf *b : {&h->pd0, &h->pd1, &h->pvin}) {
+            if ((rc = b->alloc(vb))) return rc;
+            EP_CUDA(cudaMemset(b->p, 0, vb));
+        }
+    }
+    if (cfg->cg_predict && !h->cg_predict) {
+        if ((rc = reset_predictor(h))) return rc;
+        EP_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    h->cg_predict = cfg->cg_predict;
     h->ionic_block = cfg->ionic_block;
     h->ionic_min = cfg->ionic_min_ctas;
     h->graph_steps = cfg->graph_steps;
@@ -1262,7 +1295,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
 namespace {
 // device state that stepping changes, saved and put back around tuning trials
 struct Snapshot {
-    DBuf V, S, track, d_step, slot;
+    DBuf V, S, track, d_step, slot, pd0, pd1;
     long long step = 0;
     int ecg_count = 0;
     std::vector<double> ecg_t;
@@ -1274,8 +1307,10 @@ int snap_copy(DBuf &dst, const DBuf &src, cudaStream_t s, bool to_snapshot) {
         int rc = dst.alloc(src.bytes);
         if (rc) return rc;
         EP_CUDA(cudaMemcpyAsync(dst.p, src.p, src.bytes, cudaMemcpyDeviceToDevice, s));
-    } else {
+    } else if (dst.p) {
         EP_CUDA(cudaMemcpyAsync((void *)src.p, dst.p, src.bytes, cudaMemcpyDeviceToDevice, s));
+    } else {
+        EP_CUDA(cudaMemsetAsync((void *)src.p, 0, src.bytes, s));   // allocated after the save: from zero
     }
     return EP_OK;
 }
@@ -1287,6 +1322,8 @@ int snapshot(ep_handle *h, Snapshot &sn, bool save) {
     if ((rc = snap_copy(sn.track, h->track, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.d_step, h->d_step, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.slot, h->ecg_slot, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.pd0, h->pd0, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.pd1, h->pd1, h->stream, save))) return rc;
     if (save) {
         sn.step = h->step; sn.ecg_count = h->ecg_count; sn.ecg_t = h->ecg_t;
     } else {
@@ -1314,6 +1351,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     cur.cg_block = h->cg_block;
     cur.cg_batch = h->cg_batch;
     cur.cg_variant = h->cg_variant;
+    cur.cg_predict = h->cg_predict;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
     cur.ionic_min_ctas = h->ionic_min;
@@ -1362,6 +1400,13 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     {
         ep_launch_config c = b;
         c.cg_variant = 1 - b.cg_variant;
+        c.cg_predict = 0;
+        const double t = trial(c);
+        if (t >= 0 && t < t_best) { t_best = t; b = c; }
+    }
+    if (b.cg_variant == 0 && h->scheme != EP_SCHEME_EXPLICIT) {
+        ep_launch_config c = b;
+        c.cg_predict = 1 - b.cg_predict;
         const double t = trial(c);
         if (t >= 0 && t < t_best) { t_best = t; b = c; }
     }

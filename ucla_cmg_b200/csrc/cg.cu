@@ -173,37 +173,47 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     const int nwarps = (nb * (int)blockDim.x) >> 5;
 
     // ---- prologue: r = B x - A x, z = dinv r, p = 0 ----
+    // With a predictor (delta: the previous solve's correction x - V of
+    // this half step) the iteration starts from x + delta instead, r = B x -
+    // A (x + delta), while the stop test keeps the reference's r0 = B x - A x;
+    // x itself is not touched before the barrier (neighbours read it here).
+    const bool pred = a.delta != nullptr;
     {
-        double v[3] = {0.0, 0.0, 0.0};
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = gwarp; s < s_hi; s += nwarps) {
             const int row = s * kSlice + lane;
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-            R ax = R(0), bx = R(0);
+            R ax = R(0), bx = R(0), ad = R(0);
             for (int k = 0; k < w; k++) {
                 const int idx = beg + k * kSlice + lane;
                 const int c = __ldg(a.col + idx);
                 const R xv = a.x[c];
-                ax += __ldg(a.Aval + idx) * xv;
+                const R av = __ldg(a.Aval + idx);
+                ax += av * xv;
                 bx += __ldg(a.Bval + idx) * xv;
+                if (pred) ad += av * a.delta[c];
             }
             if (row >= rb && row < re) {
-                const R r = bx - ax;
+                const R rref = bx - ax;
+                const R r = pred ? rref - ad : rref;
                 const R z = __ldg(a.dinv + row) * r;
                 a.r[row] = r;
                 a.p0[row] = R(0);
+                if (pred) a.vin[row] = a.x[row];
                 v[0] += (double)r * (double)z;
                 v[1] += (double)r * (double)r;
                 v[2] += (double)bx * (double)bx;
+                v[3] += (double)rref * (double)rref;
             }
         }
-        block_reduce_store<3>(v, a.partial, G);
+        block_reduce_store<4>(v, a.partial + 6 * G, G);      // slots [6G, 10G): the iterations use [0, 4G)
     }
     if (!grid_sync(bar, nblk)) return;
-    double rz, rr0, bb;
+    double rz, rr_start, bb, rr0;
     {
-        double t[3];
-        grid_total<3>(a.partial, G, b0, nb, t);
-        rz = t[0]; rr0 = t[1]; bb = t[2];
+        double t[4];
+        grid_total<4>(a.partial + 6 * G, G, b0, nb, t);
+        rz = t[0]; rr_start = t[1]; bb = t[2]; rr0 = t[3];
     }
     // ||r|| <= tol ||r0||, or the residual is at the resolution of b in the
     // vector type (FP32 cannot resolve a 1e-7 reduction of an r0 that is
@@ -212,8 +222,8 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     const double stop2 = fmax(a.tol * a.tol * rr0, floor2);
     double beta = 0.0;
     int it = 0;
-    bool converged = (rr0 <= stop2);
-    double rr_last = rr0;
+    bool converged = (rr_start <= stop2);
+    double rr_last = rr_start;
     R *pc = a.p0, *pn = a.p1;
     while (!converged && it < a.maxit) {
         // ---- phase A: p' = z + beta p; q = A p' ----
@@ -272,6 +282,19 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         beta = t[0] / rz;
         rz = t[0];
         R *tmp = pc; pc = pn; pn = tmp;
+    }
+    if (pred) {
+        // the solution x + delta, and the correction this solve made, for the
+        // next solve of this half step (own rows; every block is past the
+        // prologue's reads of delta)
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            if (row >= rb && row < re) {
+                const R xf = a.x[row] + a.delta[row];
+                a.x[row] = xf;
+                a.delta[row] = xf - a.vin[row];
+            }
+        }
     }
     if ((int)blockIdx.x == b0 && threadIdx.x == 0) {
         atomicAdd(a.iters_total, (unsigned long long)it);
