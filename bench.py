@@ -130,35 +130,46 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic(kernel, form, cg_iters):
+def _traffic(kernel, form, cg_iters, cg_predict=0):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/traffic.json); the CG launch's bytes grow with its
-    iteration count, so they are stored as prologue + per iteration."""
+    iteration count, so they are stored as prologue + per iteration, plus the
+    predictor's own passes when one is on (None if that was not captured)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
     except Exception:
         return None
     if kernel == "cg" and "cg" in t:
-        return t["cg"]["prologue_bytes"] + cg_iters * t["cg"]["per_iteration_bytes"]
+        extra = 0
+        if cg_predict:
+            extra = t["cg"].get("predict_extra_bytes", {}).get(str(cg_predict))
+            if extra is None:
+                return None
+        return t["cg"]["prologue_bytes"] + extra + cg_iters * t["cg"]["per_iteration_bytes"]
     if kernel == "ionic":
         return t.get("surrogate" if form == "surrogate" else "ionic_plain_fp32" if form == "plain_fp32" else "-")
     return None
 
 
-def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_every=10):
+def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_every=10, cg_predict=0):
     """Bytes one launch must move at minimum.
 
     cg (one half diffusion step, SELL values + int32 columns):
       prologue  nnz*(A + B + col) + n*(x + dinv + r_write + p_write)
       iteration nnz*(A + col) + n*(r, dinv, p_old read + p_new, q write)   [phase A]
                 + n*(p_new, x, r, q, dinv read + x, r write)                [phase B]
+      predictor (cg_predict k = 1, 2): n*(k corrections read + V saved) in the
+                prologue, n*(x, V, k corrections read + x, k corrections
+                written) after the iterations
     ionic: the V + stored states read and written once, the activation
       record read (16 B), node type (1 B), G_Ks scale and stimulus head (4 B each).
     ecg: V and the ne weight rows read once per sample.
     """
     if kernel == "cg":
         pro = nnz * (2 * rbytes + 4) + n * 4 * rbytes
+        if cg_predict:
+            pro += n * rbytes * ((cg_predict + 1) + (2 + cg_predict + 1 + cg_predict))
         it = nnz * (rbytes + 4) + n * 5 * rbytes + n * 7 * rbytes
         return pro + cg_iters_per_solve * it
     if kernel == "ionic":
@@ -251,6 +262,8 @@ def run_ours(args, rank, world, local):
         g.step(min(500, pre - k))
     # the project's autotuner picks the launch shape (state is restored)
     tuned = g.autotune(20) if not args.no_tune else None
+    if args.launch:
+        g.set_launch_config(**json.loads(args.launch))
     g.set_profiling(True)
     g.step(args.warmup)
     torch.cuda.synchronize()
@@ -291,11 +304,11 @@ def run_ours(args, rank, world, local):
     per_launch_ms = kms[dom] / max(1, launches[dom])
     nstate = capi.model_nstate(wl.model)
     alg = algorithmic_bytes(dom, n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes),
-                            ecg_every=ecg_every)
+                            ecg_every=ecg_every, cg_predict=g.launch_config()["cg_predict"])
     peak, peak_kind = _peaks()
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom, args.form, cg_per_solve) if wl.name == "shell_c2" else None,
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom, args.form, cg_per_solve, g.launch_config()["cg_predict"]) if wl.name == "shell_c2" else None,
             "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
             "kernel_ms": kms}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -472,6 +485,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3", "slab_c0", "slab_c1"])
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--launch", default="", help='launch-shape fields set after tuning, JSON ({"cg_predict": 2})')
     ap.add_argument("--no-compare", action="store_true",
                     help="surrogate form: skip the plain FP32 run over the same window")
     ap.add_argument("--t-start", type=float, default=40.0,

@@ -262,8 +262,10 @@ int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_
 typedef struct ep_launch_config {
     int32_t cg_block, cg_per_sm, ionic_block, graph_steps, ionic_min_ctas, cg_batch, cg_variant;
     int32_t cg_predict;   /* 1: each CG solve starts from V + the previous solve's
-                             correction of the same half step (cg_variant 0 only);
-                             the stop test stays relative to B V - A V */
+                             correction of the same half step; 2: from V + the
+                             linear extrapolation of the last two corrections
+                             (cg_variant 0 only); the stop test stays relative
+                             to B V - A V */
 } ep_launch_config;
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);

@@ -121,15 +121,17 @@ def _slab_run(var=0, predict=0, prec=capi.FP64, steps=400, graph_steps=0):
 
 
 @pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
-def test_predictor_in_tissue(gpu, prec):
+@pytest.mark.parametrize("predict", [1, 2])
+def test_predictor_in_tissue(gpu, prec, predict):
     """Starting each solve from V + the previous correction of the same half
-    step: the stop test is the reference's (relative to B V - A V), so the
-    field agrees with the plain start to the CG tolerance's level, in fewer
-    iterations, and no solve fails."""
+    step (or the linear extrapolation of the last two): the stop test is the
+    reference's (relative to B V - A V), so the field agrees with the plain
+    start to the CG tolerance's level, in fewer iterations, and no solve
+    fails."""
     g0, V0, st0 = _slab_run(0, 0, prec)
     g0.close()
-    g1, V1, st1 = _slab_run(0, 1, prec)
-    assert g1.launch_config()["cg_predict"] == 1
+    g1, V1, st1 = _slab_run(0, predict, prec)
+    assert g1.launch_config()["cg_predict"] == predict
     g1.close()
     assert np.max(V0) > 0.0
     assert st1["cg_failures"] == 0 and st1["nonfinite"] == 0
@@ -141,8 +143,8 @@ def test_predictor_in_tissue(gpu, prec):
 def test_predictor_restarts_on_voltage_upload(gpu):
     """A voltage upload restarts the predictor from zero, so a run from an
     uploaded state repeats bit for bit (also under graph replay)."""
-    for gs in (0, 50):
-        g, V, st = _slab_run(0, 1, steps=100, graph_steps=gs)
+    for gs, predict in ((0, 1), (50, 1), (50, 2)):
+        g, V, st = _slab_run(0, predict, steps=100, graph_steps=gs)
         S = g.states()
         out = []
         for rep in range(2):

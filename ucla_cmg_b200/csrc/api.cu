@@ -76,6 +76,7 @@ struct ep_handle {
     DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
     DBuf pd0, pd1, pvin;                 // CG predictor: x - V of the first / second half step, scratch
+    DBuf pq0, pq1;                       // linear CG predictor: the corrections one step older
     DBuf partial, bar, status, cg_stats, cg_last, d_step, track;
     DBuf stim_head, stim_next, stim_on, stim_off, stim_amp;
     int nstim = 0;
@@ -210,13 +211,13 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.inst_blk = h->d_inst_blk.as<int>();
     a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
-    a.delta = nullptr; a.vin = nullptr;      // the time step sets the predictor per half step
+    a.delta = nullptr; a.delta_prev = nullptr; a.vin = nullptr;   // the time step sets the predictor
 }
 
 // start the CG predictor from x0 = V again (after a state upload or when it
 // is switched on)
 static int reset_predictor(ep_handle *h) {
-    for (DBuf *b : {&h->pd0, &h->pd1})
+    for (DBuf *b : {&h->pd0, &h->pd1, &h->pq0, &h->pq1})
         if (b->p) EP_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, h->stream));
     return EP_OK;
 }
@@ -450,6 +451,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     if (h->cg_predict) {
         ca.delta = h->pd0.as<R>(); ca2.delta = h->pd1.as<R>();
         ca.vin = ca2.vin = h->pvin.as<R>();
+        if (h->cg_predict == 2) { ca.delta_prev = h->pq0.as<R>(); ca2.delta_prev = h->pq1.as<R>(); }
     }
     int rc;
     for (int s = 0; s < nsteps; s++) {
@@ -1253,7 +1255,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
                  "cg_block must be 128, 256, 512 or 768");
     EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8 || cfg->cg_batch == 16, "cg_batch must be 4, 8 or 16");
     EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
-    EP_CHECK_ARG(cfg->cg_predict == 0 || cfg->cg_predict == 1, "cg_predict must be 0 or 1");
+    EP_CHECK_ARG(cfg->cg_predict >= 0 && cfg->cg_predict <= 2, "cg_predict must be 0, 1 or 2");
     EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
@@ -1274,14 +1276,20 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
         plan_cg(h);
         return rc;
     }
+    const size_t vb = (size_t)h->pitch * h->rsize;
     if (cfg->cg_predict && !h->pd0.p) {
-        const size_t vb = (size_t)h->pitch * h->rsize;
         for (DBuf *b : {&h->pd0, &h->pd1, &h->pvin}) {
             if ((rc = b->alloc(vb))) return rc;
             EP_CUDA(cudaMemset(b->p, 0, vb));
         }
     }
-    if (cfg->cg_predict && !h->cg_predict) {
+    if (cfg->cg_predict == 2 && !h->pq0.p) {
+        for (DBuf *b : {&h->pq0, &h->pq1}) {
+            if ((rc = b->alloc(vb))) return rc;
+            EP_CUDA(cudaMemset(b->p, 0, vb));
+        }
+    }
+    if (cfg->cg_predict != h->cg_predict) {
         if ((rc = reset_predictor(h))) return rc;
         EP_CUDA(cudaStreamSynchronize(h->stream));
     }
@@ -1295,7 +1303,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
 namespace {
 // device state that stepping changes, saved and put back around tuning trials
 struct Snapshot {
-    DBuf V, S, track, d_step, slot, pd0, pd1;
+    DBuf V, S, track, d_step, slot, pd0, pd1, pq0, pq1;
     long long step = 0;
     int ecg_count = 0;
     std::vector<double> ecg_t;
@@ -1324,6 +1332,8 @@ int snapshot(ep_handle *h, Snapshot &sn, bool save) {
     if ((rc = snap_copy(sn.slot, h->ecg_slot, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.pd0, h->pd0, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.pd1, h->pd1, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.pq0, h->pq0, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.pq1, h->pq1, h->stream, save))) return rc;
     if (save) {
         sn.step = h->step; sn.ecg_count = h->ecg_count; sn.ecg_t = h->ecg_t;
     } else {
@@ -1405,10 +1415,14 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
         if (t >= 0 && t < t_best) { t_best = t; b = c; }
     }
     if (b.cg_variant == 0 && h->scheme != EP_SCHEME_EXPLICIT) {
-        ep_launch_config c = b;
-        c.cg_predict = 1 - b.cg_predict;
-        const double t = trial(c);
-        if (t >= 0 && t < t_best) { t_best = t; b = c; }
+        const ep_launch_config b0 = b;
+        for (int pr : {0, 1, 2}) {
+            if (pr == b0.cg_predict) continue;
+            ep_launch_config c = b0;
+            c.cg_predict = pr;
+            const double t = trial(c);
+            if (t >= 0 && t < t_best) { t_best = t; b = c; }
+        }
     }
     for (int ib : {64, 128}) {
         if (ib == b.ionic_block) continue;

@@ -174,10 +174,13 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
 
     // ---- prologue: r = B x - A x, z = dinv r, p = 0 ----
     // With a predictor (delta: the previous solve's correction x - V of
-    // this half step) the iteration starts from x + delta instead, r = B x -
-    // A (x + delta), while the stop test keeps the reference's r0 = B x - A x;
-    // x itself is not touched before the barrier (neighbours read it here).
+    // this half step; with delta_prev the one before it too, extrapolated
+    // linearly to 2 delta - delta_prev) the iteration starts from x + pred
+    // instead, r = B x - A (x + pred), while the stop test keeps the
+    // reference's r0 = B x - A x; x itself is not touched before the barrier
+    // (neighbours read it here).
     const bool pred = a.delta != nullptr;
+    const bool lin = a.delta_prev != nullptr;
     {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = gwarp; s < s_hi; s += nwarps) {
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                 const R av = __ldg(a.Aval + idx);
                 ax += av * xv;
                 bx += __ldg(a.Bval + idx) * xv;
-                if (pred) ad += av * a.delta[c];
+                if (pred) ad += av * (lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c]);
             }
             if (row >= rb && row < re) {
                 const R rref = bx - ax;
@@ -290,8 +293,10 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         for (int s = gwarp; s < s_hi; s += nwarps) {
             const int row = s * kSlice + lane;
             if (row >= rb && row < re) {
-                const R xf = a.x[row] + a.delta[row];
+                const R d = a.delta[row];
+                const R xf = a.x[row] + (lin ? R(2) * d - a.delta_prev[row] : d);
                 a.x[row] = xf;
+                if (lin) a.delta_prev[row] = d;
                 a.delta[row] = xf - a.vin[row];
             }
         }

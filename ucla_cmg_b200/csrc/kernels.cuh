@@ -112,8 +112,9 @@ template <typename R> struct CGArgs {
     // (two buffers each); p lives in p0
     R *r1, *w0, *w1, *s0, *s1;
     // predictor (two-reduction variant only; nullable): delta = the previous
-    // solve's x - V for this half step, updated in place; vin scratch of n
-    R *delta, *vin;
+    // solve's x - V for this half step, updated in place; delta_prev (nullable)
+    // the one before it, for a linear extrapolation; vin scratch of n
+    R *delta, *delta_prev, *vin;
 };
 
 // batch: SELL columns gathered per group (4 or 8; two register budgets);
