@@ -75,11 +75,37 @@ __device__ __forceinline__ void grid_total(const double *partial, int stride, in
     __syncthreads();
 }
 
+// The columns k .. w-1 (fewer than NB) of a slice as one group: loads of the
+// columns that exist (the test is the same for the whole warp), then their
+// gathers, then the products added in column order.
+template <int NB, typename R, typename F>
+__device__ __forceinline__ R slice_tail(const int *__restrict__ col, const R *__restrict__ val, int beg, int k, int w,
+                                        int lane, F gather, R acc) {
+    int c[NB];
+    R v[NB], g[NB];
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        if (k + u < w) {
+            const int idx = beg + (k + u) * kSlice + lane;
+            c[u] = __ldg(col + idx);
+            v[u] = __ldg(val + idx);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+        if (k + u < w) g[u] = gather(c[u]);
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+        if (k + u < w) acc += v[u] * g[u];
+    return acc;
+}
+
 // Row sums of one SELL slice, NB slice columns at a time: the column and
 // value loads of a group are issued together, then the gathers, so each lane
 // has 3 NB independent loads in flight (at one lane per row the kernel is
-// bound by memory latency, not bandwidth).  The products are still added in
-// column order, so the sums are those of the plain loop whatever NB is.
+// bound by memory latency, not bandwidth); the w mod NB columns left over
+// form one more, partial group.  The products are still added in column
+// order, so the sums are those of the plain loop whatever NB is.
 template <int NB, typename R, typename F>
 __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R *__restrict__ val, int beg, int w,
                                            int lane, F gather) {
@@ -99,11 +125,45 @@ __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R 
 #pragma unroll
         for (int u = 0; u < NB; u++) acc += v[u] * g[u];
     }
-    for (; k < w; k++) {
-        const int idx = beg + k * kSlice + lane;
-        acc += __ldg(val + idx) * gather(__ldg(col + idx));
-    }
+    if (k < w) acc = slice_tail<NB>(col, val, beg, k, w, lane, gather, acc);
     return acc;
+}
+
+// Prologue sums of one slice row: A x and B x, and A d when pred (d = the
+// predictor's start correction, dget(c) its value at column c), NB columns
+// a group like slice_row_sum; each sum is added in column order.
+template <int NB, typename R, typename FD>
+__device__ __forceinline__ void slice_ab_sums(const int *__restrict__ col, const R *__restrict__ Av,
+                                              const R *__restrict__ Bv, const R *x, int beg, int w, int lane,
+                                              bool pred, FD dget, R &ax, R &bx, R &ad) {
+    for (int k = 0; k < w; k += NB) {
+        int c[NB];
+        R av[NB], bv[NB], xv[NB], dv[NB];
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            if (k + u < w) {
+                const int idx = beg + (k + u) * kSlice + lane;
+                c[u] = __ldg(col + idx);
+                av[u] = __ldg(Av + idx);
+                bv[u] = __ldg(Bv + idx);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            if (k + u < w) {
+                xv[u] = x[c[u]];
+                if (pred) dv[u] = dget(c[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            if (k + u < w) {
+                ax += av[u] * xv[u];
+                bx += bv[u] * xv[u];
+                if (pred) ad += av[u] * dv[u];
+            }
+        }
+    }
 }
 
 // The same sum with the next group's column and value loads issued before
@@ -140,10 +200,7 @@ __device__ __forceinline__ R slice_row_sum_pipe(const int *__restrict__ col, con
 #pragma unroll
         for (int u = 0; u < NB; u++) { c[u] = cn[u]; v[u] = vn[u]; }
     }
-    for (int k = full * NB; k < w; k++) {
-        const int idx = beg + k * kSlice + lane;
-        acc += __ldg(val + idx) * gather(__ldg(col + idx));
-    }
+    if (full * NB < w) acc = slice_tail<NB>(col, val, beg, full * NB, w, lane, gather, acc);
     return acc;
 }
 
@@ -187,15 +244,9 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
             const int row = s * kSlice + lane;
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
             R ax = R(0), bx = R(0), ad = R(0);
-            for (int k = 0; k < w; k++) {
-                const int idx = beg + k * kSlice + lane;
-                const int c = __ldg(a.col + idx);
-                const R xv = a.x[c];
-                const R av = __ldg(a.Aval + idx);
-                ax += av * xv;
-                bx += __ldg(a.Bval + idx) * xv;
-                if (pred) ad += av * (lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c]);
-            }
+            slice_ab_sums<NB == 4 ? 2 : 4>(a.col, a.Aval, a.Bval, a.x, beg, w, lane, pred, [&](int c) {
+                return lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c];
+            }, ax, bx, ad);
             if (row >= rb && row < re) {
                 const R rref = bx - ax;
                 const R r = pred ? rref - ad : rref;
@@ -356,13 +407,9 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         for (int s = gwarp; s < s_hi; s += nwarps) {
             const int row = s * kSlice + lane;
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-            R ax = R(0), bx = R(0);
-            for (int k = 0; k < w; k++) {
-                const int idx = beg + k * kSlice + lane;
-                const R xv = a.x[__ldg(a.col + idx)];
-                ax += __ldg(a.Aval + idx) * xv;
-                bx += __ldg(a.Bval + idx) * xv;
-            }
+            R ax = R(0), bx = R(0), ad = R(0);
+            slice_ab_sums<NB == 4 ? 2 : 4>(a.col, a.Aval, a.Bval, a.x, beg, w, lane, false, [](int) { return R(0); },
+                                           ax, bx, ad);
             if (row >= rb && row < re) {
                 const R r = bx - ax;
                 a.r[row] = r;
