@@ -266,6 +266,9 @@ typedef struct ep_launch_config {
                              linear extrapolation of the last two corrections
                              (cg_variant 0 only); the stop test stays relative
                              to B V - A V */
+    int32_t cg_prefetch;  /* 0..4: each warp of the CG launch asks L2 for the
+                             SELL indices and values of the slice it reads that
+                             many slices ahead (cg_variant 0; 0 = off) */
 } ep_launch_config;
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);

@@ -73,7 +73,7 @@ struct ep_handle {
     long long step = 0;
     int nslices = 0;
     // device memory
-    DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, consts, gks, lr_table, type, slice_ptr, col;
+    DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, zv, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
     DBuf pd0, pd1, pvin;                 // CG predictor: x - V of the first / second half step, scratch
     DBuf pq0, pq1;                       // linear CG predictor: the corrections one step older
@@ -102,8 +102,8 @@ struct ep_handle {
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
-    int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, cg_predict = 0, ionic_block = 128, ionic_min = 0,
-        graph_steps = 0;
+    int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, cg_predict = 0, cg_prefetch = 0, ionic_block = 128,
+        ionic_min = 0, graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
     int g_steps = 0;                     // steps in the instantiated graph
     long long g_launches = 0;            // kernel launches per graph replay
@@ -195,7 +195,7 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.n = h->n; a.nslices = h->nslices;
     a.slice_ptr = h->slice_ptr.as<int>(); a.col = h->col.as<int>();
     a.Aval = h->Aval.as<R>(); a.Bval = h->Bval.as<R>(); a.dinv = h->dinv.as<R>();
-    a.x = h->V.as<R>(); a.r = h->r.as<R>(); a.q = h->q.as<R>();
+    a.x = h->V.as<R>(); a.r = h->r.as<R>(); a.q = h->q.as<R>(); a.z = h->zv.as<R>();
     a.p0 = h->p0.as<R>(); a.p1 = h->p1.as<R>();
     a.partial = h->partial.as<double>();
     a.bar = h->bar.as<GridBarrier>();
@@ -212,6 +212,7 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
     a.delta = nullptr; a.delta_prev = nullptr; a.vin = nullptr;   // the time step sets the predictor
+    a.prefetch = h->cg_prefetch;
 }
 
 // start the CG predictor from x0 = V again (after a state upload or when it
@@ -243,9 +244,10 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
     }
     if ((rc = upload<R>(h->dinv, dinv))) return rc;
     const size_t vb = (size_t)h->pitch * sizeof(R);
-    if ((rc = h->r.alloc(vb)) || (rc = h->q.alloc(vb)) || (rc = h->p0.alloc(vb)) || (rc = h->p1.alloc(vb)))
+    if ((rc = h->r.alloc(vb)) || (rc = h->q.alloc(vb)) || (rc = h->p0.alloc(vb)) || (rc = h->p1.alloc(vb)) ||
+        (rc = h->zv.alloc(vb)))
         return rc;
-    EP_CUDA(cudaMemset(h->r.p, 0, vb)); EP_CUDA(cudaMemset(h->q.p, 0, vb));
+    EP_CUDA(cudaMemset(h->r.p, 0, vb)); EP_CUDA(cudaMemset(h->q.p, 0, vb)); EP_CUDA(cudaMemset(h->zv.p, 0, vb));
     EP_CUDA(cudaMemset(h->p0.p, 0, vb)); EP_CUDA(cudaMemset(h->p1.p, 0, vb));
     // cell states (SoA) and voltage
     std::vector<double> V(h->pitch, 0.0), S((size_t)h->ns * h->pitch, 0.0);
@@ -1239,6 +1241,7 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     cfg->cg_batch = h->cg_batch;
     cfg->cg_variant = h->cg_variant;
     cfg->cg_predict = h->cg_predict;
+    cfg->cg_prefetch = h->cg_prefetch;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1257,6 +1260,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
     EP_CHECK_ARG(cfg->cg_predict >= 0 && cfg->cg_predict <= 2, "cg_predict must be 0, 1 or 2");
     EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
+    EP_CHECK_ARG(cfg->cg_prefetch >= 0 && cfg->cg_prefetch <= 4, "cg_prefetch must be 0..4");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
     EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
@@ -1294,6 +1298,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
         EP_CUDA(cudaStreamSynchronize(h->stream));
     }
     h->cg_predict = cfg->cg_predict;
+    h->cg_prefetch = cfg->cg_prefetch;
     h->ionic_block = cfg->ionic_block;
     h->ionic_min = cfg->ionic_min_ctas;
     h->graph_steps = cfg->graph_steps;
@@ -1362,6 +1367,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     cur.cg_batch = h->cg_batch;
     cur.cg_variant = h->cg_variant;
     cur.cg_predict = h->cg_predict;
+    cur.cg_prefetch = h->cg_prefetch;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
     cur.ionic_min_ctas = h->ionic_min;

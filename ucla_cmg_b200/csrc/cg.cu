@@ -31,6 +31,9 @@ __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
 // row and every neighbour that recomputes it round identically
 template <typename R>
 __device__ __forceinline__ R pdir(R dinv, R r, R beta, R p) { return fma(beta, p, dinv * r); }
+// the same with z = dinv r already rounded and stored
+template <typename R>
+__device__ __forceinline__ R pdir_z(R z, R beta, R p) { return fma(beta, p, z); }
 
 template <int NV>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double *out, int stride) {
@@ -73,6 +76,27 @@ __device__ __forceinline__ void grid_total(const double *partial, int stride, in
 #pragma unroll
     for (int k = 0; k < NV; k++) tot[k] = sh[k];
     __syncthreads();
+}
+
+// Ask L2 for the column indices and values (and the B values when Bv is
+// given) of slice sn, which this warp reads next: one lane issues bulk L2
+// prefetches, so the warp's next index loads hit L2 instead of waiting on
+// DRAM.  A hint only: nothing waits on it.  Every slice starts on a 128-byte
+// boundary of the arrays and spans a multiple of 128 bytes.
+__device__ __forceinline__ void l2_prefetch(const void *p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+template <typename R>
+__device__ __forceinline__ void prefetch_slice(const int *__restrict__ slice_ptr, const int *col, const R *Av,
+                                               const R *Bv, int sn, int s_hi, int lane) {
+    if (lane == 0 && sn < s_hi) {
+        const int b = slice_ptr[sn], e = slice_ptr[sn + 1];
+        if (e > b) {
+            l2_prefetch(col + b, (unsigned)(e - b) * 4u);
+            l2_prefetch(Av + b, (unsigned)(e - b) * (unsigned)sizeof(R));
+            if (Bv) l2_prefetch(Bv + b, (unsigned)(e - b) * (unsigned)sizeof(R));
+        }
+    }
 }
 
 // The columns k .. w-1 (fewer than NB) of a slice as one group: loads of the
@@ -241,6 +265,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = gwarp; s < s_hi; s += nwarps) {
+            if (a.prefetch) prefetch_slice(a.slice_ptr, a.col, a.Aval, a.Bval, s + a.prefetch * nwarps, s_hi, lane);
             const int row = s * kSlice + lane;
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
             R ax = R(0), bx = R(0), ad = R(0);
@@ -252,6 +277,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                 const R r = pred ? rref - ad : rref;
                 const R z = __ldg(a.dinv + row) * r;
                 a.r[row] = r;
+                a.z[row] = z;
                 a.p0[row] = R(0);
                 if (pred) a.vin[row] = a.x[row];
                 v[0] += (double)r * (double)z;
@@ -285,15 +311,17 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
             double v[1] = {0.0};
             const R bR = (R)beta;
             for (int s = gwarp; s < s_hi; s += nwarps) {
+                if (a.prefetch)
+                    prefetch_slice<R>(a.slice_ptr, a.col, a.Aval, nullptr, s + a.prefetch * nwarps, s_hi, lane);
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
                 const R *pcc = pc;
-                auto gat = [&](int c) { return pdir(__ldg(a.dinv + c), ldcg(a.r + c), bR, ldcg(pcc + c)); };
+                auto gat = [&](int c) { return pdir_z(ldcg(a.z + c), bR, ldcg(pcc + c)); };
                 R q;
                 if constexpr (NB == 16) q = slice_row_sum_pipe<8>(a.col, a.Aval, beg, w, lane, gat);
                 else q = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, gat);
                 if (row >= rb && row < re) {
-                    const R pi = pdir(__ldg(a.dinv + row), a.r[row], bR, ldcg(pc + row));
+                    const R pi = pdir_z(a.z[row], bR, ldcg(pc + row));
                     pn[row] = pi;
                     a.q[row] = q;
                     v[0] += (double)pi * (double)q;
@@ -309,18 +337,36 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
             pq = t[0];
         }
         const double alpha = rz / pq;
-        // ---- phase B: x += alpha p', r -= alpha q ----
+        // ---- phase B: x += alpha p', r -= alpha q, z = dinv r ----
+        // two of the warp's slices a pass: both slices' loads are issued
+        // before either is updated (the rows are added to the dots in the
+        // same order as one slice at a time)
         {
             double v[2] = {0.0, 0.0};
             const R aR = (R)alpha;
-            for (int s = gwarp; s < s_hi; s += nwarps) {
-                const int row = s * kSlice + lane;
-                if (row >= rb && row < re) {
-                    const R pi = pn[row];
-                    a.x[row] += aR * pi;
-                    const R r = a.r[row] - aR * a.q[row];
+            for (int s = gwarp; s < s_hi; s += 2 * nwarps) {
+                const int row = s * kSlice + lane, row2 = row + nwarps * kSlice;
+                const bool on = row >= rb && row < re;
+                const bool on2 = s + nwarps < s_hi && row2 >= rb && row2 < re;
+                R pi = R(0), xi = R(0), ri = R(0), qi = R(0), di = R(0);
+                R pi2 = R(0), xi2 = R(0), ri2 = R(0), qi2 = R(0), di2 = R(0);
+                if (on) { pi = pn[row]; xi = a.x[row]; ri = a.r[row]; qi = a.q[row]; di = __ldg(a.dinv + row); }
+                if (on2) { pi2 = pn[row2]; xi2 = a.x[row2]; ri2 = a.r[row2]; qi2 = a.q[row2]; di2 = __ldg(a.dinv + row2); }
+                if (on) {
+                    a.x[row] = xi + aR * pi;
+                    const R r = ri - aR * qi;
                     a.r[row] = r;
-                    const R z = __ldg(a.dinv + row) * r;
+                    const R z = di * r;
+                    a.z[row] = z;
+                    v[0] += (double)r * (double)z;
+                    v[1] += (double)r * (double)r;
+                }
+                if (on2) {
+                    a.x[row2] = xi2 + aR * pi2;
+                    const R r = ri2 - aR * qi2;
+                    a.r[row2] = r;
+                    const R z = di2 * r;
+                    a.z[row2] = z;
                     v[0] += (double)r * (double)z;
                     v[1] += (double)r * (double)r;
                 }
@@ -519,16 +565,17 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
 
 template <typename R>
 int cg_max_per_sm(int block, int *per, int batch, int variant) {
-    if (variant == 1) {
-        if (batch >= 8) EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 8>, block, 0));
-        else EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half_cg1<R, 4>, block, 0));
-    } else if (batch == 8) {
-        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 8>, block, 0));
-    } else if (batch == 16) {
-        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 16>, block, 0));
-    } else {
-        EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_cn_half<R, 4>, block, 0));
+    const void *fn = variant == 1 ? (batch >= 8 ? (const void *)k_cn_half_cg1<R, 8> : (const void *)k_cn_half_cg1<R, 4>)
+                     : batch == 8 ? (const void *)k_cn_half<R, 8>
+                     : batch == 16 ? (const void *)k_cn_half<R, 16>
+                                   : (const void *)k_cn_half<R, 4>;
+    cudaFuncAttributes fa;
+    EP_CUDA(cudaFuncGetAttributes(&fa, fn));
+    if (block > fa.maxThreadsPerBlock) {
+        set_error("CG gather width %d takes at most %d threads per CTA (asked %d)", batch, fa.maxThreadsPerBlock, block);
+        return EP_ERR_ARG;
     }
+    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, fn, block, 0));
     if (*per < 1) { set_error("CG kernel cannot be resident with %d threads per CTA", block); return EP_ERR_CUDA; }
     return EP_OK;
 }

@@ -94,6 +94,7 @@ template <typename R> struct CGArgs {
     const int *col;
     const R *Aval, *Bval, *dinv;
     R *x, *r, *q, *p0, *p1;
+    R *z;                        // two-reduction variant: z = dinv r of the own rows, gathered by the neighbours
     double *partial;             // 12 * grid: consecutive phases use disjoint slots
     GridBarrier *bar;
     double tol;
@@ -115,6 +116,9 @@ template <typename R> struct CGArgs {
     // solve's x - V for this half step, updated in place; delta_prev (nullable)
     // the one before it, for a linear extrapolation; vin scratch of n
     R *delta, *delta_prev, *vin;
+    // two-reduction variant: each warp asks L2 for the indices and values of
+    // the slice it reads `prefetch` slices ahead (0: no prefetch)
+    int prefetch;
 };
 
 // batch: SELL columns gathered per group (4 or 8; two register budgets);

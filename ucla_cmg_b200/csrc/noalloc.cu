@@ -30,7 +30,7 @@ namespace ep {
 constexpr int kNoAllocMaxRows = 262144;                 // 2^18 rows
 constexpr int kNoAllocMaxGrid = 2048;                   // >= 148 SMs x 8 blocks
 constexpr size_t kVecBytes = sizeof(double) * (size_t)kNoAllocMaxRows;   // one vector, FP64
-constexpr size_t kScratchBytes = 4 * kVecBytes                            // r, q, p0, p1
+constexpr size_t kScratchBytes = 5 * kVecBytes                            // r, q, p0, p1, z
                                + sizeof(double) * 12 * kNoAllocMaxGrid    // reduction partials (12 slots)
                                + 256;                                     // barrier, stats, result
 
@@ -71,8 +71,9 @@ int run(unsigned char *base, int n, int nslices, const int *slice_ptr, const int
     a.q = (R *)(base + 1 * kVecBytes);
     a.p0 = (R *)(base + 2 * kVecBytes);
     a.p1 = (R *)(base + 3 * kVecBytes);
-    a.partial = (double *)(base + 4 * kVecBytes);
-    unsigned char *tail = base + 4 * kVecBytes + sizeof(double) * 12 * kNoAllocMaxGrid;
+    a.z = (R *)(base + 4 * kVecBytes);
+    a.partial = (double *)(base + 5 * kVecBytes);
+    unsigned char *tail = base + 5 * kVecBytes + sizeof(double) * 12 * kNoAllocMaxGrid;
     a.bar = (GridBarrier *)tail;                                   // 16 B
     unsigned long long *st = (unsigned long long *)(tail + 64);   // 32 B of counters
     a.iters_total = st;

@@ -119,7 +119,8 @@ class Monodomain:
         return c.as_dict()
 
     def set_launch_config(self, cg_block=None, cg_per_sm=None, ionic_block=None, graph_steps=None,
-                          ionic_min_ctas=None, cg_batch=None, cg_variant=None, cg_predict=None):
+                          ionic_min_ctas=None, cg_batch=None, cg_variant=None, cg_predict=None,
+                          cg_prefetch=None):
         cur = self.launch_config()
         c = capi.LaunchConfig()
         c.cg_block = cur["cg_block"] if cg_block is None else int(cg_block)
@@ -130,6 +131,7 @@ class Monodomain:
         c.cg_batch = cur["cg_batch"] if cg_batch is None else int(cg_batch)
         c.cg_variant = cur["cg_variant"] if cg_variant is None else int(cg_variant)
         c.cg_predict = cur["cg_predict"] if cg_predict is None else int(cg_predict)
+        c.cg_prefetch = cur["cg_prefetch"] if cg_prefetch is None else int(cg_prefetch)
         check(capi.lib().ep_set_launch_config(self._h, C.byref(c)))
 
     def autotune(self, trial_steps=20):
