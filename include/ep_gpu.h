@@ -273,10 +273,10 @@ typedef struct ep_launch_config {
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);
 /* Autotuner: times trial_steps steps (after one untimed pass) for the
- * current shape, then by coordinate descent over the CG block size and CTAs
- * per SM, the ionic block size and register budget, and graph replay,
- * keeps the fastest and sets
- * it.  The simulation state (V, states, trackers, step, ECG samples) is put
+ * current shape, then by coordinate descent over the CG gather width, block
+ * size and CTAs per SM, the CG variant, predictor and L2 prefetch, the ionic
+ * block size and register budget, and graph replay, keeps the fastest and
+ * sets it.  The simulation state (V, states, trackers, step, ECG samples) is put
  * back afterwards.  best_ms / start_ms: device ms per step of the chosen and
  * of the starting shape; any output may be NULL. */
 int  ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, double *best_ms,

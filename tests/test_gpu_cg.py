@@ -165,3 +165,24 @@ def test_predictor_needs_two_reduction_variant(gpu):
         g.set_launch_config(cg_variant=1, cg_predict=1)
     assert g.launch_config()["cg_predict"] == 0
     g.close()
+
+
+def test_prefetch_changes_no_bits(gpu, shell):
+    """The L2 prefetch of the next slice is a hint: same bits with it on."""
+    wl, V, c = shell
+    out = []
+    for pf in (0, 2):
+        g = Monodomain(wl.mesh, capi.TUSSCHER, capi.FP32, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
+        g.set_launch_config(cg_batch=8, cg_per_sm=4, cg_prefetch=pf)
+        g.set_voltage(V)
+        it, rr = g.diffusion_half_step()
+        out.append((g.voltage(), it))
+        g.close()
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+    with pytest.raises(capi.EPError):
+        g = Monodomain(wl.mesh, capi.TUSSCHER, capi.FP32, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D)
+        try:
+            g.set_launch_config(cg_variant=1, cg_prefetch=2)
+        finally:
+            g.close()

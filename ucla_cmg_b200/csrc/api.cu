@@ -1261,6 +1261,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(cfg->cg_predict >= 0 && cfg->cg_predict <= 2, "cg_predict must be 0, 1 or 2");
     EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_prefetch >= 0 && cfg->cg_prefetch <= 4, "cg_prefetch must be 0..4");
+    EP_CHECK_ARG(!(cfg->cg_prefetch && cfg->cg_variant), "cg_prefetch needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
     EP_CHECK_ARG(cfg->ionic_min_ctas == 0 || cfg->ionic_min_ctas == 3 || cfg->ionic_min_ctas == 4,
@@ -1417,6 +1418,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
         ep_launch_config c = b;
         c.cg_variant = 1 - b.cg_variant;
         c.cg_predict = 0;
+        c.cg_prefetch = 0;
         const double t = trial(c);
         if (t >= 0 && t < t_best) { t_best = t; b = c; }
     }
@@ -1426,6 +1428,14 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
             if (pr == b0.cg_predict) continue;
             ep_launch_config c = b0;
             c.cg_predict = pr;
+            const double t = trial(c);
+            if (t >= 0 && t < t_best) { t_best = t; b = c; }
+        }
+        const ep_launch_config b1 = b;
+        for (int pf : {0, 2}) {
+            if (pf == b1.cg_prefetch) continue;
+            ep_launch_config c = b1;
+            c.cg_prefetch = pf;
             const double t = trial(c);
             if (t >= 0 && t < t_best) { t_best = t; b = c; }
         }
