@@ -55,10 +55,6 @@ struct ep_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // learned step: the fallback list runs on a second stream beside the
-    // gate/current update of the taken nodes (disjoint nodes), fork and join
-    cudaStream_t aux = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int n = 0, pitch = 0, model = 0, precision = 0, nstate = 0, ns = 0, ntypes = 1;
     size_t rsize = 8;                    // bytes per real
     double dt = 0.1, ionic_dt = 0.1, Cm = 1.0, Xi = 0.0;
@@ -408,20 +404,11 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     fill_surrogate_args(h, ia, sa);
     int rc = launch_surrogate(sa, h->stream);
     if (rc) return rc;
+    if (h->sg_vupdate == 2 && (rc = launch_hybrid(sa, h->stream))) return rc;
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
-    if (h->sg_vupdate != 2) return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block, h->ionic_min);
-    // the listed nodes and the taken nodes are disjoint: the plain model over
-    // the list on the second stream, the hybrid update on the first, joined
-    // before the next half step (graph capture follows the fork and join)
-    EP_CUDA(cudaEventRecord(h->ev_fork, h->stream));
-    EP_CUDA(cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
-    if ((rc = launch_ionic<float>(EP_TUSSCHER, fb, h->aux, h->ionic_block, h->ionic_min))) return rc;
-    if ((rc = launch_hybrid(sa, h->stream))) return rc;
-    EP_CUDA(cudaEventRecord(h->ev_join, h->aux));
-    EP_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
-    return EP_OK;
+    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block, h->ionic_min);
 }
 
 enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
@@ -607,9 +594,6 @@ void ep_destroy(ep_handle *h) {
     for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
-    if (h->aux) { cudaStreamSynchronize(h->aux); cudaStreamDestroy(h->aux); }
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->pin) cudaFreeHost(h->pin);
     delete h;
@@ -768,11 +752,8 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
         for (int i = 0; i < n; i++) h->model_V0[i] = st[(size_t)i * nst];
     int rc = EP_OK;
     EP_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    EP_CUDA(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
     EP_CUDA(cudaEventCreate(&h->ev0));
     EP_CUDA(cudaEventCreate(&h->ev1));
-    EP_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-    EP_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     if (!node_type.empty()) {
         if ((rc = upload_raw(h->type, node_type.data(), node_type.size()))) return rc;
     }
