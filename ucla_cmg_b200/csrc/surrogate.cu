@@ -337,6 +337,15 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
 #pragma unroll
             for (int j = 0; j < SG_NOUT; j++) a.rawY[(size_t)i * SG_NOUT + j] = __uint_as_float(yv[j]) + aux->b4[j];
         } else if (valid) {
+            // the six concentrations the hybrid form replaces, loaded before
+            // any store of this node (the stores below could alias them for
+            // the compiler, which would otherwise serialise load and store)
+            const int cslot[6] = {0, 1, 2, 9, 16, 17};
+            float xs[6];
+            if (aux->v_update == 2) {
+#pragma unroll
+                for (int j = 0; j < 6; j++) xs[j] = a.S[(size_t)cslot[j] * a.pitch + i];
+            }
             // de-normalise; a used output outside the range seen in training
             // sends the node to the plain model as well
             float d[SG_NY];
@@ -356,20 +365,21 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
                 my_fb++;
             } else if (aux->v_update == 2) {
                 // the new concentrations; k_hybrid advances gates and V
-                const int cslot[6] = {0, 1, 2, 9, 16, 17};
 #pragma unroll
                 for (int j = 0; j < 6; j++) {
                     const int q = cslot[j];
-                    const float xk = a.S[(size_t)q * a.pitch + i];
-                    a.pred[(size_t)j * a.pitch + i] = ((lm >> (q + 1)) & 1u) ? xk * __expf(d[q + 1]) : xk + d[q + 1];
+                    a.pred[(size_t)j * a.pitch + i] =
+                        ((lm >> (q + 1)) & 1u) ? xs[j] * __expf(d[q + 1]) : xs[j] + d[q + 1];
                 }
             } else {
-                // every quantity from the network
+                // every quantity from the network (all loads before the stores)
+                float xk[18];
+#pragma unroll
+                for (int k = 0; k < 18; k++) xk[k] = a.S[(size_t)k * a.pitch + i];
 #pragma unroll
                 for (int k = 0; k < 18; k++) {
                     // log-scaled states are updated multiplicatively: x' = x exp(d)
-                    const float xk = a.S[(size_t)k * a.pitch + i];
-                    a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk * __expf(d[k + 1]) : xk + d[k + 1];
+                    a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk[k] * __expf(d[k + 1]) : xk[k] + d[k + 1];
                 }
                 const float V0 = a.V[i], V1 = V0 + d[0];
                 a.V[i] = V1;
