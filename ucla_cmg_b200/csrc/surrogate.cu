@@ -184,6 +184,29 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, const float *
     }
 }
 
+// Ask L2 for the 128-byte lines that build_row will read for tile nt (V,
+// the 18 stored states, G_Ks scale, stimulus heads, node types), one line
+// per thread t of the CTA's second half, so the row build at the end of the
+// current tile finds them in L2.  A hint only; every address is below n.
+__device__ __forceinline__ void prefetch_rows(const SurrogateArgs &a, int nt, int t) {
+    const int base = nt * SG_M;
+    const void *p = nullptr;
+    if (t < 80) {
+        const int arr = t >> 2, off = base + 32 * (t & 3);
+        if (off < a.n) {
+            if (arr == 0) p = a.V + off;
+            else if (arr <= 18) p = a.S + (size_t)(arr - 1) * a.pitch + off;
+            else if (a.gks) p = a.gks + off;
+        }
+    } else if (t < 84) {
+        const int off = base + 32 * (t - 80);
+        if (a.stim_head && off < a.n) p = a.stim_head + off;
+    } else if (t == 84) {
+        if (a.type && base < a.n) p = a.type + base;
+    }
+    if (p) asm volatile("prefetch.L2 [%0];" ::"l"(p));
+}
+
 // One node's input row: features (V, 18 states, I_stim, G_Ks, G_to, s-gate),
 // logarithms of the wide-range ones, normalisation, BF16 row of A (K = 32
 // layout); returns whether the node is inside the training envelope.
@@ -291,6 +314,7 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int i = tile * SG_M + row;
         const bool valid = owner && i < a.n;
+        if (!owner && !raw && tile + (int)gridDim.x < ntiles) prefetch_rows(a, tile + (int)gridDim.x, row);
         // layer 1 (K = 32), 2, 3 (K = 128): hidden, tanh
         const uint32_t sW[3] = {sW1, sW2, sW3};
         const float *bias[3] = {aux->b1, aux->b2, aux->b3};
