@@ -706,6 +706,161 @@ double epo_lr_compute_ion(double *s, const double *table, double Xi_unused,
 }
 
 /* ====================================================================== */
+/* Corrias 2011 rabbit Purkinje -- Purkinje.h/.cc, SetUpIonicConstants.h:16-85 */
+/* ====================================================================== */
+
+/* the 63-entry parameter set of SetUpPurkinjeParameters (SetUpIonicConstants.h:16-85);
+ * [11..15] are the model's own pacing stimulus, unused on this path */
+void epo_pk_constants(double *c)
+{
+    static const double base[57] = {
+        310.0, 96485.3415, 8314.472, 2.0, 140, 5.4, 69.0, 13266.5, 0.6, 0.2,
+        0.06, 700, 9000000, 500, 0.5, -4320.0, 1.0, 0.9, 0.7, 5.4,
+        5.0, 350.0, 10.0, 3.0, 0.005, 2.0, 1140.0, 15.0, 2.0, 20.0,
+        1.5, 3.0, 3, 0.001, 0.001, 0.5, 442.2, 0.01, 0.01, 0.0001,
+        5.0, 0.0001, 1.5, 0.188709677, 0.045290323, 2500.0, 0.001, 120.0, 0.000246, 1.7,
+        1.6, 120.0, 0.000246, 1.7, 1.6, 10.0, 5000.0};
+    for (int k = 0; k < 57; k++) c[k] = base[k];
+    c[57] = c[1] / (c[2] * c[0]);          /* F/RT */
+    c[58] = (c[2] * c[0]) / c[1];          /* RT/F */
+    c[59] = c[9] * c[7];                   /* the three compartment volumes */
+    c[60] = c[8] * c[7];
+    c[61] = (c[8] + c[9]) * c[7];
+    c[62] = c[10] * c[7];
+}
+
+/* Purkinje.h:43-51 */
+void epo_pk_initial_state(double *s)
+{
+    static const double s0[EPO_PK_NSTATE] = {
+        -88.34, 0.00001, 0.000032, 0.17, 6.7, 140, 0.001337, 0.01, 0.000003, 0.1,
+        0.7, 0.0, 0.7, 0.000007, 0.978861, 0.000012, 0.864489, 0.25, 1.0, 0.0,
+        0.011099, 0.011099};
+    for (int k = 0; k < EPO_PK_NSTATE; k++) s[k] = s0[k];
+}
+
+/* Purkinje::ComputeRates (Purkinje.cc:5-103): r[0] = dV/dt, the gates relax
+ * to their steady states, the ion concentrations follow the currents.
+ * istim_pA enters the balances as the reference's Algebraic[0]. */
+static void pk_rates(const double *s, const double *c, double istim_pA, double *r)
+{
+    const double V = s[0];
+    /* gates: steady state and time constant */
+    const double ss6 = 1.0 / (1.0 + exp((V + 47.8) / -5.5));
+    const double ss8 = 1.0 / (1.0 + exp((V + 14.6) / -5.5));
+    const double ss11 = 1.0 / (1.0 + exp((V + -7.0) / -9.0));
+    const double ss12 = 1.0 / (1.0 + exp((V + 27.5) / 8.0));
+    const double ss13 = 1.0 / (1.0 + exp((V + 25.0) / -5.0));
+    const double ss14 = 1.0 / (1.0 + exp((V + 69.0) / 3.96));
+    const double ss15 = 1.0 / (1.0 + exp((V + 30.0) / -5.0));
+    const double ss7 = 1.0 / (1.0 + exp((V + 67.9) / 3.87));
+    const double tau7 = 1.42271 * exp(-0.05119 * V);
+    const double ss9 = 1.0 / (1.0 + exp((V + 31.0) / 5.54));
+    const double tau9 = 25.1 / (0.04 + 0.7 * exp(-1.0 * pow(0.028 * (V + 14.5), 2.0)));
+    const double cai_f = 1.0 + pow(s[1] / 0.0001, 2.0);
+    const double ss10 = 0.4 + 0.6 / cai_f;
+    const double tau10 = 2.0 + 80.0 / cai_f;
+    const double ss16 = 0.1 + 0.9 / (1.0 + exp((V + 75.6) / 6.3));
+    const double tau16 = 120.0 + 1.0 * exp((V + 100.0) / 25.0);
+    const double ss18 = 1.0 / (1.0 + exp((V - 1.5) / -16.7));
+    const double v30 = V + 30.0;
+    const double tau18 = fabs(v30) < 0.0145 ? 417.946
+        : 1.0 / ((7.19e-05 * v30) / (1.0 - exp(-0.148 * v30)) + (0.000131 * v30) / (exp(0.0687 * v30) - 1.0));
+    const double ss_f = 1.0 / (1.0 + exp((V + 109.0) / 10.0));       /* s20 and s21 */
+    const double tau_f = 6000.0 / (exp(-1.0 * (2.9 + 0.04 * V)) + exp(1.0 * (3.6 + 0.11 * V)));
+    const double ss17 = 1.0 / (1.0 + exp((V + 50.0) / -7.5));
+    const double v7 = V + 7.0, v10 = V + 10.0;
+    const double al17 = fabs(v7) > 0.001 ? (0.00138 * 1.0 * v7) / (1.0 - exp(-0.123 * v7)) : 0.00138 / 0.123;
+    const double be17 = fabs(v10) > 0.001 ? (6.1e-05 * 1.0 * v10) / (exp(0.145 * v10) - 1.0) : 0.00061 / 0.145;
+    const double tau17 = 1.0 / (al17 + be17);
+    r[6] = (ss6 - s[6]) / c[16];
+    r[8] = (ss8 - s[8]) / c[18];
+    r[11] = (ss11 - s[11]) / c[20];
+    r[12] = (ss12 - s[12]) / c[21];
+    r[13] = (ss13 - s[13]) / c[24];
+    r[14] = (ss14 - s[14]) / c[25];
+    r[15] = (ss15 - s[15]) / c[27];
+    r[7] = (ss7 - s[7]) / tau7;
+    r[9] = (ss9 - s[9]) / tau9;
+    r[10] = (ss10 - s[10]) / tau10;
+    r[16] = (ss16 - s[16]) / tau16;
+    r[18] = (ss18 - s[18]) / tau18;
+    r[20] = (ss_f - s[20]) / tau_f;
+    r[21] = (ss_f - s[21]) / tau_f;
+    r[17] = (ss17 - s[17]) / tau17;
+    r[19] = (ss18 - s[19]) / (4.0 * tau18);
+    /* reversal potentials */
+    const double RTF = c[58];
+    const double EK = RTF * log(c[5] / s[5]);
+    const double ENa = RTF * log(c[4] / s[4]);
+    const double ECa = 0.5 * RTF * log(c[3] / s[1]);
+    /* potassium currents */
+    const double iK1 = c[29] * pow(c[5] / 5.4, 0.8) * (1.0 / (1.0 + exp((92.0 + V) / 10.0))) * (V - EK);
+    const double ito = c[22] * s[11] * s[12] * (V - EK);
+    const double iKp = c[23] * (1.0 / (1.0 + exp((5.0 - V) / 17.0))) * (V - EK);
+    const double iKr = c[30] * pow(c[5] / 5.4, 1.0) * (1.0 / (1.0 + exp((33.0 + V) / 22.4))) * s[17] * (V - EK);
+    const double iKs = c[31] * s[18] * s[19] * (V - EK);
+    const double iKb = c[37] * (V - EK);
+    const double iNaK = c[36] * (1.0 / (1.0 + exp((V + 80.0) / -45.0))) * (1.0 / (1.0 + exp((V + 0.0) / 125.0))) *
+                        (1.0 / (1.0 + pow(1.9 / c[5], 1.45))) * (1.0 / (1.0 + pow(31.98 / s[4], 1.0)));
+    const double ifK = c[43] * s[20] * (V - EK);
+    /* calcium and sodium currents */
+    const double iCaL = c[19] * s[8] * s[9] * s[10] * (V - ECa);
+    const double iCaT = c[17] * s[6] * s[7] * (V - ECa);
+    const double iNa = c[26] * s[13] * s[14] * (V - ENa);
+    const double iNaL = c[28] * s[15] * s[16] * (V - ENa);
+    const double ipCa = c[40] * (1.0 / (1.0 + pow(c[41] / s[1], c[42])));
+    const double iCab = c[39] * (V - ECa);
+    const double ifNa = c[44] * s[21] * (V - ENa);
+    const double iNaCa = (512.009 * c[33] *
+                          (exp((c[35] * (c[32] - 2.0) * V) / RTF) * pow(s[4], c[32]) * c[3] -
+                           s[1] * exp(((c[35] - 1.0) * (c[32] - 2.0) * V) / RTF) * pow(c[4], c[32]))) /
+                         ((1.0 + c[34] * (s[1] * pow(c[4], c[32]) + c[3] * pow(s[4], c[32]))) * (1.0 + s[1] / 0.0069));
+    const double iNab = c[38] * (V - ENa);
+    r[5] = ((-ito - iKp - iKr - iKs - iK1 - iKb - ifK - istim_pA + 2.0 * iNaK) * 1000.0) / (c[1] * c[61]);
+    r[0] = ((-1.0 * 1.0) / c[6]) * (iK1 + ito + iKp + iKr + iKs + iKb + iNaK + iCaL + iCaT + iNa + iNaL + ipCa +
+                                     iCab + ifNa + ifK + iNaCa + iNab + istim_pA);
+    /* calcium handling: release, two uptakes, transfer */
+    const double jrel = c[45] * (s[3] / (1.0 + pow(c[46] / s[1], 2.0)));
+    const double jup1 = c[47] * ((pow(s[1] / c[48], c[50]) - pow(s[3] / c[49], c[50])) /
+                                 (1.0 + pow(s[1] / c[48], c[50]) + pow(s[3] / c[49], c[50])));
+    const double jup2 = c[51] * ((pow(s[2] / c[52], c[54]) - pow(s[3] / c[53], c[54])) /
+                                 (1.0 + pow(s[2] / c[52], c[54]) + pow(s[3] / c[53], c[54])));
+    const double jtr = c[55] * (s[3] - s[2]);
+    const double jdiff = c[56] * (s[1] - s[2]);
+    r[3] = ((-jrel - jtr + jup2 + jup1) * 1000.0) / (2.0 * c[1] * c[62]);
+    r[4] = ((-iNa - iNaL - 3.0 * iNaK - 3.0 * iNaCa - ifNa - iNab) * 1000.0) / (c[1] * c[61]);
+    r[1] = ((-iCaL - iCaT - iCab + 1.0 * jrel - jup1 - jdiff + 2.0 * iNaCa - ipCa) * 1000.0) / (2.0 * c[1] * c[59]);
+    r[2] = ((-jup2 + jdiff + jtr) * 1000.0) / (2.0 * c[1] * c[60]);
+}
+
+/* Purkinje::Compute_Ion + UpdateStateVariables (Purkinje.cc:183-213,
+ * 157-173): V into State[0], the stimulus [uA/cm^3] as pA through the cell's
+ * surface area (4.612e-5 cm^2) and Xi, then one forward-Euler step of dt --
+ * or ten of dt/10 when |dV/dt| > 1.5 mV/ms at the start.  Every state,
+ * V included, is advanced; the returned dV/dt is the last evaluated rate.
+ * C_m is not used by the model. */
+double epo_pk_compute_ion(double *s, const double *c, double Xi, double dt, double V, double istim,
+                          int *substepped)
+{
+    double r[EPO_PK_NSTATE];
+    s[0] = V;
+    const double istim_pA = -1e6 * istim * 4.612e-5 / Xi;
+    pk_rates(s, c, istim_pA, r);
+    if (fabs(r[0]) > 1.5) {
+        for (int k = 0; k < 10; k++) {
+            pk_rates(s, c, istim_pA, r);
+            for (int j = 0; j < EPO_PK_NSTATE; j++) s[j] += r[j] * dt / 10;
+        }
+        if (substepped) *substepped = 1;
+    } else {
+        for (int j = 0; j < EPO_PK_NSTATE; j++) s[j] += r[j] * dt;
+        if (substepped) *substepped = 0;
+    }
+    return r[0];
+}
+
+/* ====================================================================== */
 /* population                                                              */
 /* ====================================================================== */
 
@@ -719,6 +874,7 @@ epo_cells *epo_cells_create(int model, int n, const uint8_t *type, int ntypes,
     case EPO_TUSSCHER: c->nstate = EPO_TT_NSTATE; c->nconst = EPO_TT_NCONST; c->Xi = 2000.; break;
     case EPO_MAHAJAN: case EPO_MAHAJAN_FAIL:
         c->nstate = EPO_MH_NSTATE; c->nconst = EPO_MH_NCONST; c->Xi = 1.55E-4 / 2.58E-8; break;
+    case EPO_PURKINJE: c->nstate = EPO_PK_NSTATE; c->nconst = EPO_PK_NCONST; c->Xi = 2500.; break;
     default: c->nstate = EPO_LR_NSTATE; c->nconst = 1;
         c->Xi = 2. * (11e-4 + 100E-4) / (11e-4 * 100E-4); break;
     }
@@ -731,6 +887,7 @@ epo_cells *epo_cells_create(int model, int n, const uint8_t *type, int ntypes,
             if (model == EPO_TUSSCHER) epo_tt_constants(k);
             else if (model == EPO_MAHAJAN) epo_mh_constants(k, t, 0);
             else if (model == EPO_MAHAJAN_FAIL) epo_mh_constants(k, t, 1);
+            else if (model == EPO_PURKINJE) epo_pk_constants(k);
         }
     }
     if (model == EPO_TUSSCHER) c->alg12 = (double *)calloc((size_t)n, sizeof(double));
@@ -740,6 +897,7 @@ epo_cells *epo_cells_create(int model, int n, const uint8_t *type, int ntypes,
         int t = type ? type[i] : 0;
         if (model == EPO_TUSSCHER) epo_tt_initial_state(s);
         else if (model == EPO_MAHAJAN || model == EPO_MAHAJAN_FAIL) epo_mh_initial_state(s, t);
+        else if (model == EPO_PURKINJE) epo_pk_initial_state(s);
         else epo_lr_initial_state(s);
     }
     return c;
@@ -786,6 +944,10 @@ void epo_cells_compute_ion(epo_cells *c, double Cm, double dt, const double *V,
         } else if (c->model == EPO_MAHAJAN || c->model == EPO_MAHAJAN_FAIL) {
             int sub = 0;
             dvdt[i] = epo_mh_compute_ion(s, k, Xi, Cm, dt, V[i], istim[i], c->mh_abs_mode, &sub);
+            nsub += sub;
+        } else if (c->model == EPO_PURKINJE) {
+            int sub = 0;
+            dvdt[i] = epo_pk_compute_ion(s, k, Xi, dt, V[i], istim[i], &sub);
             nsub += sub;
         } else {
             dvdt[i] = epo_lr_compute_ion(s, c->lr_table, Xi, Cm, dt, V[i], istim[i]);

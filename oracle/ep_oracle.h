@@ -26,13 +26,18 @@ extern "C" {
 
 /* model ids follow the reference enum CellModelType (Body/CardiacBody.h:57) */
 enum { EPO_LUORUDY = 0, EPO_LUORUDYWITHGATE = 1, EPO_TUSSCHER = 2,
-       EPO_MAHAJAN = 3, EPO_MAHAJAN_FAIL = 4 };
+       EPO_MAHAJAN = 3, EPO_MAHAJAN_FAIL = 4,
+       /* not in CellModelType: CardiacBody::New gives every .purk node a
+        * Purkinje cell (CardiacBody.cc:982-1101) */
+       EPO_PURKINJE = 5 };
 
 #define EPO_TT_NSTATE 19
 #define EPO_TT_NCONST 54   /* 53 reference constants + [53] s-gate variant (0 epi, 1 endo) */
 #define EPO_MH_NSTATE 26
 #define EPO_MH_NCONST 35
 #define EPO_LR_NSTATE 8
+#define EPO_PK_NSTATE 22
+#define EPO_PK_NCONST 63
 
 /* ---------------- cell models (single cell, in place) ---------------- */
 void   epo_tt_constants(double *c);                  /* SetUpTusscherParameters */
@@ -60,6 +65,13 @@ void   epo_lr_params(double v, double *tab);         /* LR.cc:102-183 (14 entrie
 double *epo_lr_gate_table(void);
 double epo_lr_compute_ion(double *s, const double *table, double Xi_unused,
                           double Cm, double dt, double V, double istim);
+
+void   epo_pk_constants(double *c);                  /* SetUpPurkinjeParameters */
+void   epo_pk_initial_state(double *s);              /* Purkinje.h:43-51 */
+/* One Compute_Ion call of the Purkinje cell (Xi: the model's 2500 or the
+ * user's); *substepped = 1 when the ten dt/10 forward-Euler steps ran. */
+double epo_pk_compute_ion(double *s, const double *c, double Xi, double dt,
+                          double V, double istim, int *substepped);
 
 /* ---------------- a population of cells ---------------- */
 typedef struct epo_cells {

@@ -21,7 +21,8 @@ _LIB = None
 _REF = None
 
 TUSSCHER, MAHAJAN, MAHAJAN_FAIL, LUORUDY, LUORUDYWITHGATE = 2, 3, 4, 0, 1
-NSTATE = {TUSSCHER: 19, MAHAJAN: 26, MAHAJAN_FAIL: 26, LUORUDY: 8, LUORUDYWITHGATE: 8}
+PURKINJE = 5          # the cell model of .purk nodes (not in CellModelType)
+NSTATE = {TUSSCHER: 19, MAHAJAN: 26, MAHAJAN_FAIL: 26, LUORUDY: 8, LUORUDYWITHGATE: 8, PURKINJE: 22}
 
 dp = C.POINTER(C.c_double)
 ip = C.POINTER(C.c_int)
@@ -101,6 +102,8 @@ def lib():
         L.epo_tt_initial_state.argtypes = [dp]
         L.epo_mh_initial_state.argtypes = [dp, C.c_int]
         L.epo_lr_initial_state.argtypes = [dp]
+        L.epo_pk_constants.argtypes = [dp]
+        L.epo_pk_initial_state.argtypes = [dp]
         _LIB = L
     return _LIB
 
@@ -155,10 +158,18 @@ def mh_constants(pos, failing=False):
     return c
 
 
+def pk_constants():
+    c = np.zeros(63)
+    lib().epo_pk_constants(_p(c))
+    return c
+
+
 def initial_state(model, pos=0):
     L = lib()
     if model == TUSSCHER:
         s = np.zeros(19); L.epo_tt_initial_state(_p(s))
+    elif model == PURKINJE:
+        s = np.zeros(22); L.epo_pk_initial_state(_p(s))
     elif model in (MAHAJAN, MAHAJAN_FAIL):
         s = np.zeros(26); L.epo_mh_initial_state(_p(s), int(pos))
     else:

@@ -1,5 +1,5 @@
 // ref_shim.cc -- C entry points around the reference's UNMODIFIED cell-model
-// classes (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR}.cc),
+// classes (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR,Purkinje}.cc),
 // compiled from their sources in place.  TEST INFRASTRUCTURE ONLY: it backs
 // the oracle checks and the reference arm of the CPU baseline.
 //
@@ -11,6 +11,7 @@
 #include "Mahajan.h"
 #include "Mahajan_fail.h"
 #include "LR.h"
+#include "Purkinje.h"
 #include "SetUpIonicConstants.h"
 #include "../ep_oracle.h"
 #include <cstring>
@@ -78,7 +79,8 @@ struct RefCells {
 
 extern "C" {
 
-// model: 0 LUORUDY, 1 LUORUDYWITHGATE, 2 TUSSCHER, 3 MAHAJAN, 4 MAHAJAN_FAIL
+// model: 0 LUORUDY, 1 LUORUDYWITHGATE, 2 TUSSCHER, 3 MAHAJAN, 4 MAHAJAN_FAIL,
+// 5 the Purkinje cell CardiacBody::New puts on .purk nodes
 void *ref_cells_create(int model, int n, const unsigned char *type)
 {
     RefCells *r = new RefCells();
@@ -107,6 +109,11 @@ void *ref_cells_create(int model, int n, const unsigned char *type)
             else r->cells.push_back(new Mahajan_fail(r->consts[t], t));
         }
         break; }
+    case 5: {
+        r->nstate = 22;
+        Real *c; SetUpPurkinjeParameters(&c); r->consts.push_back(c);
+        for (int i = 0; i < n; i++) r->cells.push_back(new Purkinje(c));
+        break; }
     default:
         delete r; return nullptr;
     }
@@ -123,6 +130,7 @@ void ref_cells_destroy(void *h)
         case 0: case 1: delete (LuoRudy *)c; break;
         case 2: delete (Tusscher *)c; break;
         case 3: delete (Mahajan *)c; break;
+        case 5: delete (Purkinje *)c; break;
         default: delete (Mahajan_fail *)c; break;
         }
     }

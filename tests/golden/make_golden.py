@@ -2,11 +2,12 @@
 
 The reference repository ships no test vectors for its ionic models, so the
 goldens are produced here by running the reference's own sources
-(voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR}.cc, compiled
+(voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR,Purkinje}.cc, compiled
 unmodified into oracle/_ref/libvoomep_ref.so by oracle/Makefile) through
 their IonicModel::Compute_Ion interface.
 
-    python tests/golden/make_golden.py        # needs oracle/_ref built
+    python tests/golden/make_golden.py [name ...]   # needs oracle/_ref built
+                                                    # (names: tt mahajan ... purkinje; default all)
 
 Outputs (npz):
   cell_<model>.npz  single-cell trajectory under the split update
@@ -27,14 +28,14 @@ from oracle import oracle as O  # noqa: E402
 
 XI = {O.TUSSCHER: 2000.0, O.MAHAJAN: 1.55e-4 / 2.58e-8, O.MAHAJAN_FAIL: 1.55e-4 / 2.58e-8,
       O.LUORUDY: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4),
-      O.LUORUDYWITHGATE: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4)}
+      O.LUORUDYWITHGATE: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4), O.PURKINJE: 2500.0}
 NAME = {O.TUSSCHER: "tt", O.MAHAJAN: "mahajan", O.MAHAJAN_FAIL: "mahajan_fail",
-        O.LUORUDY: "lr", O.LUORUDYWITHGATE: "lrgate"}
+        O.LUORUDY: "lr", O.LUORUDYWITHGATE: "lrgate", O.PURKINJE: "purkinje"}
 # (dt, T, types, stimulus start): TT needs dt <= 0.01 with the reference
 # Newton layout; LR starts with j = 1e-4 and needs ~100 ms to become excitable
 CASES = {O.TUSSCHER: (0.01, 400.0, None, 0.0), O.MAHAJAN: (0.02, 400.0, [0, 4, 8], 0.0),
          O.MAHAJAN_FAIL: (0.02, 400.0, [2, 6], 0.0), O.LUORUDY: (0.02, 500.0, None, 100.0),
-         O.LUORUDYWITHGATE: (0.02, 500.0, None, 100.0)}
+         O.LUORUDYWITHGATE: (0.02, 500.0, None, 100.0), O.PURKINJE: (0.02, 500.0, None, 10.0)}
 
 
 def trajectory(model, dt, T, types, sample_every, t_stim):
@@ -60,8 +61,14 @@ def main():
     if O.ref_lib() is None:
         raise SystemExit("oracle/_ref/libvoomep_ref.so missing: run make -C oracle")
     rng = np.random.default_rng(1234)
+    only = set(sys.argv[1:])
     for model, (dt, T, types, t_stim) in CASES.items():
         cells, t, Vs, Vend, snaps, tarr = trajectory(model, dt, T, types, int(round(1.0 / dt)), t_stim)
+        if only and NAME[model] not in only:
+            rng.choice(len(snaps), size=128, replace=False)      # keep the other models' draws
+            n_in = 128 * (len(types) if types is not None else 1)
+            rng.normal(0, 2.0, n_in); rng.random(n_in)
+            continue
         np.savez_compressed(os.path.join(HERE, f"cell_{NAME[model]}.npz"), t=t, V=Vs, V_end=Vend,
                             states_end=cells.state, dt=dt, t_stim=t_stim, types=tarr if tarr is not None else np.zeros(0, np.uint8))
         # KAT batch: 256 snapshots x cells, perturbed V and stimulus

@@ -20,10 +20,10 @@ from ucla_cmg_b200 import mesh as M
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = {"tt": O.TUSSCHER, "mahajan": O.MAHAJAN, "mahajan_fail": O.MAHAJAN_FAIL,
-         "lr": O.LUORUDY, "lrgate": O.LUORUDYWITHGATE}
+         "lr": O.LUORUDY, "lrgate": O.LUORUDYWITHGATE, "purkinje": O.PURKINJE}
 XI = {O.TUSSCHER: 2000.0, O.MAHAJAN: 1.55e-4 / 2.58e-8, O.MAHAJAN_FAIL: 1.55e-4 / 2.58e-8,
       O.LUORUDY: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4),
-      O.LUORUDYWITHGATE: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4)}
+      O.LUORUDYWITHGATE: 2 * (11e-4 + 100e-4) / (11e-4 * 100e-4), O.PURKINJE: 2500.0}
 
 
 @pytest.mark.parametrize("name", list(NAMES))
@@ -89,6 +89,29 @@ def test_live_reference_matches():
         assert np.max(np.abs(a - b)) <= 1e-9 * max(1.0, np.max(np.abs(a)))
         V = V + 0.01 * a
     assert np.allclose(ref.state, port.state, rtol=1e-10, atol=1e-14)
+
+
+def test_live_reference_matches_purkinje():
+    """Where oracle/_ref is built: the Purkinje restatement equals the
+    reference's Purkinje objects bit for bit through an action potential,
+    both branches of its adaptive forward Euler (|dV/dt| > 1.5 takes ten
+    dt/10 steps) included."""
+    if O.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    n = 3
+    ref = O.RefCells(O.PURKINJE, n)
+    port = O.Cells(O.PURKINJE, n)
+    V = np.array([-88.34, -70.0, -30.0])
+    fast = 0
+    for k in range(2000):
+        ist = np.where(np.arange(n) == 0, 50.0 * 2500.0 if 100 <= k < 150 else 0.0, 0.0)
+        a = ref.compute_ion(V, ist, 0.02)
+        b = port.compute_ion(V, ist, 0.02)
+        assert np.array_equal(a, b)
+        fast += int(np.sum(np.abs(a) > 1.5))
+        V = V + 0.02 * a
+    assert fast > 0
+    assert np.array_equal(ref.state, port.state)
 
 
 def test_tt_reference_jacobian_diverges_at_dt_002():
