@@ -1025,13 +1025,13 @@ static void elem_tensor(const double *fib, const double D[3], double De[3][3])
 
 typedef struct { int r, c; double k, m; } trip_t;
 
-int epo_assemble(int n, const double *xyz, int m, const int *tets,
-                 const double *fibers, const double D[3], double Cm,
-                 double dt_diff, double smoothing_alpha, epo_csr *out)
+#define EPO_PI 3.14159265358979323846      /* M_PI */
+
+/* the 16 entries of every tet, in element order (TetMesh::Compute +
+ * CardiacBody::Compute), and their lumped capacitance */
+static int tet_triplets(const double *xyz, int m, const int *tets, const double *fibers, const double D[3],
+                        double Cm, trip_t *t, double *CL)
 {
-    memset(out, 0, sizeof *out);
-    trip_t *t = (trip_t *)malloc(sizeof(trip_t) * (size_t)m * 16);
-    double *CL = (double *)calloc((size_t)n, sizeof(double));
     int bad = 0;
     for (int e = 0; e < m; e++) {
         const int *v = tets + 4 * (size_t)e;
@@ -1056,10 +1056,85 @@ int epo_assemble(int n, const double *xyz, int m, const int *tets,
                 p->r = v[a]; p->c = v[b]; p->k = Ke[a][b]; p->m = Me[a][b];
             }
     }
+    return bad;
+}
+
+/* 2-node cable elements of a mixed mesh (MixedMesh3D.cc:62-108 for the
+ * geometry and quadrature, CardiacBody.cc:100-187 for D, K, M and
+ * CardiacBody.cc:32-67 for the capacitance): the 4 entries of every bar in
+ * element order after the tets' entries. */
+static int bar_triplets(const double *xyz, const epo_cables *cb, double Cm, trip_t *t, double *CL)
+{
+    /* LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc) */
+    double qx[3], qw[3];
+    int nq;
+    const int qord = 2 * (cb->quad_order > 0 ? cb->quad_order : 2) - 1;
+    if (qord == 1) { nq = 1; qx[0] = 0.0; qw[0] = 2.0; }
+    else if (qord == 3) { nq = 2; qx[0] = -0.577350269189626; qx[1] = 0.577350269189626; qw[0] = qw[1] = 1.0; }
+    else if (qord == 5) {
+        nq = 3; qx[0] = -0.774596669241483; qx[1] = 0.0; qx[2] = 0.774596669241483;
+        qw[0] = qw[2] = 5.0 / 9.0; qw[1] = 8.0 / 9.0;
+    } else return -2;
+    int bad = 0;
+    int pmj = 0;                    /* once set, stays set: see the note in ep_oracle.h */
+    double pmj_data[4] = {0., 0., 0., 0.};
+    for (int e = 0; e < cb->nb; e++) {
+        const int *v = cb->bars + 2 * (size_t)e;
+        if (cb->orient_has && cb->orient_has[v[0]]) {
+            pmj = 1;
+            for (int k = 0; k < 4; k++) pmj_data[k] = cb->orient[4 * (size_t)v[0] + k];
+        }
+        double ang[3], mag;
+        for (int k = 0; k < 3; k++) ang[k] = xyz[3 * v[1] + k] - xyz[3 * v[0] + k];
+        mag = sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
+        for (int k = 0; k < 3; k++) ang[k] /= mag;
+        if (pmj && cb->orient_sticky) {
+            for (int k = 0; k < 3; k++) ang[k] = pmj_data[k];
+            mag = pmj_data[3];
+        } else if (cb->orient_has && cb->orient_has[v[0]]) {
+            for (int k = 0; k < 3; k++) ang[k] = pmj_data[k];
+            mag = pmj_data[3];
+        }
+        if (!(mag > 0.0)) bad = 1;
+        /* conductivity: LV cables (a node of tissue type 11) take DpLeft */
+        const int lv = cb->lv ? cb->lv[e] : 0;
+        double Dc[3];
+        for (int k = 0; k < 3; k++) Dc[k] = lv ? cb->DpLeft[k] : cb->Dp[k];
+        double De[3][3];
+        elem_tensor(cb->fibers ? cb->fibers + 9 * (size_t)e : NULL, Dc, De);
+        const double fac = 2. / mag;
+        const double dN[2] = {-0.5, 0.5};
+        double dx[2][3];
+        for (int a = 0; a < 2; a++)
+            for (int k = 0; k < 3; k++) dx[a][k] = dN[a] * ang[k] * fac;
+        double Ke[2][2] = {{0}}, Me[2][2] = {{0}};
+        for (int q = 0; q < nq; q++) {
+            const double N[2] = {0.5 * (1. - qx[q]), 0.5 * (1. + qx[q])};
+            const double w = qw[q] * EPO_PI * (cb->radius * cb->radius) * mag;
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    Me[a][b] += N[a] * N[b] * w;
+                    for (int mm = 0; mm < 3; mm++)
+                        for (int nn = 0; nn < 3; nn++)
+                            Ke[a][b] += De[mm][nn] * dx[a][mm] * dx[b][nn] * w * Cm;
+                }
+            for (int a = 0; a < 2; a++) CL[v[a]] += N[a] * Cm * w;
+        }
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) {
+                trip_t *p = t + 4 * (size_t)e + 2 * a + b;
+                p->r = v[a]; p->c = v[b]; p->k = Ke[a][b]; p->m = Me[a][b];
+            }
+    }
+    return bad;
+}
+
+static void csr_from_triplets(int n, trip_t *t, size_t nt, double *CL, double Cm, double dt_diff,
+                              double smoothing_alpha, epo_csr *out)
+{
     /* group the element entries by (row, col) keeping element order inside
      * each run, so duplicates are summed in insertion order */
     {
-        const size_t nt = (size_t)m * 16;
         trip_t *tmp = (trip_t *)malloc(sizeof(trip_t) * nt);
         /* counting sort by row, then insertion by column inside a row keeps order */
         int *cnt = (int *)calloc((size_t)n + 1, sizeof(int));
@@ -1122,6 +1197,31 @@ int epo_assemble(int n, const double *xyz, int m, const int *tets,
         out->A = A; out->B = B; out->K = K; out->M = M; out->CL = CL;
         free(tmp); free(cnt); free(pos);
     }
+}
+
+int epo_assemble(int n, const double *xyz, int m, const int *tets,
+                 const double *fibers, const double D[3], double Cm,
+                 double dt_diff, double smoothing_alpha, epo_csr *out)
+{
+    return epo_assemble_mixed(n, xyz, m, tets, fibers, D, NULL, Cm, dt_diff, smoothing_alpha, out);
+}
+
+int epo_assemble_mixed(int n, const double *xyz, int m, const int *tets,
+                       const double *fibers, const double D[3], const epo_cables *cables,
+                       double Cm, double dt_diff, double smoothing_alpha, epo_csr *out)
+{
+    memset(out, 0, sizeof *out);
+    const size_t nb = cables ? (size_t)cables->nb : 0;
+    const size_t nt = (size_t)m * 16 + nb * 4;
+    trip_t *t = (trip_t *)malloc(sizeof(trip_t) * (nt ? nt : 1));
+    double *CL = (double *)calloc((size_t)n, sizeof(double));
+    int bad = tet_triplets(xyz, m, tets, fibers, D, Cm, t, CL);
+    if (nb) {
+        const int rb = bar_triplets(xyz, cables, Cm, t + (size_t)m * 16, CL);
+        if (rb == -2) { free(t); free(CL); return -2; }
+        bad |= rb;
+    }
+    csr_from_triplets(n, t, nt, CL, Cm, dt_diff, smoothing_alpha, out);
     free(t);
     return bad ? -1 : 0;
 }

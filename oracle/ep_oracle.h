@@ -117,6 +117,31 @@ typedef struct epo_csr {
 int  epo_assemble(int n, const double *xyz, int m, const int *tets,
                   const double *fibers, const double D[3], double Cm,
                   double dt_diff, double smoothing_alpha, epo_csr *out);
+/* 2-node Purkinje cables of a mixed (MIX3D) mesh, MixedMesh3D.cc:62-108 and
+ * CardiacBody.cc:100-187.  The quadrature weight is w_q * pi r^2 * length
+ * with Gauss weights summing to 2 on [-1, 1], as in the reference: a cable's
+ * mass and stiffness are twice those of a cylinder of that radius.  A node
+ * listed in the .angle file overrides the direction and length of a cable
+ * starting there; in the reference the override, once met, stays on for
+ * every later cable (a flag that is never reset, MixedMesh3D.cc:14-34):
+ * orient_sticky = 1 keeps that, 0 applies it to its own cable only. */
+typedef struct epo_cables {
+    int nb;
+    const int *bars;             /* nb * 2 zero-based node ids */
+    const double *fibers;        /* nb * 9 (f, s, n) or NULL: isotropic Dp[0] */
+    const uint8_t *lv;           /* nb or NULL: 1 = a node of tissue type 11 (DpLeft) */
+    double Dp[3], DpLeft[3];     /* setPurkinjeDiffusion / ...InLV */
+    double radius;               /* Mesh::setRadius (TWODRADIUS, 0.0275 cm) */
+    int quad_order;              /* the mesh's order; 2 -> two Gauss points */
+    const uint8_t *orient_has;   /* n or NULL */
+    const double *orient;        /* n * 4: direction, length */
+    int orient_sticky;
+} epo_cables;
+
+/* tets then cables, summed in that element order; tets alone == epo_assemble */
+int  epo_assemble_mixed(int n, const double *xyz, int m, const int *tets,
+                        const double *fibers, const double D[3], const epo_cables *cables,
+                        double Cm, double dt_diff, double smoothing_alpha, epo_csr *out);
 void epo_csr_free(epo_csr *a);
 /* y = A x for one of the value arrays */
 void epo_spmv(const epo_csr *a, const double *vals, const double *x, double *y);

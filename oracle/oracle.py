@@ -37,6 +37,13 @@ class _Csr(C.Structure):
                 ("A", dp), ("B", dp), ("M", dp), ("K", dp), ("CL", dp)]
 
 
+class _Cables(C.Structure):
+    _fields_ = [("nb", C.c_int), ("bars", ip), ("fibers", dp), ("lv", C.POINTER(C.c_uint8)),
+                ("Dp", C.c_double * 3), ("DpLeft", C.c_double * 3), ("radius", C.c_double),
+                ("quad_order", C.c_int), ("orient_has", C.POINTER(C.c_uint8)), ("orient", dp),
+                ("orient_sticky", C.c_int)]
+
+
 class _Cells(C.Structure):
     _fields_ = [("model", C.c_int), ("n", C.c_int), ("nstate", C.c_int), ("nconst", C.c_int),
                 ("state", dp), ("consts", dp), ("ntypes", C.c_int),
@@ -80,6 +87,8 @@ def lib():
         L.epo_cells_initial_voltage.argtypes = [C.c_void_p, dp]
         L.epo_assemble.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_double, C.c_double,
                                    C.c_double, C.POINTER(_Csr)]
+        L.epo_assemble_mixed.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.POINTER(_Cables),
+                                         C.c_double, C.c_double, C.c_double, C.POINTER(_Csr)]
         L.epo_csr_free.argtypes = [C.POINTER(_Csr)]
         L.epo_spmv.argtypes = [C.POINTER(_Csr), dp, dp, dp]
         L.epo_pcg.argtypes = [C.POINTER(_Csr), dp, dp, dp, C.c_double, C.c_int, C.c_int, dp]
@@ -127,6 +136,8 @@ def ref_lib():
         L.ref_cells_set_user_xi.argtypes = [C.c_void_p, C.c_double]
         L.epo_assemble.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_double, C.c_double,
                                    C.c_double, C.POINTER(_Csr)]
+        L.epo_assemble_mixed.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.POINTER(_Cables),
+                                         C.c_double, C.c_double, C.c_double, C.POINTER(_Csr)]
         L.epo_csr_free.argtypes = [C.POINTER(_Csr)]
         L.epo_sim_init.argtypes = [C.POINTER(_Sim), C.POINTER(_Csr), C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
@@ -283,20 +294,59 @@ class RefCells:
             pass
 
 
+class Cables:
+    """2-node Purkinje cables of a mixed mesh for ``Csr`` (see epo_cables):
+    bars (nb x 2, zero-based), optional per-bar fibres and LV flags, the
+    Purkinje diffusion, the cable radius and the .angle overrides."""
+
+    def __init__(self, bars, Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, fibers=None, lv=None,
+                 quad_order=2, orient=None, sticky=True, n=None):
+        self.bars = np.ascontiguousarray(bars, dtype=np.int32).reshape(-1, 2)
+        self.fibers = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
+        self.lv = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
+        self.c = _Cables()
+        self.c.nb = len(self.bars)
+        self.c.bars = _p(self.bars, ip)
+        self.c.fibers = _p(self.fibers)
+        self.c.lv = _p(self.lv, C.POINTER(C.c_uint8)) if self.lv is not None else None
+        for k in range(3):
+            self.c.Dp[k] = Dp[k]
+            self.c.DpLeft[k] = (DpLeft if DpLeft is not None else Dp)[k]
+        self.c.radius = radius
+        self.c.quad_order = quad_order
+        self.c.orient_sticky = int(bool(sticky))
+        self.has = self.orient = None
+        if orient:                       # {node (zero-based): (dx, dy, dz, length)}
+            self.has = np.zeros(n, np.uint8)
+            self.orient = np.zeros((n, 4))
+            for k, v in orient.items():
+                self.has[k] = 1
+                self.orient[k] = v
+            self.c.orient_has = _p(self.has, C.POINTER(C.c_uint8))
+            self.c.orient = _p(self.orient)
+
+
 class Csr:
-    """Assembled CN system (oracle)."""
+    """Assembled CN system (oracle); ``cables`` adds the 2-node Purkinje
+    elements of a mixed mesh after the tets."""
 
     def __init__(self, xyz, tets, fibers=None, D=(1e-3, 1e-3, 1e-3), Cm=1.0, dt=0.02,
-                 smoothing_alpha=0.0, L=None):
+                 smoothing_alpha=0.0, L=None, cables=None):
         self._L = L or lib()
         self.xyz = np.ascontiguousarray(xyz, dtype=np.float64)
-        self.tets = np.ascontiguousarray(tets, dtype=np.int32)
+        self.tets = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
         self.fibers = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
         self.D = np.ascontiguousarray(D, dtype=np.float64)
         self.c = _Csr()
-        rc = self._L.epo_assemble(len(self.xyz), _p(self.xyz), len(self.tets), _p(self.tets, ip),
-                                  _p(self.fibers), _p(self.D), Cm, dt, smoothing_alpha,
-                                  C.byref(self.c))
+        self.cables = cables
+        if cables is None:
+            rc = self._L.epo_assemble(len(self.xyz), _p(self.xyz), len(self.tets), _p(self.tets, ip),
+                                      _p(self.fibers), _p(self.D), Cm, dt, smoothing_alpha,
+                                      C.byref(self.c))
+        else:
+            rc = self._L.epo_assemble_mixed(len(self.xyz), _p(self.xyz), len(self.tets), _p(self.tets, ip),
+                                            _p(self.fibers), _p(self.D), C.byref(cables.c), Cm, dt,
+                                            smoothing_alpha, C.byref(self.c))
         self.degenerate = rc != 0
         self.n, self.nnz = self.c.n, self.c.nnz
 

@@ -245,3 +245,77 @@ def test_substep_schedule():
     assert abs(sum(sub) - 0.1) < 1e-15 and len(sub) in (5, 6)
     s2 = O.Sim(c, cells, 0.02, 0.05)
     assert s2.sub_dt == [0.02]
+
+
+def _cable(k=5, h=0.1, axis=0):
+    xyz = np.zeros((k + 1, 3))
+    xyz[:, axis] = np.arange(k + 1) * h
+    bars = np.stack([np.arange(k), np.arange(1, k + 1)], 1)
+    return xyz, bars
+
+
+def test_cable_elements_match_the_closed_form():
+    """A straight Purkinje cable of 2-node elements (MixedMesh3D beam branch,
+    two Gauss points): K = 2 Dp pi r^2 C_m / h * tridiag(-1, 2, -1), M row sums
+    = C_L / C_m, K 1 = 0, symmetric, and the total mass is 2 pi r^2 L -- twice
+    the cylinder's volume, because the reference scales Gauss weights that sum
+    to 2 by the element length (parity hazard, kept)."""
+    k, h, r, Dp, Cm = 6, 0.05, 0.0275, 0.0016, 1.3
+    xyz, bars = _cable(k, h, axis=1)
+    c = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=O.Cables(bars, Dp=(Dp,) * 3, radius=r), Cm=Cm, dt=0.1)
+    K = c.scipy("K").toarray()
+    M = c.scipy("M").toarray()
+    ref = 2 * Dp * np.pi * r * r * Cm / h * (2 * np.eye(k + 1) - np.eye(k + 1, k=1) - np.eye(k + 1, k=-1))
+    ref[0, 0] = ref[-1, -1] = 2 * Dp * np.pi * r * r * Cm / h
+    assert np.allclose(K, ref, rtol=1e-12, atol=1e-18)
+    assert np.allclose(K, K.T, rtol=0, atol=1e-18)
+    assert np.max(np.abs(K.sum(1))) < 1e-15
+    assert np.isclose(M.sum(), 2 * np.pi * r * r * k * h, rtol=1e-12)
+    assert np.allclose(M.sum(1) * Cm, c.arr("CL"), rtol=1e-12)
+    # A = Cm M + dt/4 K, B = Cm M - dt/4 K on the same pattern
+    assert np.allclose(c.scipy("A").toarray(), Cm * M + 0.1 / 4 * K, rtol=1e-12, atol=1e-18)
+
+
+def test_mixed_mesh_is_tets_plus_cables(small_slab):
+    """Tets and cables sharing nodes: the mixed operators are the sum of the
+    tet-only and the cable-only operators; the LV flag selects DpLeft."""
+    m = small_slab
+    n0 = m.n
+    # a cable from three surface nodes of the slab out to two extra nodes
+    extra = m.xyz[[0]] + np.array([[0.0, 0.0, -0.05], [0.0, 0.0, -0.1]])
+    xyz = np.vstack([m.xyz, extra])
+    bars = np.array([[1, 0], [0, n0], [n0, n0 + 1]])
+    D = (1.2e-3, 2e-4, 2e-4)
+    lv = np.array([0, 1, 1], np.uint8)
+    cb = O.Cables(bars, Dp=(0.0016,) * 3, DpLeft=(0.003,) * 3, lv=lv, radius=0.02)
+    mix = O.Csr(xyz, m.tets, m.fibers, D, 1.0, 0.1, cables=cb)
+    tet = O.Csr(xyz, m.tets, m.fibers, D, 1.0, 0.1)
+    only = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=cb, D=D, Cm=1.0, dt=0.1)
+    for name in ("K", "M", "A", "B"):
+        diff = mix.scipy(name) - tet.scipy(name) - only.scipy(name)
+        assert abs(diff).max() <= 1e-15 * max(1.0, abs(mix.scipy(name)).max())
+    assert np.allclose(mix.arr("CL"), tet.arr("CL") + only.arr("CL"), rtol=1e-13)
+    # the LV bars conduct with DpLeft: stiffness scales with D along the bar
+    lvK = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=O.Cables(bars, Dp=(0.0016,) * 3, DpLeft=(0.0016,) * 3,
+                                                             lv=lv, radius=0.02), D=D, Cm=1.0, dt=0.1)
+    k1 = only.scipy("K").toarray()[n0, n0 + 1]
+    k2 = lvK.scipy("K").toarray()[n0, n0 + 1]
+    assert np.isclose(k1 / k2, 0.003 / 0.0016, rtol=1e-12)
+
+
+def test_cable_orientation_override_sticks_like_the_reference():
+    """A node listed in the .angle file replaces the direction and length of
+    the cable that starts there; in the reference the flag is never reset, so
+    every later cable takes the last override (sticky) -- the non-sticky
+    option applies it to its own cable only."""
+    xyz, bars = _cable(4, 0.1)
+    orient = {1: (1.0, 0.0, 0.0, 0.2)}          # bar 1 starts at node 1: length 0.2
+    Ks = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=O.Cables(bars, orient=orient, sticky=True, n=len(xyz)),
+               Cm=1.0, dt=0.1).scipy("K").toarray()
+    Kn = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=O.Cables(bars, orient=orient, sticky=False, n=len(xyz)),
+               Cm=1.0, dt=0.1).scipy("K").toarray()
+    Kp = O.Csr(xyz, np.zeros((0, 4), np.int32), cables=O.Cables(bars), Cm=1.0, dt=0.1).scipy("K").toarray()
+    assert np.isclose(Kp[0, 1], Ks[0, 1]) and np.isclose(Kp[0, 1], Kn[0, 1])     # bar 0: before the override
+    assert np.isclose(Ks[1, 2], Kp[1, 2] / 2) and np.isclose(Kn[1, 2], Kp[1, 2] / 2)   # bar 1: length 0.2
+    assert np.isclose(Ks[3, 4], Kp[3, 4] / 2)                                    # bar 3: sticky
+    assert np.isclose(Kn[3, 4], Kp[3, 4])                                        # bar 3: its own geometry
