@@ -244,6 +244,41 @@ int  ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres);
  * slices by largest remainder.  inst_blk[n_inst + 1]. */
 int  ep_batch_plan(int32_t n_inst, const int32_t *inst_row, int32_t grid, int32_t *inst_blk);
 
+/* 2-node Purkinje cables of a mixed (MIX3D) mesh: the beam elements of
+ * MixedMesh3D::Compute (Mesh/MixedMesh3D.cc:62-108) with the Purkinje
+ * diffusion of CardiacBody::Compute (Body/CardiacBody.cc:100-187).  The
+ * reference scales Gauss weights that sum to 2 by the cable length, so a
+ * cable carries twice the mass and stiffness of a cylinder of that radius;
+ * kept.  A node listed in the .angle file (Mesh.cc:403-416) overrides the
+ * direction and length of the cable that starts there, and in the reference
+ * the override, once met, stays on for every later cable (angle_sticky = 1;
+ * 0 applies it to its own cable only). */
+typedef struct ep_cables_desc {
+    int32_t n_bars;
+    const int32_t *bars;        /* 2 * n_bars node ids, in .ele order */
+    int32_t one_based;          /* 1: ids as in the .ele / .angle files */
+    const double *fibers;       /* 9 * n_bars (f, s, n) or NULL: isotropic Dp[0] */
+    const uint8_t *lv;          /* n_bars or NULL: 1 = a node of tissue type 11 (DpLeft) */
+    double Dp[3], DpLeft[3];    /* PURKINJEDIFFUSION / LVPURKINJEDIFFUSION, cm^2/ms */
+    double radius;              /* TWODRADIUS, cm (the driver's default 0.0275) */
+    int32_t quad_order;         /* the mesh's quadrature order (0: 2 = two Gauss points) */
+    int32_t n_angle;            /* .angle entries */
+    const int32_t *angle_nodes; /* n_angle node ids */
+    const double *angle;        /* 4 * n_angle: direction (3), length */
+    int32_t angle_sticky;
+} ep_cables_desc;
+
+/* The FP64 operators ep_create assembles for the solver's scheme, on the
+ * host only (no GPU, no device memory): CSR of n_nodes rows, zero-based
+ * sorted columns, A and B (CN: C_m M +- dt/4 K; BE: C_L + dt/2 K and C_L;
+ * explicit: -K) and the lumped capacitance C_L, with the tets of `mesh`
+ * followed by the optional cables (EP_CrankNicholson::Initialize,
+ * Solvers/EP_CrankNicholson.cc:5-76, over CardiacBody::Compute).  Call with
+ * rowptr == NULL for *nnz, then with rowptr[n+1], col/A/B[nnz], CL[n]. */
+int  ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_desc *cables,
+                           const ep_solver_desc *solver, int64_t *nnz, int32_t *rowptr,
+                           int32_t *col, double *A, double *B, double *CL);
+
 /* Launch shape of ep_step (no reference counterpart).  cg_block: threads
  * per CTA of the persistent CG launch (128, 256, 512 or 768); cg_per_sm: its CTAs per
  * SM (0 = as many as are co-resident); ionic_block: threads per CTA of the

@@ -281,6 +281,76 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
 // CTA groups of the persistent CG launch: every instance gets at least one
 // CTA, the rest in proportion to its SELL slices (largest remainder).
 // Returns -1 if there are more instances than CTAs.
+// host only: the operators ep_create would build (tests and inspection)
+extern "C" int ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_desc *cables,
+                                     const ep_solver_desc *sd, int64_t *nnz, int32_t *rowptr, int32_t *col,
+                                     double *A, double *B, double *CL) {
+    EP_CHECK_ARG(mesh && sd && nnz, "null argument");
+    EP_CHECK_ARG(mesh->n_nodes > 0 && mesh->xyz && (mesh->n_tets == 0 || mesh->tets), "bad mesh");
+    EP_CHECK_ARG(sd->scheme >= EP_SCHEME_CN && sd->scheme <= EP_SCHEME_EXPLICIT, "unknown scheme");
+    EP_CHECK_ARG(sd->dt > 0.0, "dt must be positive");
+    const int n = mesh->n_nodes;
+    std::vector<int> tl((size_t)mesh->n_tets * 4);
+    for (size_t e = 0; e < tl.size(); e++) {
+        const int v = mesh->tets[e] - (mesh->one_based ? 1 : 0);
+        EP_CHECK_ARG(v >= 0 && v < n, "tet node id out of range");
+        tl[e] = v;
+    }
+    HostCables hc;
+    std::vector<int> bl;
+    std::vector<uint8_t> ohas;
+    std::vector<double> orient;
+    if (cables && cables->n_bars > 0) {
+        EP_CHECK_ARG(cables->bars, "null cable list");
+        EP_CHECK_ARG(cables->radius > 0.0, "cable radius must be positive");
+        const int off = cables->one_based ? 1 : 0;
+        bl.resize((size_t)cables->n_bars * 2);
+        for (size_t k = 0; k < bl.size(); k++) {
+            bl[k] = cables->bars[k] - off;
+            EP_CHECK_ARG(bl[k] >= 0 && bl[k] < n, "cable node id out of range");
+        }
+        hc.nb = cables->n_bars;
+        hc.bars = bl.data();
+        hc.fibers = cables->fibers;
+        hc.lv = cables->lv;
+        for (int k = 0; k < 3; k++) { hc.Dp[k] = cables->Dp[k]; hc.DpLeft[k] = cables->DpLeft[k]; }
+        hc.radius = cables->radius;
+        hc.quad_order = cables->quad_order > 0 ? cables->quad_order : 2;
+        EP_CHECK_ARG(hc.quad_order >= 1 && hc.quad_order <= 3, "cable quadrature order must be 1, 2 or 3");
+        hc.orient_sticky = cables->angle_sticky ? 1 : 0;
+        if (cables->n_angle > 0) {
+            EP_CHECK_ARG(cables->angle_nodes && cables->angle, "null .angle data");
+            ohas.assign(n, 0);
+            orient.assign((size_t)n * 4, 0.0);
+            for (int k = 0; k < cables->n_angle; k++) {
+                const int v = cables->angle_nodes[k] - off;
+                EP_CHECK_ARG(v >= 0 && v < n, ".angle node id out of range");
+                ohas[v] = 1;
+                for (int c = 0; c < 4; c++) orient[4 * (size_t)v + c] = cables->angle[4 * (size_t)k + c];
+            }
+            hc.orient_has = ohas.data();
+            hc.orient = orient.data();
+        }
+    }
+    const double Cm = mesh->Cm > 0.0 ? mesh->Cm : 1.0;
+    HostCSR csr;
+    const int rc = assemble_cn(n, mesh->xyz, mesh->n_tets, tl.data(), mesh->fibers, mesh->D, Cm, sd->dt,
+                               sd->smoothing_alpha, csr, sd->scheme, hc.nb ? &hc : nullptr);
+    if (rc) {
+        set_error(rc == -2 ? "unsupported cable quadrature order" : "an element has non-positive volume or length");
+        return EP_ERR_MESH;
+    }
+    *nnz = (int64_t)csr.col.size();
+    if (!rowptr) return EP_OK;
+    EP_CHECK_ARG(col && A && B && CL, "null output array");
+    std::memcpy(rowptr, csr.rowptr.data(), sizeof(int32_t) * ((size_t)n + 1));
+    std::memcpy(col, csr.col.data(), sizeof(int32_t) * csr.col.size());
+    std::memcpy(A, csr.A.data(), sizeof(double) * csr.A.size());
+    std::memcpy(B, csr.B.data(), sizeof(double) * csr.B.size());
+    std::memcpy(CL, csr.CL.data(), sizeof(double) * (size_t)n);
+    return EP_OK;
+}
+
 extern "C" int ep_batch_plan(int32_t ninst, const int32_t *inst_row, int32_t grid, int32_t *inst_blk) {
     if (ninst <= 0 || !inst_row || !inst_blk || grid < ninst) return EP_ERR_ARG;
     std::vector<long long> sl(ninst);

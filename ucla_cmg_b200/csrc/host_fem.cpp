@@ -105,12 +105,105 @@ void incidence(int n, int m, const int *tets, std::vector<int> &ptr, std::vector
         for (int a = 0; a < 4; a++) elem[pos[tets[4 * (size_t)e + a]]++] = e;
 }
 
+// element matrices of the cables, in element order (the .angle override
+// can carry over from one cable to the next)
+struct BarMat {
+    int nq = 0;
+    double K[2][2] = {{0, 0}, {0, 0}}, M[2][2] = {{0, 0}, {0, 0}};
+    double CL[3][2] = {{0, 0}, {0, 0}, {0, 0}};   // per quadrature point, for the element-order sums
+};
+
+int bar_mats(const double *xyz, const HostCables &cb, double Cm, std::vector<BarMat> &out) {
+    // LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc), weights summing to 2
+    double qx[3], qw[3];
+    int nq;
+    const int qord = 2 * (cb.quad_order > 0 ? cb.quad_order : 2) - 1;
+    if (qord == 1) { nq = 1; qx[0] = 0.0; qw[0] = 2.0; }
+    else if (qord == 3) { nq = 2; qx[0] = -0.577350269189626; qx[1] = 0.577350269189626; qw[0] = qw[1] = 1.0; }
+    else if (qord == 5) {
+        nq = 3; qx[0] = -0.774596669241483; qx[1] = 0.0; qx[2] = 0.774596669241483;
+        qw[0] = qw[2] = 5.0 / 9.0; qw[1] = 8.0 / 9.0;
+    } else {
+        return -2;
+    }
+    out.assign(cb.nb, BarMat());
+    int bad = 0;
+    bool carried = false;
+    double carry[4] = {0, 0, 0, 0};
+    for (int e = 0; e < cb.nb; e++) {
+        const int *v = cb.bars + 2 * (size_t)e;
+        const bool listed = cb.orient_has && cb.orient_has[v[0]];
+        if (listed) {
+            carried = true;
+            for (int k = 0; k < 4; k++) carry[k] = cb.orient[4 * (size_t)v[0] + k];
+        }
+        double ang[3], len;
+        for (int k = 0; k < 3; k++) ang[k] = xyz[3 * (size_t)v[1] + k] - xyz[3 * (size_t)v[0] + k];
+        len = std::sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
+        for (int k = 0; k < 3; k++) ang[k] /= len;
+        if (listed || (carried && cb.orient_sticky)) {
+            for (int k = 0; k < 3; k++) ang[k] = carry[k];
+            len = carry[3];
+        }
+        if (!(len > 0.0)) bad = 1;
+        const bool lv = cb.lv && cb.lv[e];
+        const double *Dc = lv ? cb.DpLeft : cb.Dp;
+        double De[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (!cb.fibers) {
+            for (int p = 0; p < 3; p++) De[p][p] = Dc[0];
+        } else {
+            const double *fib = cb.fibers + 9 * (size_t)e;
+            for (int p = 0; p < 3; p++)
+                for (int m = 0; m < 3; m++)
+                    for (int q = 0; q < 3; q++) De[m][q] += Dc[p] * fib[3 * p + m] * fib[3 * p + q];
+        }
+        const double fac = 2. / len;
+        const double dshape[2] = {-0.5, 0.5};
+        double dx[2][3];
+        for (int a = 0; a < 2; a++)
+            for (int k = 0; k < 3; k++) dx[a][k] = dshape[a] * ang[k] * fac;
+        BarMat &bm = out[e];
+        bm.nq = nq;
+        for (int q = 0; q < nq; q++) {
+            const double N[2] = {0.5 * (1. - qx[q]), 0.5 * (1. + qx[q])};
+            const double w = qw[q] * M_PI * (cb.radius * cb.radius) * len;
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    bm.M[a][b] += N[a] * N[b] * w;
+                    for (int m = 0; m < 3; m++)
+                        for (int r = 0; r < 3; r++) bm.K[a][b] += De[m][r] * dx[a][m] * dx[b][r] * w * Cm;
+                }
+            for (int a = 0; a < 2; a++) bm.CL[q][a] = N[a] * Cm * w;
+        }
+    }
+    return bad;
+}
+
+void bar_incidence(int n, const HostCables *cb, std::vector<int> &ptr, std::vector<int> &elem) {
+    ptr.assign((size_t)n + 1, 0);
+    const int nb = cb ? cb->nb : 0;
+    for (size_t k = 0; k < (size_t)nb * 2; k++) ptr[cb->bars[k] + 1]++;
+    for (int i = 0; i < n; i++) ptr[i + 1] += ptr[i];
+    elem.resize((size_t)nb * 2);
+    std::vector<int> pos(ptr.begin(), ptr.end() - 1);
+    for (int e = 0; e < nb; e++)
+        for (int a = 0; a < 2; a++) elem[pos[cb->bars[2 * (size_t)e + a]]++] = e;
+}
+
 }  // namespace
 
 int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *fibers,
-                const double D[3], double Cm, double dt, double smoothing_alpha, HostCSR &out, int scheme) {
-    std::vector<int> eptr, elem;
+                const double D[3], double Cm, double dt, double smoothing_alpha, HostCSR &out, int scheme,
+                const HostCables *cables) {
+    std::vector<int> eptr, elem, bptr, belem;
     incidence(n, m, tets, eptr, elem);
+    bar_incidence(n, cables, bptr, belem);
+    std::vector<BarMat> bars;
+    int bad_bar = 0;
+    if (cables && cables->nb > 0) {
+        bad_bar = bar_mats(xyz, *cables, Cm, bars);
+        if (bad_bar == -2) return -2;
+    }
     out.n = n;
     out.rowptr.assign((size_t)n + 1, 0);
     // pattern: union of the vertices of each node's elements
@@ -120,6 +213,8 @@ int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *
         std::vector<int> &r = rows[i];
         for (int k = eptr[i]; k < eptr[i + 1]; k++)
             for (int a = 0; a < 4; a++) r.push_back(tets[4 * (size_t)elem[k] + a]);
+        for (int k = bptr[i]; k < bptr[i + 1]; k++)
+            for (int a = 0; a < 2; a++) r.push_back(cables->bars[2 * (size_t)belem[k] + a]);
         std::sort(r.begin(), r.end());
         r.erase(std::unique(r.begin(), r.end()), r.end());
     }
@@ -180,6 +275,29 @@ int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *
                     }
                 }
             }
+            // the cables at this node, after its tets
+            for (int k = bptr[i]; k < bptr[i + 1]; k++) {
+                const int e = belem[k];
+                const int *v = cables->bars + 2 * (size_t)e;
+                const BarMat &bm = bars[e];
+                const int a = v[0] == i ? 0 : 1;
+                if (pass == 1) {
+                    if (mass)
+                        for (int b = 0; b < 2; b++) {
+                            const int p = find(v[b]);
+                            A[p] += bm.M[a][b] * Cm;
+                            B[p] += bm.M[a][b] * Cm;
+                        }
+                    for (int q = 0; q < bm.nq; q++) cl += bm.CL[q][a];
+                } else {
+                    const double f = pass == 0 ? s : sm;
+                    for (int b = 0; b < 2; b++) {
+                        const int p = find(v[b]);
+                        A[p] += bm.K[a][b] * f;
+                        if (mass) B[p] += bm.K[a][b] * (-f);
+                    }
+                }
+            }
         }
         out.CL[i] = cl;
         if (scheme == 1) {                       // lumped capacitance on the diagonal
@@ -189,7 +307,7 @@ int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *
         }
         std::vector<int>().swap(rows[i]);
     }
-    return bad ? -1 : 0;
+    return (bad || bad_bar) ? -1 : 0;
 }
 
 void ecg_weights(int n, const double *xyz, int m, const int *tets, const double *fibers,

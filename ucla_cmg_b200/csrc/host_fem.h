@@ -13,13 +13,34 @@ struct HostCSR {
     std::vector<double> CL;         // lumped capacitance (row sums of Cm M)
 };
 
-// Returns 0, or -1 if an element has a non-positive Jacobian.
+// 2-node Purkinje cables of a mixed mesh (MixedMesh3D.cc:62-108,
+// CardiacBody.cc:100-187): zero-based bars, optional per-bar fibres (else
+// isotropic Dp[0]) and LV flags (DpLeft), cable radius, the mesh's
+// quadrature order (2: two Gauss points), and the .angle overrides of
+// direction and length for cables starting at a listed node (sticky: the
+// reference's never-reset flag keeps the last override for every later cable).
+struct HostCables {
+    int nb = 0;
+    const int *bars = nullptr;
+    const double *fibers = nullptr;
+    const uint8_t *lv = nullptr;
+    double Dp[3] = {0.0016, 0.0016, 0.0016}, DpLeft[3] = {0.0016, 0.0016, 0.0016};
+    double radius = 0.0275;
+    int quad_order = 2;
+    const uint8_t *orient_has = nullptr;    // n
+    const double *orient = nullptr;         // n * 4
+    int orient_sticky = 1;
+};
+
+// Returns 0, -1 if an element has a non-positive Jacobian (or a cable a
+// non-positive length), -2 for an unsupported cable quadrature order.
 // tets are zero-based.  s = dt/4 (+ smoothing 4 alpha / dt).
 // scheme 0: Crank-Nicolson (A = Cm M + s K, B = Cm M - s K); 1: backward
 // Euler (A = C_L + dt/2 K, B = diag C_L); 2: explicit (A = -K, B zero).
+// Cables (optional) are summed after the tets of the same entry.
 int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *fibers,
                 const double D[3], double Cm, double dt, double smoothing_alpha, HostCSR &out,
-                int scheme = 0);
+                int scheme = 0, const HostCables *cables = nullptr);
 
 // W[k * n + i] with ECG_k = sum_i W V_i (ComputeECG.h:30-189 with grad V
 // constant on a P1 tet).

@@ -336,6 +336,54 @@ def batch_plan(inst_row, grid):
     return out
 
 
+def assemble_operators(mesh, D, dt, Cm=1.0, scheme=capi.SCHEME_CN, smoothing_alpha=0.0, bars=None,
+                       Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, bar_fibers=None, lv=None, quad_order=2,
+                       angle=None, angle_sticky=True):
+    """The FP64 operators ep_create builds, assembled on the host only
+    (ep_assemble_operators; no GPU): scipy CSR matrices A and B and the
+    lumped capacitance C_L.  ``bars`` (nb x 2, zero-based) adds 2-node
+    Purkinje cables after the tets; ``angle`` maps a zero-based node to
+    (dx, dy, dz, length) as in a .angle file."""
+    import scipy.sparse as sp
+    md, _, keep = _instance_descs(mesh, capi.TUSSCHER, D, Cm, None, None, None, None, 0.0, 0, 0, 0, None)
+    sd = _solver_desc(dt, dt, 1e-7, 1000, smoothing_alpha, capi.FP64, 0.0, 0, -40.0, scheme)
+    cd = None
+    if bars is not None:
+        keep["bars"] = np.ascontiguousarray(bars, dtype=np.int32).reshape(-1, 2)
+        keep["bfib"] = None if bar_fibers is None else np.ascontiguousarray(bar_fibers, dtype=np.float64)
+        keep["lv"] = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
+        cd = capi.CablesDesc()
+        cd.n_bars = len(keep["bars"])
+        cd.bars = ptr(keep["bars"], C.POINTER(C.c_int32))
+        cd.one_based = 0
+        cd.fibers = ptr(keep["bfib"])
+        cd.lv = ptr(keep["lv"], C.POINTER(C.c_uint8))
+        for k in range(3):
+            cd.Dp[k] = float(Dp[k])
+            cd.DpLeft[k] = float((DpLeft if DpLeft is not None else Dp)[k])
+        cd.radius = float(radius)
+        cd.quad_order = int(quad_order)
+        cd.angle_sticky = int(bool(angle_sticky))
+        if angle:
+            keep["an"] = np.array(sorted(angle), dtype=np.int32)
+            keep["ad"] = np.array([angle[k] for k in sorted(angle)], dtype=np.float64).reshape(-1, 4)
+            cd.n_angle = len(keep["an"])
+            cd.angle_nodes = ptr(keep["an"], C.POINTER(C.c_int32))
+            cd.angle = ptr(keep["ad"])
+    nnz = C.c_int64(0)
+    L = capi.lib()
+    cdp = C.byref(cd) if cd is not None else None
+    check(L.ep_assemble_operators(C.byref(md), cdp, C.byref(sd), C.byref(nnz), None, None, None, None, None))
+    n = mesh.n
+    rowptr = np.zeros(n + 1, np.int32)
+    col = np.zeros(nnz.value, np.int32)
+    A, B, CL = np.zeros(nnz.value), np.zeros(nnz.value), np.zeros(n)
+    ip = C.POINTER(C.c_int32)
+    check(L.ep_assemble_operators(C.byref(md), cdp, C.byref(sd), C.byref(nnz), ptr(rowptr, ip), ptr(col, ip),
+                                  ptr(A), ptr(B), ptr(CL)))
+    return (sp.csr_matrix((A, col, rowptr), shape=(n, n)), sp.csr_matrix((B, col, rowptr), shape=(n, n)), CL)
+
+
 def ionic_step(model, V, istim, states, dt, Cm=1.0, precision=capi.FP64, node_type=None,
                type_consts=None, gks_scale=None, user_xi=0.0, newton_cap=0,
                tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0):
