@@ -121,6 +121,18 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -228,7 +240,8 @@ def run_reference(args, rank, world):
                                    "ten Tusscher, dt 0.1 / ionic 0.02 ms, 200 PMJ stimuli",
                        "form": "reference CPU (FP64)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{len(timed)} steps of a {n}-node shell (h={h} cm) from t=0"},
+                             "sample": f"{len(timed)} steps of a {n}-node shell (h={h} cm) from t=0",
+                             "cpu": cpu_model()},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -352,7 +365,8 @@ def run_ours(args, rank, world, local):
         v = ncpu * 5 / sum(times[1:])
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"5 steps (after 1 untimed) of a {ncpu}-node shell "
-                                          f"(h={h} cm) from t=0, same model, dt and stimuli"}
+                                          f"(h={h} cm) from t=0, same model, dt and stimuli",
+                                "cpu": cpu_model()}
         # the same path on one host thread (the reference runs one MPI rank
         # per core; this is one rank's speed), on a coarser sample
         n1, t1, _ = cpu_sample("reference", 0.2, 3, 1)
