@@ -1,0 +1,109 @@
+"""The library's cell-model source (csrc/tt.cuh, mahajan.cuh, purkinje.cuh:
+host+device code) compiled for the host by a small test harness
+(tests/native/cells_host.cu) and checked against the golden vectors made by
+the reference's own cell models -- the formulas the sm_100a kernels run,
+verified without a GPU.  The Purkinje cell's GPU kernel is not wired yet;
+its device source is pinned here first."""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from ucla_cmg_b200 import capi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+GOLD = os.path.join(HERE, "golden")
+SRC = os.path.join(HERE, "native", "cells_host.cu")
+OUT = os.path.join(HERE, "native", "_build", "libcells_host.so")
+DEPS = [SRC] + [os.path.join(ROOT, "ucla_cmg_b200", "csrc", f)
+                for f in ("tt.cuh", "mahajan.cuh", "purkinje.cuh", "common.cuh")]
+PURKINJE = 5
+XI = {capi.TUSSCHER: 2000.0, capi.MAHAJAN: 1.55e-4 / 2.58e-8, capi.MAHAJAN_FAIL: 1.55e-4 / 2.58e-8,
+      PURKINJE: 2500.0}
+NAMES = {"tt": capi.TUSSCHER, "mahajan": capi.MAHAJAN, "mahajan_fail": capi.MAHAJAN_FAIL,
+         "purkinje": PURKINJE}
+
+
+@pytest.fixture(scope="module")
+def harness():
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    if not os.path.exists(nvcc) and shutil.which("nvcc") is None:
+        pytest.skip("nvcc not available to build the host harness")
+    nvcc = nvcc if os.path.exists(nvcc) else shutil.which("nvcc")
+    if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(d) for d in DEPS):
+        os.makedirs(os.path.dirname(OUT), exist_ok=True)
+        subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17",
+                        "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-I", os.path.join(ROOT, "include"),
+                        "-o", OUT, SRC], check=True, capture_output=True)
+    L = C.CDLL(OUT)
+    dp = C.POINTER(C.c_double)
+    L.cells_host_compute_ion.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_int,
+                                         C.c_void_p, dp, C.c_int, C.c_int, C.c_double, C.c_int, dp, dp, dp, dp,
+                                         C.POINTER(C.c_longlong)]
+    return L
+
+
+def _consts(model, types):
+    if model == PURKINJE:
+        return O.pk_constants()[None, :]
+    ntypes = int(types.max()) + 1 if types is not None and len(types) else 1
+    return np.stack([capi.default_consts(model, t) for t in range(ntypes)])
+
+
+def compute(L, model, V, istim, states, dt, types=None, jac_true=0):
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    istim = np.ascontiguousarray(istim, dtype=np.float64)
+    states = np.array(states, dtype=np.float64)
+    k = np.ascontiguousarray(_consts(model, types))
+    t = None if types is None else np.ascontiguousarray(types, dtype=np.uint8)
+    dv = np.zeros(len(V))
+    work = C.c_longlong(0)
+    rc = L.cells_host_compute_ion(model, len(V), dt, 1.0, XI[model], p(k), k.shape[1],
+                                  t.ctypes.data_as(C.c_void_p) if t is not None else None, None, jac_true,
+                                  0, 0.0, 0, p(V), p(istim), p(states), p(dv), C.byref(work))
+    assert rc == 0
+    return dv, states, work.value
+
+
+@pytest.mark.parametrize("name", list(NAMES))
+def test_device_model_source_matches_the_reference_kat(harness, name):
+    """One Compute_Ion call on 128-384 states from the reference's own
+    trajectory: returned dV/dt and advanced states to 1e-9 relative."""
+    g = np.load(os.path.join(GOLD, f"kat_{name}.npz"))
+    model = NAMES[name]
+    types = g["types"] if model in (capi.MAHAJAN, capi.MAHAJAN_FAIL) else None
+    dv, so, _ = compute(harness, model, g["V"], g["istim"], g["states_in"], float(g["dt"]), types)
+    scale = np.maximum(np.abs(g["dvdt"]), 1.0)
+    assert np.max(np.abs(dv - g["dvdt"]) / scale) < 1e-9
+    sr = g["states_out"]
+    assert np.max(np.abs(so - sr) / np.maximum(np.abs(sr), 1e-12)) < 1e-9
+
+
+def test_purkinje_device_source_follows_the_reference_action_potential(harness):
+    """The Purkinje cell's device source through the reference's single-cell
+    action potential (500 ms, split update V += dt dV/dt, 1 ms stimulus):
+    both branches of the adaptive Euler taken, V within 1e-6 mV of the
+    reference everywhere."""
+    g = np.load(os.path.join(GOLD, "cell_purkinje.npz"))
+    dt, t_stim = float(g["dt"]), float(g["t_stim"])
+    s = O.initial_state(O.PURKINJE)[None, :]
+    V = s[:, 0].copy()
+    every = int(round(1.0 / dt))
+    Vs, sub = [], 0
+    for k in range(int(round(g["t"][-1] / dt)) + every):
+        ist = np.full(1, 50.0 * 2500.0 if t_stim <= k * dt < t_stim + 1.0 else 0.0)
+        if k % every == 0:
+            Vs.append(V.copy())
+        dv, s, w = compute(harness, PURKINJE, V, ist, s, dt)
+        sub += w
+        V = V + dt * dv
+    Vs = np.array(Vs)
+    assert sub > 0
+    assert np.max(np.abs(Vs - g["V"])) < 1e-6
+    assert np.max(np.abs(V - g["V_end"])) < 1e-6
