@@ -93,6 +93,56 @@ def test_mesh_reader_skips_cables(tmp_path):
     assert m.m == 1 and other == 1 and list(purk) == [4, 5]
 
 
+def test_mixed_mesh_cables_read_and_assembled(tmp_path):
+    """A MIX3D mesh (tets + 2-node cables, .cell with LV Purkinje type 11,
+    .fibers for every element, .angle override): the cable reader feeds the
+    library's host assembly, which equals the oracle's on the same data."""
+    from oracle import oracle as O
+    from ucla_cmg_b200 import simulation as S
+    m = M.slab(5, 4, 3, 0.4, 0.3, 0.2)
+    n0 = m.n
+    extra = m.xyz[[0]] + np.array([[0.0, 0.0, -0.05], [0.0, 0.0, -0.1]])
+    xyz = np.vstack([m.xyz, extra])
+    bars = np.array([[0, n0], [n0, n0 + 1], [1, 0]])
+    base = str(tmp_path / "mix")
+    with open(base + ".node", "w") as f:
+        f.write(f"{len(xyz)} 3 0 0\n")
+        for i, p in enumerate(xyz):
+            f.write(f"{i + 1} {p[0]:.17g} {p[1]:.17g} {p[2]:.17g}\n")
+    # elements interleaved as a MIX3D .ele may hold them
+    rng = np.random.default_rng(0)
+    bfib = np.array([np.linalg.qr(rng.normal(size=(3, 3)))[0].T.reshape(-1) for _ in bars])
+    elems, fibs = [], []
+    for e, tet in enumerate(m.tets):
+        elems.append([4] + list(tet + 1)); fibs.append(m.fibers[e])
+        if e < len(bars):
+            elems.append([2] + list(bars[e] + 1)); fibs.append(bfib[e])
+    with open(base + ".ele", "w") as f:
+        f.write(f"{len(elems)} 0 0\n")
+        for e, el in enumerate(elems):
+            f.write(" ".join(str(v) for v in [e + 1] + el) + "\n")
+    np.savetxt(base + ".fibers", np.array(fibs))
+    cell = np.zeros(len(xyz), np.uint8); cell[[n0 + 1]] = 11
+    with open(base + ".cell", "w") as f:
+        for i in range(len(xyz)):
+            f.write(f"{i + 1} {cell[i]}\n")
+    with open(base + ".angle", "w") as f:
+        f.write(f"{n0 + 1} 0 0 -1 0.06\n")
+    mesh, t, purk, other = IO.read_mesh(base)
+    cab = IO.read_cables(base, t)
+    assert other == len(bars) and np.array_equal(cab["bars"], bars)
+    assert np.allclose(cab["fibers"], bfib) and list(cab["lv"]) == [0, 1, 0]
+    assert cab["angle"] == {n0: (0.0, 0.0, -1.0, 0.06)}
+    kw = dict(Dp=(0.0016, 0.0008, 0.0004), DpLeft=(0.003, 0.001, 0.0005), radius=0.0275)
+    D = M.sigma_to_D(1.2, 0.2)
+    A, B, CL = S.assemble_operators(mesh, D, 0.1, bars=cab["bars"], bar_fibers=cab["fibers"], lv=cab["lv"],
+                                    angle=cab["angle"], **kw)
+    o = O.Csr(mesh.xyz, mesh.tets, mesh.fibers, D, 1.0, 0.1,
+              cables=O.Cables(cab["bars"], fibers=cab["fibers"], lv=cab["lv"], orient=cab["angle"], n=mesh.n, **kw))
+    assert abs(A - o.scipy("A")).max() <= 1e-15 * abs(A).max()
+    assert np.allclose(CL, o.arr("CL"), rtol=1e-15, atol=0)
+
+
 def test_schedule_matches_oracle_restatement():
     """The driver's two-pointer schedule against the oracle's C restatement
     of the same EPSimulator logic, on sorted and unsorted lists."""

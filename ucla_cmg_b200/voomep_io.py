@@ -12,7 +12,10 @@ Formats as the reference reads them (voomEP/src/Mesh/Mesh.cc):
 * ``<base>.cell``: lines ``nodeID typeID`` (1-based node ids), the tissue
   type of each node, default 0 (Mesh.cc:391-401);
 * ``<base>.purk``: ``n`` then n 1-based node ids of Purkinje nodes
-  (Mesh.cc:377-388).
+  (Mesh.cc:377-388);
+* ``<base>.angle``: lines ``nodeID dx dy dz length`` overriding the direction
+  and length of the cable that starts at that node (Mesh.cc:403-416,
+  MixedMesh3D.cc:31-34, 89-92).
 """
 import os
 
@@ -49,6 +52,41 @@ def read_ele(path):
         else:
             other += 1
     return np.array(tets, dtype=np.int32).reshape(-1, 4), np.array(which, dtype=np.int64), other
+
+
+def read_cables(base, node_type=None):
+    """The 2-node Purkinje cables of a mixed mesh ``base``: dict with
+    ``bars`` [nb x 2] zero-based in .ele order, ``fibers`` [nb x 9] or None
+    (from .fibers, in .ele order), ``lv`` [nb] (1 where either node has
+    tissue type 11: the left-ventricular Purkinje diffusion,
+    CardiacBody.cc:107-110) and ``angle`` {zero-based node: (dx, dy, dz,
+    length)} from .angle (empty if absent)."""
+    with open(base + ".ele") as f:
+        tok = f.read().split()
+    ne = int(tok[0])
+    pos = 3
+    bars, which = [], []
+    for e in range(ne):
+        k = int(tok[pos + 1])
+        conn = tok[pos + 2:pos + 2 + k]
+        pos += 2 + k
+        if k == 2:
+            bars.append([int(c) - 1 for c in conn])
+            which.append(e)
+    bars = np.array(bars, dtype=np.int32).reshape(-1, 2)
+    fib = None
+    if os.path.exists(base + ".fibers") and len(bars):
+        fib = read_fibers(base + ".fibers", ne)[np.array(which, dtype=np.int64)]
+    lv = np.zeros(len(bars), np.uint8)
+    if node_type is not None and len(bars):
+        lv = ((node_type[bars[:, 0]] == 11) | (node_type[bars[:, 1]] == 11)).astype(np.uint8)
+    angle = {}
+    if os.path.exists(base + ".angle"):
+        with open(base + ".angle") as f:
+            a = f.read().split()
+        for k in range(len(a) // 5):
+            angle[int(a[5 * k]) - 1] = tuple(float(v) for v in a[5 * k + 1:5 * k + 5])
+    return {"bars": bars, "fibers": fib, "lv": lv, "angle": angle}
 
 
 def read_fibers(path, n_elems):
