@@ -191,6 +191,16 @@ def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=
     raise ValueError(kernel)
 
 
+def node_step_bytes(n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_every=10, cg_predict=0):
+    """Algorithmic bytes of one node-step: the ionic phase, the two CN half
+    steps and the ECG sample share, per node (the whole-step roofline: these
+    bytes x node-steps/s against the copy bandwidth)."""
+    tot = (algorithmic_bytes("ionic", n, nnz, cg_iters_per_solve, rbytes, nstate=nstate)
+           + 2 * algorithmic_bytes("cg", n, nnz, cg_iters_per_solve, rbytes, cg_predict=cg_predict)
+           + algorithmic_bytes("ecg", n, nnz, cg_iters_per_solve, rbytes, ne=ne) / max(1, ecg_every))
+    return tot / n
+
+
 def cpu_sample(kind, h, steps, threads):
     """Time the CPU path on a coarser shell (same model, dt, stimuli).
     kind 'reference': the reference cell objects (oracle/_ref) in the C
@@ -326,6 +336,9 @@ def run_ours(args, rank, world, local):
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom, args.form, cg_per_solve, g.launch_config()["cg_predict"]) if wl.name == "shell_c2" else None,
             "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
             "kernel_ms": kms}
+    b_ns = node_step_bytes(n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes), ecg_every=ecg_every,
+                           cg_predict=g.launch_config()["cg_predict"])
+    roof["step"] = {"bytes_per_node_step": b_ns, "achieved": b_ns * value / 1e9, "frac": b_ns * value / 1e9 / peak}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else ("bf16+f32" if prec == capi.SURROGATE else "f32"),

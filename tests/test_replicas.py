@@ -49,3 +49,15 @@ def test_reference_arm_only_on_rank0(capsys):
         gpus, steps, warmup = 2, 1, 1
     assert bench.run_reference(A, 1, 2) is None
     assert capsys.readouterr().out == ""
+
+
+def test_node_step_bytes_is_the_sum_of_the_phases():
+    """The whole-step roofline counts, per node-step, the ionic phase, two CN
+    half steps (prologue + iterations, predictor passes) and the ECG share."""
+    n, nnz = 1000, 15000
+    z = nnz / n
+    for k, pred in ((4.0, 0), (8.5, 1), (8.5, 2)):
+        b = bench.node_step_bytes(n, nnz, k, 4, nstate=19, ne=10, ecg_every=10, cg_predict=pred)
+        extra = 0 if not pred else (3 * pred + 4) * 4      # k gathers + V saved; x, V, k read, x + k written
+        cg = z * 12 + 5 * 4 + extra + k * (z * 8 + 12 * 4)
+        assert abs(b - ((2 * 19 * 4 + 16 + 1 + 4 + 4) + 2 * cg + 11 * 4 / 10)) < 1e-9
