@@ -964,6 +964,45 @@ void epo_cells_ionic_cb(void *ctx, double Cm, double dt, const double *V,
     epo_cells_compute_ion((epo_cells *)ctx, Cm, dt, V, istim, dvdt);
 }
 
+void epo_mixed_init(epo_mixed *m, int n, const uint8_t *is_purk, epo_ionic_fn tfn, void *tctx,
+                    epo_ionic_fn pfn, void *pctx)
+{
+    memset(m, 0, sizeof *m);
+    m->n = n;
+    m->tmap = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    m->pmap = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; i++) {
+        if (is_purk && is_purk[i]) m->pmap[m->np++] = i;
+        else m->tmap[m->nt++] = i;
+    }
+    m->tfn = tfn; m->tctx = tctx; m->pfn = pfn; m->pctx = pctx;
+    m->buf = (double *)malloc(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
+}
+
+void epo_mixed_free(epo_mixed *m)
+{
+    free(m->tmap); free(m->pmap); free(m->buf);
+    memset(m, 0, sizeof *m);
+}
+
+/* one population: gather, Compute_Ion, scatter */
+static void mixed_part(const epo_mixed *m, const int *map, int cnt, epo_ionic_fn fn, void *ctx, double Cm,
+                       double dt, const double *V, const double *istim, double *dvdt)
+{
+    if (cnt == 0) return;
+    double *v = m->buf, *ist = m->buf + m->n, *d = m->buf + 2 * (size_t)m->n;
+    for (int k = 0; k < cnt; k++) { v[k] = V[map[k]]; ist[k] = istim[map[k]]; }
+    fn(ctx, Cm, dt, v, ist, d);
+    for (int k = 0; k < cnt; k++) dvdt[map[k]] = d[k];
+}
+
+void epo_mixed_ionic_cb(void *ctx, double Cm, double dt, const double *V, const double *istim, double *dvdt)
+{
+    const epo_mixed *m = (const epo_mixed *)ctx;
+    mixed_part(m, m->tmap, m->nt, m->tfn, m->tctx, Cm, dt, V, istim, dvdt);
+    mixed_part(m, m->pmap, m->np, m->pfn, m->pctx, Cm, dt, V, istim, dvdt);
+}
+
 /* ====================================================================== */
 /* P1 tetrahedra -- TetMesh.cc, CardiacBody.cc                             */
 /* ====================================================================== */

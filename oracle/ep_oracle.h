@@ -207,6 +207,26 @@ double epo_cells_ionic_node_cb(void *ctx, int i, double Cm, double dt, double V,
 void epo_cells_ionic_cb(void *ctx, double Cm, double dt, const double *V,
                         const double *istim, double *dvdt);
 
+/* Two cell populations in one tissue (CardiacBody::New, CardiacBody.cc:982-1101:
+ * the .purk nodes carry the Purkinje cell, every other node the tissue model):
+ * each population is a compact set of cells behind its own callback (the
+ * restatement's epo_cells_ionic_cb or the reference objects'), the mixed
+ * callback gathers V and istim per population, calls both and scatters
+ * dV/dt back. */
+typedef struct epo_mixed {
+    int n, nt, np;
+    int *tmap, *pmap;                 /* compact index -> node */
+    epo_ionic_fn tfn, pfn;
+    void *tctx, *pctx;
+    double *buf;                      /* 3 * n scratch */
+} epo_mixed;
+/* is_purk[n]: 1 on Purkinje nodes.  The populations must hold nt and np
+ * cells in increasing node order. */
+void epo_mixed_init(epo_mixed *m, int n, const uint8_t *is_purk, epo_ionic_fn tfn, void *tctx,
+                    epo_ionic_fn pfn, void *pctx);
+void epo_mixed_free(epo_mixed *m);
+void epo_mixed_ionic_cb(void *ctx, double Cm, double dt, const double *V, const double *istim, double *dvdt);
+
 /* Stimulus schedule of EPSimulator.cc:483-570 for nodal stimuli: given
  * stimuli (t_start, t_stop) in list order, the step indices at which each
  * one starts/stops under the reference's single-pointer logic.  A value of

@@ -112,6 +112,9 @@ def lib():
         L.epo_mh_initial_state.argtypes = [dp, C.c_int]
         L.epo_lr_initial_state.argtypes = [dp]
         L.epo_pk_constants.argtypes = [dp]
+        L.epo_mixed_init.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+        L.epo_mixed_free.argtypes = [C.c_void_p]
         L.epo_pk_initial_state.argtypes = [dp]
         _LIB = L
     return _LIB
@@ -412,6 +415,42 @@ def num_steps(dt, T):
     return lib().epo_num_steps(dt, T)
 
 
+class _Mixed(C.Structure):
+    _fields_ = [("n", C.c_int), ("nt", C.c_int), ("np", C.c_int), ("tmap", ip), ("pmap", ip),
+                ("tfn", C.c_void_p), ("pfn", C.c_void_p), ("tctx", C.c_void_p), ("pctx", C.c_void_p),
+                ("buf", dp)]
+
+
+def _cb(cells):
+    """(callback, context) of a population for the split step."""
+    if isinstance(cells, RefCells):
+        return C.cast(ref_lib().ref_cells_ionic_cb, C.c_void_p), C.c_void_p(cells.h)
+    return C.cast(lib().epo_cells_ionic_cb, C.c_void_p), C.cast(cells.h, C.c_void_p)
+
+
+class MixedCells:
+    """A tissue model on every node but the Purkinje nodes (is_purk), which
+    carry the Purkinje cell (CardiacBody::New): two compact populations in
+    increasing node order, each a Cells or a RefCells."""
+
+    def __init__(self, tissue, purk, is_purk):
+        self.tissue, self.purk = tissue, purk
+        self.is_purk = np.ascontiguousarray(is_purk, dtype=np.uint8)
+        self.n = len(self.is_purk)
+        assert tissue.n == int((self.is_purk == 0).sum()) and purk.n == int(self.is_purk.sum())
+        self.m = _Mixed()
+        tf, tc = _cb(tissue)
+        pf, pc = _cb(purk)
+        self._mp = C.cast(C.pointer(self.m), C.c_void_p)
+        lib().epo_mixed_init(self._mp, self.n, self.is_purk.ctypes.data_as(C.c_void_p), tf, tc, pf, pc)
+
+    def __del__(self):
+        try:
+            lib().epo_mixed_free(self._mp)
+        except Exception:
+            pass
+
+
 class Sim:
     """The split time step (EP_CrankNicholson::Solve) on the oracle.
 
@@ -423,7 +462,12 @@ class Sim:
                  jacobi_steps=3):
         self.csr, self.cells = csr, cells
         self.s = _Sim()
-        if isinstance(cells, RefCells):
+        if isinstance(cells, MixedCells):
+            L = lib()
+            fn = C.cast(L.epo_mixed_ionic_cb, C.c_void_p)
+            ctx = C.cast(C.pointer(cells.m), C.c_void_p)
+            self._L = L
+        elif isinstance(cells, RefCells):
             L = ref_lib()
             fn = C.cast(L.ref_cells_ionic_cb, C.c_void_p)
             ctx = C.c_void_p(cells.h)

@@ -319,3 +319,95 @@ def test_cable_orientation_override_sticks_like_the_reference():
     assert np.isclose(Ks[1, 2], Kp[1, 2] / 2) and np.isclose(Kn[1, 2], Kp[1, 2] / 2)   # bar 1: length 0.2
     assert np.isclose(Ks[3, 4], Kp[3, 4] / 2)                                    # bar 3: sticky
     assert np.isclose(Kn[3, 4], Kp[3, 4])                                        # bar 3: its own geometry
+
+
+def _cable_slab(k=10, h=0.05):
+    m = M.slab(9, 7, 4, 0.8, 0.6, 0.3)
+    n0 = m.n
+    extra = m.xyz[[0]] + np.stack([np.zeros(k), np.zeros(k), -h * np.arange(1, k + 1)], 1)
+    xyz = np.vstack([m.xyz, extra])
+    bars = np.array([[0, n0]] + [[n0 + j, n0 + j + 1] for j in range(k - 1)])
+    is_purk = np.zeros(len(xyz), np.uint8)
+    is_purk[n0:] = 1
+    return m, xyz, bars, is_purk
+
+
+def test_mixed_populations_without_purkinje_nodes_equal_the_tissue_alone(small_slab):
+    m = small_slab
+    D = M.sigma_to_D(1.2, 0.2)
+    c = O.Csr(m.xyz, m.tets, m.fibers, D, 1.0, 0.02)
+    a_cells = O.Cells(O.TUSSCHER, m.n, tt_jac_true=1)
+    b_cells = O.Cells(O.TUSSCHER, m.n, tt_jac_true=1)
+    mix = O.MixedCells(b_cells, O.Cells(O.PURKINJE, 0), np.zeros(m.n, np.uint8))
+    sa = O.Sim(c, a_cells, 0.02, 0.02, jacobi_steps=1)
+    sb = O.Sim(c, mix, 0.02, 0.02, jacobi_steps=1)
+    blk = M.corner_block(m, 3, 3)
+    for s in (sa, sb):
+        s.V[:] = -85.423
+    for step in range(150):
+        for s in (sa, sb):
+            s.istim[:] = 0.0
+            if step < 50:
+                s.istim[blk] = 50.0 * 2000.0
+            s.step(1)
+    assert np.max(sa.V) > 0.0
+    # the oracle's OpenMP dot products combine partial sums in thread order:
+    # equal to rounding, not bit for bit
+    assert np.max(np.abs(sa.V - sb.V)) < 1e-9 * np.max(np.abs(sa.V))
+
+
+def test_mixed_restatement_equals_the_reference_objects():
+    """Tissue (TT) plus a Purkinje cable whose far end is stimulated: the
+    split step with the restated populations follows the one with the
+    reference's own cell objects in both populations."""
+    if O.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    m, xyz, bars, is_purk = _cable_slab()
+    n0, n = m.n, len(xyz)
+    D = M.sigma_to_D(1.2, 0.2)
+    dt = 0.01                                    # the reference TT Newton layout needs dt <= 0.01
+    c = O.Csr(xyz, m.tets, m.fibers, D, 1.0, dt, cables=O.Cables(bars, radius=0.0275))
+    sims = []
+    for ref in (False, True):
+        tis = O.RefCells(O.TUSSCHER, n0) if ref else O.Cells(O.TUSSCHER, n0)
+        pk = O.RefCells(O.PURKINJE, n - n0) if ref else O.Cells(O.PURKINJE, n - n0)
+        mix = O.MixedCells(tis, pk, is_purk)
+        s = O.Sim(c, mix, dt, dt, jacobi_steps=1, cg_tol=1e-12)
+        s.V[:n0] = -85.423
+        s.V[n0:] = -88.34
+        sims.append((s, mix))
+    for step in range(400):
+        for s, _ in sims:
+            s.istim[:] = 0.0
+            if step < 200:
+                s.istim[n - 3:] = 2 * 50.0 * 2500.0
+            s.step(1)
+    Va, Vb = sims[0][0].V, sims[1][0].V
+    assert np.max(Va[n0:]) > 0.0                # the cable fired
+    assert np.max(np.abs(Va - Vb)) < 1e-6 * np.max(np.abs(Vb))
+
+
+def test_purkinje_cable_drives_the_tissue():
+    """The stimulated far end of a 10-element cable (0.5 cm, r = 0.0275 cm)
+    sends a wave down the Purkinje cells (~1 m/s) into the tissue at the
+    junction node, which then activates part of the slab."""
+    m, xyz, bars, is_purk = _cable_slab()
+    n0, n = m.n, len(xyz)
+    c = O.Csr(xyz, m.tets, m.fibers, M.sigma_to_D(1.2, 0.2), 1.0, 0.02, cables=O.Cables(bars, radius=0.0275))
+    mix = O.MixedCells(O.Cells(O.TUSSCHER, n0, tt_jac_true=1), O.Cells(O.PURKINJE, n - n0), is_purk)
+    s = O.Sim(c, mix, 0.02, 0.02, jacobi_steps=1, cg_tol=1e-10)
+    s.V[:n0] = -85.423
+    s.V[n0:] = -88.34
+    tact = np.full(n, -1.0)
+    for step in range(700):
+        s.istim[:] = 0.0
+        if step < 100:
+            s.istim[n - 3:] = 2 * 50.0 * 2500.0
+        s.step(1)
+        new = (tact < 0) & (s.V > -40.0)
+        tact[new] = (step + 1) * 0.02
+    cable = tact[n0:]
+    assert np.all(cable > 0) and np.all(np.diff(cable[:8]) < 0)     # activation travels toward the junction
+    speed = 7 * 0.05 / (cable[0] - cable[7])                           # cm/ms
+    assert 0.05 < speed < 0.5
+    assert tact[0] > cable[0] and np.sum(tact[:n0] > 0) > 5
