@@ -44,7 +44,7 @@ def harness():
     dp = C.POINTER(C.c_double)
     L.cells_host_compute_ion.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_int,
                                          C.c_void_p, dp, C.c_int, C.c_int, C.c_double, C.c_int, dp, dp, dp, dp,
-                                         C.POINTER(C.c_longlong)]
+                                         C.POINTER(C.c_longlong), C.c_int]
     return L
 
 
@@ -55,7 +55,7 @@ def _consts(model, types):
     return np.stack([capi.default_consts(model, t) for t in range(ntypes)])
 
 
-def compute(L, model, V, istim, states, dt, types=None, jac_true=0):
+def compute(L, model, V, istim, states, dt, types=None, jac_true=0, fp32=False):
     p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
     V = np.ascontiguousarray(V, dtype=np.float64)
     istim = np.ascontiguousarray(istim, dtype=np.float64)
@@ -66,7 +66,7 @@ def compute(L, model, V, istim, states, dt, types=None, jac_true=0):
     work = C.c_longlong(0)
     rc = L.cells_host_compute_ion(model, len(V), dt, 1.0, XI[model], p(k), k.shape[1],
                                   t.ctypes.data_as(C.c_void_p) if t is not None else None, None, jac_true,
-                                  0, 0.0, 0, p(V), p(istim), p(states), p(dv), C.byref(work))
+                                  0, 0.0, 0, p(V), p(istim), p(states), p(dv), C.byref(work), int(fp32))
     assert rc == 0
     return dv, states, work.value
 
@@ -83,6 +83,20 @@ def test_device_model_source_matches_the_reference_kat(harness, name):
     assert np.max(np.abs(dv - g["dvdt"]) / scale) < 1e-9
     sr = g["states_out"]
     assert np.max(np.abs(so - sr) / np.maximum(np.abs(sr), 1e-12)) < 1e-9
+
+
+@pytest.mark.parametrize("name", list(NAMES))
+def test_device_model_source_in_fp32(harness, name):
+    """The same source in FP32 (the FP32 kernels' precision, with the scaled
+    Newton tolerance for TT): the returned rate within the bounds the GPU
+    FP32 test holds the kernels to."""
+    g = np.load(os.path.join(GOLD, f"kat_{name}.npz"))
+    model = NAMES[name]
+    types = g["types"] if model in (capi.MAHAJAN, capi.MAHAJAN_FAIL) else None
+    dv, _, _ = compute(harness, model, g["V"], g["istim"], g["states_in"], float(g["dt"]), types, fp32=True)
+    scale = np.maximum(np.abs(g["dvdt"]), 1.0)
+    assert np.median(np.abs(dv - g["dvdt"]) / scale) < 1e-4
+    assert np.max(np.abs(dv - g["dvdt"]) / scale) < 5e-2
 
 
 def test_purkinje_device_source_follows_the_reference_action_potential(harness):
