@@ -25,6 +25,9 @@ Stimulus Circ 0.1 0.2 0.0 0.05 5.0 6.0 30000
 Stimulus Zonal y 0.1 7 8
 Stimulus Plane 0 0 0 1 0 0 9 10 100
 MechDt 999
+TwoDRadius 0.03
+PurkinjeDiffusion 0.004 0.004 0.004
+LVPurkinjeDiffusion 0.008 0.008 0.008
 """)
     c = D.parse_input(str(f))
     assert c["model"] == "Mesh/slab" and c["output_dir"] == "out/" and c["cell_model"] == "Tusscher"
@@ -38,6 +41,10 @@ MechDt 999
     assert s[2]["axis"] == 1 and s[2]["limit"] == 0.1
     assert s[3]["normal"] == [1.0, 0.0, 0.0] and s[3]["t_start"] == 9.0
     assert "MECHDT" in c["ignored"]
+    assert c["radius"] == 0.03 and c["Dp"] == [0.004] * 3 and c["DpLeft"] == [0.008] * 3
+    f.write_text("MODEL m\n")
+    d = D.parse_input(str(f))
+    assert d["radius"] == 0.0275 and d["Dp"] == [0.0032] * 3        # EPSimulator.cc:89, 102-103
 
 
 def test_stimulus_pointer_schedule():
@@ -130,14 +137,19 @@ def test_mixed_mesh_cables_read_and_assembled(tmp_path):
         f.write(f"{n0 + 1} 0 0 -1 0.06\n")
     mesh, t, purk, other = IO.read_mesh(base)
     cab = IO.read_cables(base, t)
+    # the driver's view: LV cables take PURKINJEDIFFUSION as in the reference
+    cfg = {"input_dir": str(tmp_path), "model": "mix", "radius": 0.0275, "Dp": [0.002] * 3,
+           "DpLeft": [0.009] * 3, "quad_order": 2}
+    setup = D.cable_setup(cfg, t)
+    assert np.array_equal(setup["bars"], bars) and setup["DpLeft"] == setup["Dp"] == (0.002,) * 3
     assert other == len(bars) and np.array_equal(cab["bars"], bars)
     assert np.allclose(cab["fibers"], bfib) and list(cab["lv"]) == [0, 1, 0]
     assert cab["angle"] == {n0: (0.0, 0.0, -1.0, 0.06)}
     kw = dict(Dp=(0.0016, 0.0008, 0.0004), DpLeft=(0.003, 0.001, 0.0005), radius=0.0275)
-    D = M.sigma_to_D(1.2, 0.2)
-    A, B, CL = S.assemble_operators(mesh, D, 0.1, bars=cab["bars"], bar_fibers=cab["fibers"], lv=cab["lv"],
+    Dt = M.sigma_to_D(1.2, 0.2)
+    A, B, CL = S.assemble_operators(mesh, Dt, 0.1, bars=cab["bars"], bar_fibers=cab["fibers"], lv=cab["lv"],
                                     angle=cab["angle"], **kw)
-    o = O.Csr(mesh.xyz, mesh.tets, mesh.fibers, D, 1.0, 0.1,
+    o = O.Csr(mesh.xyz, mesh.tets, mesh.fibers, Dt, 1.0, 0.1,
               cables=O.Cables(cab["bars"], fibers=cab["fibers"], lv=cab["lv"], orient=cab["angle"], n=mesh.n, **kw))
     assert abs(A - o.scipy("A")).max() <= 1e-15 * abs(A).max()
     assert np.allclose(CL, o.arr("CL"), rtol=1e-15, atol=0)

@@ -34,9 +34,16 @@ Same as the reference:
   ``int(FREQUENCY/DT)`` steps; restart files every ``long(WRITERESTART/DT)``
   steps; simulated time accumulated as ``simtime += dt``.
 
+The Purkinje keys (TWODRADIUS, PURKINJEDIFFUSION, LVPURKINJEDIFFUSION, with
+the reference's defaults 0.0275 cm and 0.0032 cm^2/ms, EPSimulator.cc:89,
+102-103) are read and the 2-node cables of a MIX3D mesh are read with their
+LV flags and .angle overrides (``voomep_io.read_cables``); as in the
+reference, the LV cables get PURKINJEDIFFUSION, not LVPURKINJEDIFFUSION
+(``setPurkinjeDiffusionInLV(Dp)``, EPSimulator.cc:420-421).  The cables are
+not yet run on the GPU: the driver reports them and runs the tets.
+
 Not on this path (accepted and ignored, with a note): the mechanics keys,
-Purkinje diffusion keys and 2-node Purkinje elements (the Purkinje network is
-not modelled), QUADORDER other than 2, CONSISTENCYCHECK.  The ZONAL stop of
+QUADORDER other than 2, CONSISTENCYCHECK.  The ZONAL stop of
 the reference also runs the PLANE stop with the start pointer's plane (a
 missing ``break``, EPSimulator.cc:557-563); that side effect is not
 reproduced.
@@ -60,7 +67,7 @@ def parse_input(path):
     cfg = dict(model=None, output_dir="Output/", cell_model="MAHAJAN", mesh_type="MIX3D", quad_order=2,
                ionic_dt=0.1, dt=0.1, read_restart=None, write_restart=99999.0, simulation_time=300.0,
                frequency=1.0, D=[0.001, 0.0005, 0.00025], smoothing=None, initial_states=None,
-               stimuli=[], ignored=[])
+               stimuli=[], ignored=[], radius=0.0275, Dp=[0.0032] * 3, DpLeft=[0.0032] * 3)
     base = os.path.dirname(os.path.abspath(path))
     with open(path) as f:
         for line in f:
@@ -93,6 +100,12 @@ def parse_input(path):
                 cfg["frequency"] = float(s[1])
             elif key == "TISSUEDIFFUSION":
                 cfg["D"] = [float(v) for v in s[1:4]]
+            elif key == "TWODRADIUS":
+                cfg["radius"] = float(s[1])
+            elif key == "PURKINJEDIFFUSION":
+                cfg["Dp"] = [float(v) for v in s[1:4]]
+            elif key == "LVPURKINJEDIFFUSION":
+                cfg["DpLeft"] = [float(v) for v in s[1:4]]
             elif key == "SMOOTHING":
                 cfg["smoothing"] = float(s[1]) if len(s) == 2 else 0.1
             elif key == "INITIALSTATES":
@@ -224,6 +237,19 @@ def read_initial_states(path):
     return np.array(cell), np.array(purk)
 
 
+def cable_setup(cfg, node_type):
+    """The 2-node cables of the input's MIX3D mesh as the reference would
+    assemble them: dict for ``simulation.assemble_operators`` (bars, fibres,
+    LV flags, .angle overrides, radius, and Dp for both RV and LV cables,
+    EPSimulator.cc:420-421), or None when the mesh has none."""
+    from .voomep_io import read_cables
+    cab = read_cables(os.path.join(cfg["input_dir"], cfg["model"]), node_type)
+    if not len(cab["bars"]):
+        return None
+    return dict(bars=cab["bars"], bar_fibers=cab["fibers"], lv=cab["lv"], angle=cab["angle"],
+                radius=cfg["radius"], Dp=tuple(cfg["Dp"]), DpLeft=tuple(cfg["Dp"]), quad_order=cfg["quad_order"])
+
+
 def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate_path=None, verbose=True,
         tt_jacobian=capi.TT_JAC_TRUE):
     cfg = parse_input(input_file)
@@ -231,7 +257,10 @@ def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate
     model = CELL_MODELS[cfg["cell_model"].upper()]
     mesh, node_type, purk, other = read_mesh(os.path.join(base_dir, cfg["model"]))
     if other and verbose:
-        print(f"** {other} non-tet elements (Purkinje cables) are not modelled on this path")
+        cab = cable_setup(cfg, node_type)
+        nb = 0 if cab is None else len(cab["bars"])
+        print(f"** {other} non-tet elements ({nb} Purkinje cables, radius {cfg['radius']} cm, "
+              f"D_p {cfg['Dp'][0]}) are read but not run on this path yet")
     nstate = capi.model_nstate(model)
     init = None
     if cfg["initial_states"]:
