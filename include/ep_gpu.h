@@ -40,6 +40,11 @@ extern "C" {
 #define EP_TUSSCHER         2
 #define EP_MAHAJAN          3
 #define EP_MAHAJAN_FAIL     4
+/* not in CellModelType: the Purkinje cell CardiacBody::New gives every .purk
+ * node (Body/CardiacBody.cc:982-1101; IonicModel/Purkinje.cc).  Plugin level
+ * (ep_ionic_step, ep_ionic_phase) only: ep_create rejects it until mixed
+ * tissues (a tissue model plus Purkinje cells on cable nodes) are built. */
+#define EP_PURKINJE         5
 
 /* ---- arithmetic of the ionic update and the SpMV ---- */
 #define EP_FP64       0   /* everything FP64 */

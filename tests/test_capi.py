@@ -48,6 +48,8 @@ def test_constants_match_oracle():
     for t in range(9):
         assert np.array_equal(capi.default_consts(capi.MAHAJAN, t), O.mh_constants(t))
         assert np.array_equal(capi.default_consts(capi.MAHAJAN_FAIL, t), O.mh_constants(t, True))
+    assert capi.lib().ep_model_nstate(capi.PURKINJE) == 22
+    assert np.array_equal(capi.default_consts(capi.PURKINJE), O.pk_constants())
 
 
 def test_bad_arguments_return_codes():

@@ -11,7 +11,7 @@ from ucla_cmg_b200.simulation import ionic_step
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = {"tt": capi.TUSSCHER, "mahajan": capi.MAHAJAN, "mahajan_fail": capi.MAHAJAN_FAIL,
-         "lr": capi.LUORUDY, "lrgate": capi.LUORUDYWITHGATE}
+         "lr": capi.LUORUDY, "lrgate": capi.LUORUDYWITHGATE, "purkinje": capi.PURKINJE}
 
 pytestmark = pytest.mark.gpu
 

@@ -18,6 +18,7 @@ ERRORS = {-1: "EP_ERR_ARG", -2: "EP_ERR_CUDA", -3: "EP_ERR_NOMEM", -4: "EP_ERR_M
           -9: "EP_ERR_UNSUPPORTED", -10: "EP_ERR_IO"}
 
 LUORUDY, LUORUDYWITHGATE, TUSSCHER, MAHAJAN, MAHAJAN_FAIL = 0, 1, 2, 3, 4
+PURKINJE = 5          # the Purkinje cell of .purk nodes (plugin level: ep_ionic_step)
 FP64, FP32, SURROGATE = 0, 1, 2
 TT_JAC_REFERENCE, TT_JAC_TRUE = 0, 1
 SCHEME_CN, SCHEME_BE, SCHEME_EXPLICIT = 0, 1, 2

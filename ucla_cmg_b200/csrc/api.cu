@@ -636,6 +636,7 @@ int ep_model_nstate(int model) {
     case EP_TUSSCHER: return 19;
     case EP_MAHAJAN: case EP_MAHAJAN_FAIL: return 26;
     case EP_LUORUDY: case EP_LUORUDYWITHGATE: return 8;
+    case EP_PURKINJE: return 22;
     default: return EP_ERR_ARG;
     }
 }
@@ -645,6 +646,7 @@ int ep_model_nconst(int model) {
     case EP_TUSSCHER: return TT_NC;
     case EP_MAHAJAN: case EP_MAHAJAN_FAIL: return MH_NC;
     case EP_LUORUDY: case EP_LUORUDYWITHGATE: return 1;
+    case EP_PURKINJE: return PK_NC;
     default: return EP_ERR_ARG;
     }
 }
@@ -683,6 +685,8 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
     const ep_model_desc *md = &models[0];
     const int nst = ep_model_nstate(md->model);
     EP_CHECK_ARG(nst > 0, "unknown cell model");
+    EP_CHECK_ARG(md->model != EP_PURKINJE,
+                 "the Purkinje cell runs at plugin level (ep_ionic_step) only; tissues of it are not built");
     EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32 ||
                      (sd->precision == EP_SURROGATE && md->model == EP_TUSSCHER),
                  "unsupported precision (EP_SURROGATE needs the ten Tusscher model)");

@@ -84,6 +84,13 @@ __device__ __forceinline__ void ionic_node(const IonicArgs<R> &a, const int i, u
             int sub = 0;
             dvdt = mh_compute_ion<R>(s, V, istim / (a.Cm * a.Xi), h, c, a.mh_abs, sub);
             my_newton += sub;
+        } else if constexpr (MODEL == EP_PURKINJE) {
+            // the stimulus in uA/cm^3 and the model's (or the user's) Xi;
+            // C_m does not enter (Purkinje.cc:183-213)
+            const R *__restrict__ c = a.consts + (size_t)ty * a.nconst;
+            int sub = 0;
+            dvdt = pk_compute_ion<R>(s, V, istim, a.Xi, h, c, sub);
+            my_newton += sub;
         } else {
             dvdt = lr_compute_ion<R>(s + 1, V, istim, a.Cm, h, a.lr_table);
         }
@@ -152,6 +159,9 @@ static void dispatch_ionic(int model, const IonicArgs<R> &a, int grid, int block
     case EP_MAHAJAN_FAIL:
         k_ionic<R, EP_MAHAJAN, MH_NS, MINB><<<grid, block, 0, st>>>(a);
         break;
+    case EP_PURKINJE:
+        k_ionic<R, EP_PURKINJE, PK_NS, MINB><<<grid, block, 0, st>>>(a);
+        break;
     default:
         k_ionic<R, EP_LUORUDY, LR_NS, 1><<<grid, block, 0, st>>>(a);
         break;
@@ -163,7 +173,7 @@ int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block, i
     if (block != 64 && block != 128) { set_error("ionic block must be 64 or 128"); return EP_ERR_ARG; }
     if (min_ctas != 0 && min_ctas != 3 && min_ctas != 4) { set_error("ionic min_ctas must be 0, 3 or 4"); return EP_ERR_ARG; }
     if (model != EP_TUSSCHER && model != EP_MAHAJAN && model != EP_MAHAJAN_FAIL && model != EP_LUORUDY &&
-        model != EP_LUORUDYWITHGATE) {
+        model != EP_LUORUDYWITHGATE && model != EP_PURKINJE) {
         set_error("unknown model %d", model);
         return EP_ERR_ARG;
     }

@@ -4,6 +4,7 @@
 #include "tt.cuh"
 #include "mahajan.cuh"
 #include "lr.cuh"
+#include "purkinje.cuh"
 
 namespace ep {
 
