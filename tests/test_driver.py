@@ -171,3 +171,27 @@ def test_schedule_matches_oracle_restatement():
         on, off = O.stim_schedule(t0, t1, 0.1, 300)
         assert sorted((s, i) for s, i, f in ev if f) == sorted((int(s), i) for i, s in enumerate(on) if s >= 0)
         assert sorted((s, i) for s, i, f in ev if not f) == sorted((int(s), i) for i, s in enumerate(off) if s >= 0)
+
+
+def test_output_files_round_trip(tmp_path):
+    """The reference's output formats: V as raw FP64, InterVariables as per
+    node (int nVar, nVar doubles) -- nVar may differ between nodes (tissue
+    model and Purkinje cells of a mixed tissue); truncation is an error."""
+    rng = np.random.default_rng(2)
+    assert IO.output_name(str(tmp_path), "Voltage", 12.5).endswith("Voltage_time_00012.50.00")
+    V = rng.normal(size=17)
+    V.tofile(IO.output_name(str(tmp_path), "Voltage", 1.0))
+    assert np.array_equal(IO.read_voltage(IO.output_name(str(tmp_path), "Voltage", 1.0)), V)
+    uni = rng.normal(size=(5, 19))
+    p = IO.output_name(str(tmp_path), "InterVariables", 1.0)
+    IO.write_intervariables(p, uni)
+    assert np.array_equal(IO.read_intervariables(p), uni)
+    mixed = [rng.normal(size=19), rng.normal(size=22), rng.normal(size=19)]
+    IO.write_intervariables(p, mixed)
+    got = IO.read_intervariables(p)
+    assert [len(v) for v in got] == [19, 22, 19] and all(np.array_equal(a, b) for a, b in zip(got, mixed))
+    with open(p, "r+b") as f:
+        f.truncate(4 + 8 * 19 + 4 + 8 * 10)
+    import pytest
+    with pytest.raises(ValueError):
+        IO.read_intervariables(p)
