@@ -11,7 +11,10 @@ Reference interface (paths inside wsklug/UCLA_CMG, voomEP/src/...):
 * ``EPSimulator`` main loop (Applications/CardiacEP/EPSimulator.cc:483-596).
 
 :class:`Monodomain` owns one device-resident tissue instance
-(``ep_create``); the method names of the reference are kept as aliases.
+(``ep_create``); the method names of the reference are kept as aliases.  The
+steps that ``setIonicTimeStep`` and ``setSolveTime`` set are constructor
+arguments here (``ionic_dt``, ``dt``): the CN operators are assembled for
+them once.
 """
 import ctypes as C
 
