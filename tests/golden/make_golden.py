@@ -10,6 +10,9 @@ their IonicModel::Compute_Ion interface.
                                                     # (names: tt mahajan ... purkinje; default all)
 
 Outputs (npz):
+  tissue_tt_slab.npz  the split step (the oracle's CN/PCG restatement) with the
+                    reference's TT objects as the cells: a 13x11x5-node slab,
+                    corner stimulus, V at t = 2, 5 and 10 ms (name "tissue")
   cell_<model>.npz  single-cell trajectory under the split update
                     V <- V + dt * Compute_Ion(V, istim) with a 1 ms stimulus:
                     t, V (every sample_every steps), final states
@@ -88,5 +91,34 @@ def main():
         print(NAME[model], "trajectory", Vs.shape, "kat", Vin.shape, "Vmax", Vs.max())
 
 
+def tissue():
+    """V fields of a small slab: reference TT cells, dt 0.01 ms (their Newton
+    layout needs dt <= 0.01), CN/PCG to 1e-12, stimulus 50 uA/cm^2 for 1 ms on
+    a 3x3 full-thickness corner block."""
+    from ucla_cmg_b200 import mesh as M
+    m = M.slab(13, 11, 5, 0.6, 0.5, 0.2)
+    D = M.sigma_to_D(1.2, 0.2)
+    dt = 0.01
+    blk = M.corner_block(m, 3, 3)
+    c = O.Csr(m.xyz, m.tets, m.fibers, D, 1.0, dt)
+    cells = O.RefCells(O.TUSSCHER, m.n)
+    s = O.Sim(c, cells, dt, dt, cg_tol=1e-12, cg_maxit=2000, jacobi_steps=1)
+    s.V[:] = -85.423
+    snaps, times = [], (2.0, 5.0, 10.0)
+    for k in range(int(round(times[-1] / dt))):
+        s.istim[:] = 0.0
+        if k * dt < 1.0:
+            s.istim[blk] = 50.0 * 2000.0
+        s.step(1)
+        if any(abs((k + 1) * dt - t) < 1e-9 for t in times):
+            snaps.append(s.V.copy())
+    np.savez_compressed(os.path.join(HERE, "tissue_tt_slab.npz"), t=np.array(times), V=np.array(snaps),
+                        dt=dt, nx=13, ny=11, nz=5, L=np.array([0.6, 0.5, 0.2]), stim_nodes=blk)
+    print("tissue", np.array(snaps).shape, "Vmax", np.max(snaps))
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["tissue"]:
+        tissue()
+    else:
+        main()

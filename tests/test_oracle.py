@@ -411,3 +411,28 @@ def test_purkinje_cable_drives_the_tissue():
     speed = 7 * 0.05 / (cable[0] - cable[7])                           # cm/ms
     assert 0.05 < speed < 0.5
     assert tact[0] > cable[0] and np.sum(tact[:n0] > 0) > 5
+
+
+def test_tissue_restatement_matches_the_reference_cells_golden():
+    """A 13x11x5 slab for 10 ms under the split step: the restated TT cells
+    reproduce the V fields made with the reference's own TT objects
+    (tests/golden/tissue_tt_slab.npz) at t = 2, 5 and 10 ms."""
+    g = np.load(os.path.join(GOLD, "tissue_tt_slab.npz"))
+    L = g["L"]
+    m = M.slab(int(g["nx"]), int(g["ny"]), int(g["nz"]), float(L[0]), float(L[1]), float(L[2]))
+    dt = float(g["dt"])
+    c = O.Csr(m.xyz, m.tets, m.fibers, M.sigma_to_D(1.2, 0.2), 1.0, dt)
+    s = O.Sim(c, O.Cells(O.TUSSCHER, m.n), dt, dt, cg_tol=1e-12, cg_maxit=2000, jacobi_steps=1)
+    s.V[:] = -85.423
+    blk = g["stim_nodes"]
+    out = []
+    for k in range(int(round(g["t"][-1] / dt))):
+        s.istim[:] = 0.0
+        if k * dt < 1.0:
+            s.istim[blk] = 50.0 * 2000.0
+        s.step(1)
+        if np.any(np.abs((k + 1) * dt - g["t"]) < 1e-9):
+            out.append(s.V.copy())
+    out = np.array(out)
+    assert np.max(g["V"]) > 0.0
+    assert np.max(np.abs(out - g["V"])) < 1e-6 * np.max(np.abs(g["V"]))
