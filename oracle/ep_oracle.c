@@ -1281,11 +1281,25 @@ void epo_spmv(const epo_csr *a, const double *vals, const double *x, double *y)
     }
 }
 
+/* sums of fixed blocks of 4096 entries, then the block sums in order: the
+ * same bits whatever the thread count (an OpenMP reduction combines thread
+ * partials in arrival order) */
 static double dotp(int n, const double *x, const double *y)
 {
+    enum { BLK = 4096 };
+    const int nb = (n + BLK - 1) / BLK;
+    double stackbuf[256];
+    double *part = nb <= 256 ? stackbuf : (double *)malloc(sizeof(double) * (size_t)nb);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; b++) {
+        const int lo = b * BLK, hi = lo + BLK < n ? lo + BLK : n;
+        double s = 0.0;
+        for (int i = lo; i < hi; i++) s += x[i] * y[i];
+        part[b] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for schedule(static) reduction(+:s)
-    for (int i = 0; i < n; i++) s += x[i] * y[i];
+    for (int b = 0; b < nb; b++) s += part[b];
+    if (part != stackbuf) free(part);
     return s;
 }
 

@@ -351,9 +351,7 @@ def test_mixed_populations_without_purkinje_nodes_equal_the_tissue_alone(small_s
                 s.istim[blk] = 50.0 * 2000.0
             s.step(1)
     assert np.max(sa.V) > 0.0
-    # the oracle's OpenMP dot products combine partial sums in thread order:
-    # equal to rounding, not bit for bit
-    assert np.max(np.abs(sa.V - sb.V)) < 1e-9 * np.max(np.abs(sa.V))
+    assert np.array_equal(sa.V, sb.V)
 
 
 def test_mixed_restatement_equals_the_reference_objects():
