@@ -5,7 +5,7 @@ Two libraries sit behind it:
 * ``libep_oracle.so`` -- the plain-C FP64 restatement of the voomEP
   monodomain path (``ep_oracle.c``);
 * ``_ref/libvoomep_ref.so`` -- the reference's own cell-model sources
-  (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR}.cc) compiled
+  (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR,Purkinje}.cc) compiled
   unmodified, used to pin the restatement and as the CPU reference arm.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may

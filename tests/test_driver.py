@@ -195,3 +195,63 @@ def test_output_files_round_trip(tmp_path):
     import pytest
     with pytest.raises(ValueError):
         IO.read_intervariables(p)
+
+
+def _mix_case(tmp_path, cell_model="Tusscher"):
+    """A slab with a 6-element Purkinje cable hanging from node 1, .purk
+    listing the cable nodes, a nodal stimulus at the cable's far end."""
+    m = M.slab(5, 4, 3, 0.4, 0.3, 0.2)
+    n0, k, h = m.n, 6, 0.05
+    extra = m.xyz[[0]] + np.stack([np.zeros(k), np.zeros(k), -h * np.arange(1, k + 1)], 1)
+    xyz = np.vstack([m.xyz, extra])
+    bars = [[0, n0]] + [[n0 + j, n0 + j + 1] for j in range(k - 1)]
+    base = tmp_path / "mix"
+    with open(str(base) + ".node", "w") as f:
+        f.write(f"{len(xyz)} 3 0 0\n")
+        for i, p in enumerate(xyz):
+            f.write(f"{i + 1} {p[0]:.17g} {p[1]:.17g} {p[2]:.17g}\n")
+    elems = [[4] + list(t + 1) for t in m.tets] + [[2, a + 1, b + 1] for a, b in bars]
+    with open(str(base) + ".ele", "w") as f:
+        f.write(f"{len(elems)} 0 0\n")
+        for e, el in enumerate(elems):
+            f.write(" ".join(str(v) for v in [e + 1] + el) + "\n")
+    (tmp_path / "mix.purk").write_text(f"{k}\n" + " ".join(str(n0 + j + 1) for j in range(k)) + "\n")
+    (tmp_path / "stim.txt").write_text(f"{n0 + k}\n{n0 + k - 1}\n")
+    (tmp_path / "case.input").write_text(f"""MODEL mix
+OutputDir out/
+CellModel {cell_model}
+DT 0.01
+IonicDT 0.01
+SimulationTime 6
+Frequency 1
+WriteRestart 3
+TissueDiffusion 1e-3 2e-4 2e-4
+Stimulus Nodal stim.txt 0 2 250000
+""")
+    return str(tmp_path / "case.input"), n0, k
+
+
+def test_oracle_driver_runs_a_mixed_case(tmp_path):
+    """The oracle's EPSimulator loop on a MIX3D case: output frames at t = 0
+    and every ms, restart files at 3 and 6 ms with 19 states on tissue nodes
+    and 22 on Purkinje nodes, the cable fires from its stimulated end; the
+    reference's own cell objects and the restatement give the same fields."""
+    from oracle import oracle as O
+    if O.ref_lib() is None:
+        import pytest
+        pytest.skip("oracle/_ref not built")
+    from oracle import driver_oracle as DO
+    inp, n0, k = _mix_case(tmp_path)
+    out_ref, out_port = str(tmp_path / "ref"), str(tmp_path / "port")
+    cfg, nsteps, is_purk = DO.run(inp, out_ref, reference_cells=True, rest_voltage=True)
+    DO.run(inp, out_port, reference_cells=False, rest_voltage=True)
+    assert nsteps == 601 and int(is_purk.sum()) == k             # simtime += dt accumulates one more step
+    frames = [IO.read_voltage(IO.output_name(out_ref, "Voltage", t)) for t in (0.0, 1.0, 2.0, 3.0)]
+    assert all(len(f) == n0 + k for f in frames)
+    assert max(f[n0:].max() for f in frames) > 0.0               # the cable fired
+    st = IO.read_intervariables(IO.output_name(out_ref, "InterVariables", 3.0))
+    assert [len(v) for v in st[:n0]] == [19] * n0 and [len(v) for v in st[n0:]] == [22] * k
+    for t in (1.0, 2.0, 3.0):
+        a = IO.read_voltage(IO.output_name(out_ref, "Voltage", t))
+        b = IO.read_voltage(IO.output_name(out_port, "Voltage", t))
+        assert np.max(np.abs(a - b)) < 1e-6 * np.max(np.abs(a))
