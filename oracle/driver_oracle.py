@@ -82,11 +82,25 @@ def run(input_file, out_dir=None, reference_cells=True, rest_voltage=False, cg_t
         V[pk_nodes] = pk.state[:, 0]
     out = out_dir or os.path.join(base, cfg["output_dir"])
     os.makedirs(out, exist_ok=True)
-    times, t = [], 0.0
+    # READRESTART: V and the cell states from the restart files, the loop
+    # starting at simtime = t, count = long(t/dt) (EPSimulator.cc:495-500,
+    # EPSolver::readRestart, EPSolver.cc:179-211)
+    simtime, count = 0.0, 0
+    if cfg["read_restart"] is not None:
+        simtime = cfg["read_restart"]
+        count = int(simtime / dt)
+        V[:] = IO.read_voltage(IO.output_name(out, "Voltage", simtime))
+        rows = IO.read_intervariables(IO.output_name(out, "InterVariables", simtime))
+        if len(rows) != n:
+            raise ValueError(f"restart file has {len(rows)} nodes, the mesh {n}")
+        _set_states(tissue, [rows[i] for i in tis_nodes])
+        if pk is not None:
+            _set_states(pk, [rows[i] for i in pk_nodes])
+    times, t = [], simtime
     while t < cfg["simulation_time"]:
         t += dt
         times.append(t)
-    nsteps = len(times)
+    nsteps = count + len(times)
     ids, on, off, amp = D.stimulus_windows(cfg["stimuli"], dt, nsteps, mesh.xyz, purk, base)
     steps_per_frame = int(cfg["frequency"] / dt)
     restart_every = int(cfg["write_restart"] / dt)
@@ -100,13 +114,26 @@ def run(input_file, out_dir=None, reference_cells=True, rest_voltage=False, cg_t
                 rows[i] = pk.state[k]
         IO.write_intervariables(IO.output_name(out, "InterVariables", tt), rows)
 
-    np.asarray(sim.V, dtype=np.float64).tofile(IO.output_name(out, "Voltage", 0.0))
-    for k in range(nsteps):
+    if cfg["read_restart"] is None:
+        np.asarray(sim.V, dtype=np.float64).tofile(IO.output_name(out, "Voltage", 0.0))
+    for k in range(count, nsteps):
         sim.istim[:] = _istim_at(k, n, ids, on, off, amp)
         sim.step(1)
         c = k + 1
+        tk = times[k - count]
         if c % steps_per_frame == 0:
-            np.asarray(sim.V, dtype=np.float64).tofile(IO.output_name(out, "Voltage", times[k]))
+            np.asarray(sim.V, dtype=np.float64).tofile(IO.output_name(out, "Voltage", tk))
         if restart_every > 0 and c % restart_every == 0:
-            write_states(times[k])
+            write_states(tk)
     return cfg, nsteps, is_purk
+
+
+def _set_states(cells, rows):
+    """Per-node state rows into a population (restatement or reference objects)."""
+    a = np.array(rows, dtype=np.float64).reshape(len(rows), -1)
+    if a.shape[1] != cells.nstate:
+        raise ValueError(f"restart rows have {a.shape[1]} values, the cell model {cells.nstate}")
+    if isinstance(cells, O.RefCells):
+        cells.state = a
+    else:
+        cells.state[:] = a

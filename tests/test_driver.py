@@ -1,5 +1,6 @@
 """The EPSimulator-compatible driver: input parsing, the reference's
 stimulus schedule and region types, and the mesh file formats (CPU)."""
+import os
 import numpy as np
 
 from ucla_cmg_b200 import capi, mesh as M
@@ -76,6 +77,34 @@ def test_stimulus_regions_and_windows():
     w = set(zip(ids.tolist(), on.tolist(), off.tolist(), amp.tolist()))
     assert w == {(0, 0, 2, 7.0), (1, 0, 2, 7.0), (0, 4, 6, 3.0), (1, 4, 6, 3.0), (2, 4, 6, 3.0),
                  (3, 8, 10, 5.0)}
+
+
+def test_zonal_stop_falls_through_to_plane_stop():
+    """The reference's ZONAL stop has no ``break`` and also runs the PLANE
+    stop with current 0 (EPSimulator.cc:557-563, CardiacBody.cc:265-287): a
+    NODAL stimulus still running elsewhere is switched off with it, Purkinje
+    nodes excepted.  Default = the reference; opt-out = the ``break``."""
+    xyz = np.array([[0.0, 0, 0], [0.05, 0, 0], [0.2, 0, 0], [0.5, 0, 0]])
+    zonal = dict(type=2, axis=0, limit=0.1, i_stim=3.0, t_start=0.0, t_stop=1.0)
+    istim = np.array([3.0, 3.0, 8.0, 8.0])                 # nodes 3, 4 (1-based) under another stimulus
+    a = istim.copy()
+    D.apply_region(a, zonal, False, xyz, np.array([4]), ".")
+    assert list(a) == [0.0, 0.0, 0.0, 8.0]                 # node 4 is a Purkinje node
+    b = istim.copy()
+    D.apply_region(b, zonal, False, xyz, np.array([4]), ".", zonal_fallthrough=False)
+    assert list(b) == [0.0, 0.0, 8.0, 8.0]
+    # in a schedule (dt 0.5): a zonal stimulus 0.0-1.0, then a plane one
+    # 0.5-5.0 over the nodes x > 0.3; the zonal stop at step 2 also ends the
+    # plane window there
+    zonal = dict(type=2, axis=0, limit=0.1, i_stim=3.0, t_start=0.0, t_stop=1.0)
+    plane = dict(type=3, center=[0.3, 0, 0], normal=[-1.0, 0, 0], i_stim=5.0, t_start=0.5, t_stop=5.0)
+    assert D.stimulus_events([zonal, plane], 0.5, 20) == [(0, 0, True), (1, 1, True), (2, 0, False),
+                                                         (10, 1, False)]
+    w = set(zip(*[x.tolist() for x in D.stimulus_windows([zonal, plane], 0.5, 20, xyz, None, ".")]))
+    assert w == {(0, 0, 1, 3.0), (1, 0, 1, 3.0), (3, 1, 2, 5.0)}
+    w = set(zip(*[x.tolist() for x in D.stimulus_windows([zonal, plane], 0.5, 20, xyz, None, ".",
+                                                         zonal_fallthrough=False)]))
+    assert (3, 1, 10, 5.0) in w
 
 
 def test_mesh_files_round_trip(tmp_path):
@@ -255,3 +284,28 @@ def test_oracle_driver_runs_a_mixed_case(tmp_path):
         a = IO.read_voltage(IO.output_name(out_ref, "Voltage", t))
         b = IO.read_voltage(IO.output_name(out_port, "Voltage", t))
         assert np.max(np.abs(a - b)) < 1e-6 * np.max(np.abs(a))
+
+
+def test_oracle_driver_read_restart(tmp_path):
+    """READRESTART in the oracle's loop: V and the per-node states (19 and
+    22 values) come from the restart files, the loop starts at simtime = t,
+    count = long(t/dt), and the frames after it equal those of the run that
+    never stopped."""
+    import shutil
+    from oracle import driver_oracle as DO
+    inp, n0, k = _mix_case(tmp_path)
+    full, cont = str(tmp_path / "full"), str(tmp_path / "cont")
+    DO.run(inp, full, reference_cells=False, rest_voltage=True)
+    os.makedirs(cont)
+    for kind in ("Voltage", "InterVariables"):
+        shutil.copy(IO.output_name(full, kind, 3.0), IO.output_name(cont, kind, 3.0))
+    txt = open(inp).read() + "ReadRestart 3\n"
+    inp2 = str(tmp_path / "restart.input")
+    open(inp2, "w").write(txt)
+    cfg, nsteps, _ = DO.run(inp2, cont, reference_cells=False, rest_voltage=True)
+    assert cfg["read_restart"] == 3.0 and nsteps == 601
+    assert not os.path.exists(IO.output_name(cont, "Voltage", 0.0))
+    for t in (4.0, 5.0, 6.0):
+        a = IO.read_voltage(IO.output_name(full, "Voltage", t))
+        b = IO.read_voltage(IO.output_name(cont, "Voltage", t))
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a))

@@ -43,10 +43,14 @@ reference, the LV cables get PURKINJEDIFFUSION, not LVPURKINJEDIFFUSION
 not yet run on the GPU: the driver reports them and runs the tets.
 
 Not on this path (accepted and ignored, with a note): the mechanics keys,
-QUADORDER other than 2, CONSISTENCYCHECK.  The ZONAL stop of
-the reference also runs the PLANE stop with the start pointer's plane (a
-missing ``break``, EPSimulator.cc:557-563); that side effect is not
-reproduced.
+QUADORDER other than 2, CONSISTENCYCHECK.
+
+The ZONAL stop of the reference falls through into the PLANE stop (a missing
+``break``, EPSimulator.cc:557-563), which calls the plane overload of
+setStimulusCurrent with its default current 0 (CardiacBody.cc:265-287): every
+non-Purkinje node is switched off, whatever the plane.  That is reproduced by
+default (``zonal_fallthrough=True``); ``--no-zonal-fallthrough`` switches off
+only the ZONAL region, as the ``break`` would.
 """
 import argparse
 import os
@@ -166,9 +170,12 @@ def stimulus_events(stimuli, dt, nsteps):
     return ev
 
 
-def apply_region(istim, st, on, xyz, purkinje, base_dir):
+def apply_region(istim, st, on, xyz, purkinje, base_dir, zonal_fallthrough=True):
     """CardiacBody::setStimulusCurrent for one stimulus (CardiacBody.cc:
-    243-324), in place on the per-node current array."""
+    243-324), in place on the per-node current array.  A ZONAL stop with
+    ``zonal_fallthrough`` also runs the PLANE stop the reference falls
+    through to (EPSimulator.cc:557-563): current 0 on every non-Purkinje
+    node."""
     amp = st["i_stim"] if on else 0.0
     n = len(istim)
     t = st["type"]
@@ -184,6 +191,8 @@ def apply_region(istim, st, on, xyz, purkinje, base_dir):
         istim[not_purk] = np.where(inside[not_purk], amp, 0.0)
     elif t == 2:
         istim[xyz[:, st["axis"]] <= st["limit"]] = amp
+        if not on and zonal_fallthrough:
+            istim[not_purk] = 0.0
     else:
         nrm = np.asarray(st["normal"], dtype=np.float64)
         nrm = nrm / np.linalg.norm(nrm)
@@ -191,7 +200,7 @@ def apply_region(istim, st, on, xyz, purkinje, base_dir):
         istim[not_purk] = np.where(below[not_purk], amp, 0.0)
 
 
-def stimulus_windows(stimuli, dt, nsteps, xyz, purkinje, base_dir):
+def stimulus_windows(stimuli, dt, nsteps, xyz, purkinje, base_dir, zonal_fallthrough=True):
     """Per-node windows (node, first step, end step, amplitude) equivalent to
     the reference's schedule over nsteps steps."""
     n = len(xyz)
@@ -202,7 +211,7 @@ def stimulus_windows(stimuli, dt, nsteps, xyz, purkinje, base_dir):
     for step, k, on in events + [(nsteps, None, None)]:
         new = istim.copy()
         if k is not None:
-            apply_region(new, stimuli[k], on, xyz, purkinje, base_dir)
+            apply_region(new, stimuli[k], on, xyz, purkinje, base_dir, zonal_fallthrough)
         changed = np.where(new != istim)[0]
         ended = changed[istim[changed] != 0.0]
         if k is None:
@@ -251,7 +260,7 @@ def cable_setup(cfg, node_type):
 
 
 def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate_path=None, verbose=True,
-        tt_jacobian=capi.TT_JAC_TRUE):
+        tt_jacobian=capi.TT_JAC_TRUE, zonal_fallthrough=True):
     cfg = parse_input(input_file)
     base_dir = cfg["input_dir"]
     model = CELL_MODELS[cfg["cell_model"].upper()]
@@ -298,7 +307,7 @@ def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate
         t += dt
         times.append(t)
     nsteps = count + len(times)
-    ids, on, off, amp = stimulus_windows(cfg["stimuli"], dt, nsteps, mesh.xyz, purk, base_dir)
+    ids, on, off, amp = stimulus_windows(cfg["stimuli"], dt, nsteps, mesh.xyz, purk, base_dir, zonal_fallthrough)
     # windows as times that round back to the same step under long(t/dt)
     g.set_stimulus(ids, (on + 0.5) * dt, (off + 0.5) * dt, amp)
     if cfg["read_restart"] is not None:
@@ -338,10 +347,14 @@ def main():
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--tt-reference-jacobian", action="store_true",
                     help="ten Tusscher Newton with the reference's transposed Jacobian (diverges at dt >= 0.02 ms)")
+    ap.add_argument("--no-zonal-fallthrough", action="store_true",
+                    help="a ZONAL stop switches off its own region only (the reference also switches "
+                         "off every other non-Purkinje node, EPSimulator.cc:557-563)")
     a = ap.parse_args()
     prec = {"fp64": capi.FP64, "fp32": capi.FP32, "surrogate": capi.SURROGATE}[a.precision]
     cfg, nsteps = run(a.input, prec, a.rest_voltage, a.device,
-                      tt_jacobian=capi.TT_JAC_REFERENCE if a.tt_reference_jacobian else capi.TT_JAC_TRUE)
+                      tt_jacobian=capi.TT_JAC_REFERENCE if a.tt_reference_jacobian else capi.TT_JAC_TRUE,
+                      zonal_fallthrough=not a.no_zonal_fallthrough)
     print(f"** {nsteps} steps done; output in {cfg['output_dir']}")
 
 
