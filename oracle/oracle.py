@@ -8,6 +8,12 @@ Two libraries sit behind it:
   (voomEP/src/IonicModel/{Tusscher,Mahajan,Mahajan_fail,LR,Purkinje}.cc) compiled
   unmodified, used to pin the restatement and as the CPU reference arm.
 
+* ``_ref/libvoomep_fem.so`` -- the reference's own mesh reader
+  (voomEP/src/Mesh/Mesh.cc), tet and cable geometry (TetMesh.cc,
+  MixedMesh3D.cc), element assembly (Body/CardiacBody.cc) and pseudo-ECG
+  (Applications/CardiacEP/ComputeECG.h), compiled unmodified against
+  stand-in headers; it pins the restatement's operators and ECG.
+
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
 import this module; the product package never does.
 """
@@ -151,6 +157,160 @@ def ref_lib():
         L.epo_set_threads.argtypes = [C.c_int]
         _REF = L
     return _REF
+
+
+_FEM = None
+
+
+def ref_fem_lib():
+    """The reference's FEM sources compiled unmodified (None if not built)."""
+    global _FEM
+    if _FEM is None:
+        path = os.path.join(HERE, "_ref", "libvoomep_fem.so")
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.fem_mesh_new.restype = C.c_void_p
+        L.fem_mesh_new.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_double]
+        L.fem_mesh_compute.argtypes = [C.c_void_p]
+        L.fem_mesh_free.argtypes = [C.c_void_p]
+        for f in ("fem_mesh_num_points", "fem_mesh_num_elements", "fem_mesh_num_local_nodes"):
+            getattr(L, f).argtypes = [C.c_void_p]
+        L.fem_mesh_points.argtypes = [C.c_void_p, ip, dp, dp, dp]
+        L.fem_body_new.restype = C.c_void_p
+        L.fem_body_new.argtypes = [C.c_void_p, C.c_int, dp, C.c_double, dp, dp]
+        L.fem_body_free.argtypes = [C.c_void_p]
+        L.fem_body_diffusion.restype = C.c_long
+        L.fem_body_diffusion.argtypes = [C.c_void_p, C.c_double, ip, ip, dp]
+        L.fem_body_capacitance.restype = C.c_long
+        L.fem_body_capacitance.argtypes = [C.c_void_p, C.c_int, ip, ip, dp]
+        L.fem_body_lumped.argtypes = [C.c_void_p, dp]
+        L.fem_ecg.argtypes = [C.c_void_p, dp, C.c_int, dp, dp, dp]
+        _FEM = L
+    return _FEM
+
+
+def write_reference_case(base, xyz, elements, fibers=None, purk=None, cell=None, angle=None):
+    """Mesh files as the reference's Mesh::New reads them (Mesh.cc:142-483):
+    <base>.node (``n 3 0 0``, then ``id x y z``), <base>.ele (``m 0 0``, then
+    ``id k n1..nk``, 1-based), <base>.fibers (9 numbers per element), the
+    one-rank partition files <base>.metis.npart.1 / .metis.epart.1 (read
+    even for one rank), and optionally .purk, .cell and .angle.
+    ``elements``: list of zero-based node-id sequences (4 for a tet, 2 for a
+    cable); ``purk``: zero-based node ids; ``cell``: per-node type;
+    ``angle``: {zero-based node: (dx, dy, dz, length)}."""
+    n = len(xyz)
+    with open(base + ".node", "w") as f:
+        f.write(f"{n} 3 0 0\n")
+        for i, p in enumerate(xyz):
+            f.write(f"{i + 1} {p[0]:.17g} {p[1]:.17g} {p[2]:.17g}\n")
+    with open(base + ".ele", "w") as f:
+        f.write(f"{len(elements)} 0 0\n")
+        for e, el in enumerate(elements):
+            f.write(" ".join(str(v) for v in [e + 1, len(el)] + [int(x) + 1 for x in el]) + "\n")
+    if fibers is not None:
+        np.savetxt(base + ".fibers", np.asarray(fibers).reshape(len(elements), 9), fmt="%.17g")
+    with open(base + ".metis.npart.1", "w") as f:
+        f.write("0\n" * n)
+    with open(base + ".metis.epart.1", "w") as f:
+        f.write("0\n" * len(elements))
+    if purk is not None:
+        with open(base + ".purk", "w") as f:
+            f.write(f"{len(purk)}\n" + "\n".join(str(int(i) + 1) for i in purk) + "\n")
+    if cell is not None:
+        with open(base + ".cell", "w") as f:
+            for i, t in enumerate(cell):
+                f.write(f"{i + 1} {int(t)}\n")
+    if angle:
+        with open(base + ".angle", "w") as f:
+            for k, v in sorted(angle.items()):
+                f.write(f"{k + 1} {v[0]:.17g} {v[1]:.17g} {v[2]:.17g} {v[3]:.17g}\n")
+
+
+class RefFemMesh:
+    """Mesh::New + setRadius of the reference on files written by
+    :func:`write_reference_case` (one rank).  ``compute=True`` runs
+    Mesh::Compute at once, as ComputeECG does; a mesh handed to
+    :class:`RefFemBody` is computed by the CardiacBody constructor instead."""
+
+    def __init__(self, base, quad_order=2, mixed=False, radius=0.0275, compute=False):
+        L = ref_fem_lib()
+        if L is None:
+            raise RuntimeError("oracle/_ref/libvoomep_fem.so is not built")
+        self.h = L.fem_mesh_new(base.encode(), int(quad_order), int(bool(mixed)), float(radius))
+        self.n = L.fem_mesh_num_local_nodes(self.h)
+        self.n_elements = L.fem_mesh_num_elements(self.h)
+        if compute:
+            L.fem_mesh_compute(self.h)
+
+    def points(self):
+        """Per quadrature point: node count k, N[4], dN/dx[4, 3], w*J."""
+        L = ref_fem_lib()
+        q = L.fem_mesh_num_points(self.h)
+        k = np.zeros(q, np.int32)
+        N = np.zeros((q, 4))
+        dN = np.zeros((q, 4, 3))
+        w = np.zeros(q)
+        L.fem_mesh_points(self.h, _p(k, ip), _p(N), _p(dN), _p(w))
+        return k, N, dN, w
+
+    def ecg(self, D, electrodes, V):
+        """ComputeECG.h's chain for the nodal voltage V (global order)."""
+        el = np.ascontiguousarray(electrodes, dtype=np.float64).reshape(-1, 3)
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        out = np.zeros(len(el))
+        ref_fem_lib().fem_ecg(self.h, _p(D), len(el), _p(el), _p(V), _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            ref_fem_lib().fem_mesh_free(self.h)
+        except Exception:
+            pass
+
+
+class RefFemBody:
+    """CardiacBody::New(mesh, model) + Compute of the reference; matrices as
+    scipy CSR (the inserted triplets summed)."""
+
+    def __init__(self, mesh, model, D, Cm=1.0, Dp=None, DpLeft=None):
+        L = ref_fem_lib()
+        self.mesh = mesh
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        Dp = None if Dp is None else np.ascontiguousarray(Dp, dtype=np.float64)
+        DpL = None if DpLeft is None else np.ascontiguousarray(DpLeft, dtype=np.float64)
+        self.h = L.fem_body_new(mesh.h, int(model), _p(D), float(Cm), _p(Dp), _p(DpL))
+
+    def _triplets(self, fn, arg):
+        import scipy.sparse as sp
+        L = ref_fem_lib()
+        m = getattr(L, fn)(self.h, arg, None, None, None)
+        r = np.zeros(m, np.int32)
+        c = np.zeros(m, np.int32)
+        v = np.zeros(m)
+        getattr(L, fn)(self.h, arg, _p(r, ip), _p(c, ip), _p(v))
+        n = self.mesh.n
+        return sp.coo_matrix((v, (r, c)), shape=(n, n)).tocsr()
+
+    def diffusion(self, scale=1.0):
+        """getDiffusionMatrix(M, scale): scale x K (K includes C_m)."""
+        return self._triplets("fem_body_diffusion", float(scale))
+
+    def capacitance(self, is_cap=True):
+        """getCapacitanceMatrix(M, isCap): C_m M (or M)."""
+        return self._triplets("fem_body_capacitance", int(bool(is_cap)))
+
+    def lumped(self):
+        out = np.zeros(self.mesh.n)
+        ref_fem_lib().fem_body_lumped(self.h, _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            ref_fem_lib().fem_body_free(self.h)
+        except Exception:
+            pass
 
 
 def set_threads(n):
