@@ -2,30 +2,49 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
                     [--form surrogate|plain_fp32|fp64] [--impl ours|reference]
-                    [--workload shell_c2|slab_c0|slab_c1|batch_c3] [--t-start MS]
-                    [--no-tune] [--no-compare] [--no-cpu] [--accuracy MS]
+                    [--workload shell_c2|slab_c0|slab_c1|batch_c3]
+                    [--no-tune] [--no-run] [--no-cpu] [--accuracy MS]
 
 One step = one global dt (0.1 ms) of EP_CrankNicholson::Solve over the whole
 shell: half diffusion step (SpMV + Jacobi-PCG to 1e-7), the ionic phase (ten
-Tusscher, endo/M/epi, PMJ stimuli; by default the learned form, with the
-plain FP32 form timed over the same window for the ratio), half diffusion
-step, and the pseudo-ECG every 10 steps.  The timed window starts at
---t-start (40 ms) after an untimed advance, and each form's launch shape is
-picked by the autotuner first.  Inputs (the operators and all cell states)
-are resident in HBM; they total > 126 MB, so no L2 flush is needed between
-steps.  Multi-GPU: independent replicas (the path does not shard), weak
-scaling, timing = max over ranks of the device (CUDA-event) time.
+Tusscher, endo/M/epi, PMJ stimuli), half diffusion step, and the pseudo-ECG
+every 10 steps.
 
---accuracy MS runs the workload that long in FP64, FP32 and the learned form
-in lockstep and prints the errors against FP64 instead of timing.
+What one default run prints (one JSON line):
 
---impl reference times the reference's own CPU implementation on the host
-cores: the reference cell-model sources compiled unmodified (oracle/_ref)
-inside the C restatement of the CN/PCG split step, on a bounded sample of the
-same workload (a coarser shell), all host threads.
+* ``value`` -- the learned form (surrogate) over the common window: W
+  untimed warm-up steps from t = 0, then exactly K timed steps.  The
+  reference arm (``--impl reference``) times the same K steps after the same
+  W warm-up steps of the same 2,004,051-node shell on the host cores, so the
+  two arms share one ``config``.
+* ``forms`` -- the plain FP32 form over the same window, and the ratio.
+* ``run_500ms`` -- the metric's whole run: the shell for 500 ms in the
+  FP64, plain FP32 and learned forms in lockstep, every step timed on the
+  device; node-steps/s of each form, the learned/plain FP32 ratio
+  (``speedup_vs_plain_fp32``, also at the top level), and the errors of the
+  FP32 and learned forms against FP64 (activation time, APD90, Vm L-inf,
+  pseudo-ECG relative L2), with a per-50-ms throughput profile.
+* ``roofline`` (the dominant kernel, from per-kernel CUDA events over the
+  timed window), ``e2e`` (the same window through the public API with host
+  buffers), ``cpu_baseline`` (the CPU port on the same shell, a 2-step
+  sample), ``clocks``.
+
+Inputs are resident in HBM and exceed the L2 (operators + states >= 0.5 GB),
+so no flush is needed.  Multi-GPU: independent replicas (the path does not
+shard), weak scaling, timing = max over ranks of the device time; the
+whole 500-ms run and the CPU sample run at N = 1 only.
+
+--accuracy MS runs --workload that long in FP64, FP32 (and, for the shell,
+the learned form) in lockstep and prints the errors against FP64.
+
+--impl reference times the CPU implementation on all host cores: the C
+restatement of the reference's split step (oracle/) with the same cell
+set-up as the GPU arm (endo/M/epi, G_Ks scale, the true-Jacobian Newton),
+never loading this project's GPU library.
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -67,10 +86,38 @@ def _env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+
+def shared_config(name, n, m, dt, ionic_dt, warmup, steps):
+    """The workload and the timed window, identical in both arms."""
+    return {"workload": WORKLOAD_TEXT[name].format(n=n, m=m), "dt_ms": dt, "ionic_dt_ms": ionic_dt,
+            "window": f"{warmup} untimed warm-up steps from t = 0, then {steps} timed steps "
+                      f"(t = {warmup * dt:.2f}-{(warmup + steps) * dt:.2f} ms)",
+            "l2": "inputs > L2 (operators + cell states >= 0.5 GB), no flush"}
+
+
+def _finite(x):
+    """JSON has no NaN/inf: map them to None."""
+    if isinstance(x, float) and not math.isfinite(x):
+        return None
+    if isinstance(x, dict):
+        return {k: _finite(v) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_finite(v) for v in x]
+    return x
+
+
+class Clocks:
+    """nvidia-smi sampler; reports the median SM clock over the samples taken
+    while the GPU was busy (utilization >= 50 %) and every throttle reason
+    seen in them."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -79,7 +126,7 @@ class Clocks:
         self.lines = []
         self.p = None
 
-    def start(self):
+    def start(self, wait_first=True):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -88,6 +135,10 @@ class Clocks:
             self.t.start()
         except Exception:
             self.p = None
+            return
+        t0 = time.time()
+        while wait_first and not self.lines and time.time() - t0 < 3.0:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.p.stdout:
@@ -102,23 +153,30 @@ class Clocks:
         except Exception:
             self.p.kill()
         self.t.join(timeout=2)
-        sm, smax, reasons = [], None, set()
+        return self.summary(self.lines)
+
+    @staticmethod
+    def summary(lines):
+        import statistics
+        sm, busy, smax, reasons = [], [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
+                mhz, smax, util = float(f[1]), float(f[2]), float(f[4])
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        import statistics
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+            sm.append(mhz)
+            if util >= 50.0:
+                busy.append(mhz)
+                for nm, v in zip(names, f[6:10]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        use = busy or sm
+        return {"sm_mhz": statistics.median(use) if use else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm), "samples_under_load": len(busy)}
 
 
 def cpu_model():
@@ -201,59 +259,201 @@ def node_step_bytes(n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=10, ecg_ev
     return tot / n
 
 
-def cpu_sample(kind, h, steps, threads):
-    """Time the CPU path on a coarser shell (same model, dt, stimuli).
-    kind 'reference': the reference cell objects (oracle/_ref) in the C
-    restatement of the CN split step with AztecOO's 3-step Jacobi;
-    kind 'port': the C restatement throughout."""
+# --------------------------------------------------------------------------
+# CPU side (the oracle; never the GPU library)
+# --------------------------------------------------------------------------
+
+def cpu_sim(wl, kind="port"):
+    """The CPU split step on the workload's mesh: the C restatement of
+    EP_CrankNicholson::Solve with AztecOO's 3-step Jacobi PCG, and as cells
+    either the restatement with the GPU arm's set-up (kind 'port': endo/M/epi
+    sets, the G_Ks scale, the true-Jacobian Newton capped at 100) or the
+    reference's own cell objects compiled from its sources (kind 'reference':
+    epicardial constants everywhere, the reference's transposed-Jacobian
+    Newton -- the only set-up those objects have)."""
     from oracle import oracle as O
-    from ucla_cmg_b200 import workloads as W
-    O.set_threads(threads)
-    wl = W.shell_c2(h=h)
     m = wl.mesh
     csr = O.Csr(m.xyz, m.tets, m.fibers, wl.D, 1.0, wl.dt)
-    if kind == "reference" and O.ref_lib() is not None:
-        cells = O.RefCells(O.TUSSCHER, m.n)        # the reference has the epicardial set only
+    if kind == "reference":
+        cells = O.RefCells(O.TUSSCHER, m.n)
     else:
-        kind = "port"
         cells = O.Cells(O.TUSSCHER, m.n, types=wl.node_type, type_consts=wl.type_consts,
                         gks_scale=wl.gks_scale, tt_jac_true=1, newton_cap=100)
     sim = O.Sim(csr, cells, wl.dt, wl.ionic_dt, cg_tol=1e-7, cg_maxit=1000, jacobi_steps=3)
     sim.V[:] = wl.V0
+    return sim, (csr, cells)
+
+
+def cpu_steps(sim, wl, k0, k1):
+    """Steps k0..k1-1 with the stimulus windows [long(t_on/dt), long(t_off/dt));
+    wall time of each step."""
     on = (wl.stim_on / wl.dt).astype(int)
     off = (wl.stim_off / wl.dt).astype(int)
     times = []
-    for k in range(steps):
+    for k in range(k0, k1):
         sim.istim[:] = 0.0
         act = (on <= k) & (k < off)
         sim.istim[wl.stim_ids[act]] = wl.stim_amp[act]
         t0 = time.perf_counter()
         sim.step()
         times.append(time.perf_counter() - t0)
-    return m.n, times, kind
+    return times
 
 
 def run_reference(args, rank, world):
+    """The CPU arm: rank 0 alone (the other ranks exit without work)."""
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    h = float(os.environ.get("EP_REF_SAMPLE_H", "0.2"))
-    n, times, kind = cpu_sample("reference", h, args.warmup + args.steps, threads)
+    from oracle import oracle as O
+    from ucla_cmg_b200 import workloads as W
+    threads = host_threads()
+    O.set_threads(threads)
+    wl = W.shell_c2(epi=O.tt_constants())          # constants from the oracle, not the GPU library
+    n = wl.mesh.n
+    sim, keep = cpu_sim(wl, "port")
+    times = cpu_steps(sim, wl, 0, args.warmup + args.steps)
     timed = times[args.warmup:]
     tot = sum(timed)
     v = n * len(timed) / tot
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(timed), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"shell_c2 sample: truncated ellipsoid shell h={h} cm ({n} nodes), "
-                                   "ten Tusscher, dt 0.1 / ionic 0.02 ms, 200 PMJ stimuli",
-                       "form": "reference CPU (FP64)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{len(timed)} steps of a {n}-node shell (h={h} cm) from t=0",
+            "impl": "reference", "form": "CPU split step (FP64)",
+            "config": shared_config("shell_c2", n, wl.mesh.m, wl.dt, wl.ionic_dt, args.warmup, args.steps),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"the whole {n}-node shell, steps {args.warmup}..{args.warmup + args.steps - 1} "
+                                       f"from t = 0 after {args.warmup} untimed steps, same cell set-up as the GPU arm",
+                             "why_port": "the reference's cell objects carry the epicardial constants only and "
+                                         "their transposed-Jacobian Newton diverges at ionic dt 0.02 ms in tissue; "
+                                         "the port runs the GPU arm's endo/M/epi set-up with the true Jacobian",
                              "cpu": cpu_model()},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    del sim, keep
+    if not getattr(args, "no_ref_objects", False):
+        # the reference's own cell objects on the same mesh and the same
+        # first step, for scale (epicardial everywhere: their only set-up)
+        rs, rkeep = cpu_sim(wl, "reference")
+        t1 = cpu_steps(rs, wl, 0, 1)
+        line["cpu_baseline"]["reference_objects"] = {
+            "value": n / t1[0], "unit": UNIT, "cores": threads,
+            "sample": "step 0 of the same shell with the reference's unmodified cell objects "
+                      "(oracle/_ref), epicardial constants everywhere"}
+        del rs, rkeep
+    print(json.dumps(_finite(line)), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU side
+# --------------------------------------------------------------------------
+
+def _deploy(h, prec):
+    from ucla_cmg_b200 import capi
+    if prec == capi.SURROGATE:
+        from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
+        Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(h)
+    return h
+
+
+def whole_run(wl, forms, shapes, local, T=None, bin_ms=50.0, tune=True):
+    """The workload for T ms in the given forms, in lockstep: every step
+    timed on the device (the handle's CUDA events), Vm compared with the
+    first form (FP64) every 1 ms; at the end activation time, APD90 and the
+    pseudo-ECG against it."""
+    import numpy as np
+    T = wl.T if T is None else T
+    steps = int(round(T / wl.dt))
+    per_ms = max(1, int(round(1.0 / wl.dt)))
+    nbin = max(1, int(math.ceil(T / bin_ms)))
+    hs = {}
+    for name, prec in forms:
+        h = _deploy(wl.create(prec, device=local), prec)
+        if name in shapes and shapes[name]:
+            h.set_launch_config(**shapes[name])
+        elif tune:
+            shapes[name] = h.autotune(20)[0]          # the state is put back afterwards
+        h.set_profiling(False)
+        hs[name] = h
+    ref = forms[0][0]
+    res = {name: dict(ms=0.0, fb=0, cg=0, vinf=0.0, bins=[0.0] * nbin) for name, _ in forms}
+    for k in range(0, steps, per_ms):
+        kk = min(per_ms, steps - k)
+        b = min(nbin - 1, int(k * wl.dt / bin_ms))
+        V = {}
+        for name, _ in forms:
+            st = hs[name].step(kk)
+            r = res[name]
+            r["ms"] += st["device_ms"]
+            r["bins"][b] += st["device_ms"]
+            r["fb"] += st["fallback_nodes"]
+            r["cg"] += st["cg_iters"]
+            V[name] = hs[name].voltage()
+        for name, _ in forms[1:]:
+            res[name]["vinf"] = max(res[name]["vinf"], float(np.abs(V[name] - V[ref]).max()))
+    n = wl.mesh.n
+    for name, _ in forms:
+        r = res[name]
+        r["ta"], r["apd"] = hs[name].activation()
+        r["ecg"] = hs[name].ecg()[1]
+        hs[name].close()
+    bin_steps = [min(steps, int(round((i + 1) * bin_ms / wl.dt))) - min(steps, int(round(i * bin_ms / wl.dt)))
+                 for i in range(nbin)]
+    out = {"t_ms": T, "steps": steps, "n_nodes": int(n),
+           "timed": "every step of the run, device time (CUDA events on each handle's stream)"}
+    R = res[ref]
+    for name, _ in forms:
+        r = res[name]
+        e = {"node_steps_per_s": n * steps / (r["ms"] * 1e-3), "ms_per_step": r["ms"] / steps,
+             "fallback_fraction": r["fb"] / float(n * steps), "cg_iters_per_solve": r["cg"] / (2.0 * steps),
+             "launch_config": shapes.get(name),
+             "node_steps_per_s_per_bin": [n * s / (ms * 1e-3) if ms > 0 else None
+                                          for s, ms in zip(bin_steps, r["bins"])]}
+        if name != ref:
+            e["vs_" + ref] = accuracy(R, r, n)
+        out[name] = e
+    out["bin_ms"] = bin_ms
+    return out
+
+
+def accuracy(R, r, n):
+    """Errors of one form's run (r) against the reference form's (R)."""
+    import numpy as np
+    both = (R["ta"] >= 0) & (r["ta"] >= 0)
+    da = np.abs(r["ta"] - R["ta"])[both]
+    ab = (R["apd"] > 0) & (r["apd"] > 0)
+    dp = np.abs(r["apd"] - R["apd"])[ab]
+    e = {"activated": float((r["ta"] >= 0).mean()), "activated_ref": float((R["ta"] >= 0).mean()),
+         "act_err_ms": {"mean": float(da.mean()) if both.any() else None,
+                        "p99": float(np.percentile(da, 99)) if both.any() else None,
+                        "max": float(da.max()) if both.any() else None},
+         "apd90_err_ms": {"n": int(ab.sum()),
+                          "mean": float(dp.mean()) if ab.any() else None,
+                          "p99": float(np.percentile(dp, 99)) if ab.any() else None,
+                          "p9999": float(np.percentile(dp, 99.99)) if ab.any() else None,
+                          "max": float(dp.max()) if ab.any() else None,
+                          "nodes_over_1ms": int((dp > 1.0).sum()), "nodes_over_5ms": int((dp > 5.0).sum()),
+                          "repolarised": float((r["apd"] > 0).mean()),
+                          "repolarised_ref": float((R["apd"] > 0).mean())},
+         "vm_linf_mv": r["vinf"],
+         "ecg_rel_l2": float(np.linalg.norm(r["ecg"] - R["ecg"]) / np.linalg.norm(R["ecg"]))}
+    if ab.any():
+        idx = np.where(ab)[0]
+        w = int(idx[int(np.argmax(dp))])
+        e["apd90_err_ms"]["worst_node"] = {"node": w, "apd90_ref": float(R["apd"][w]), "apd90": float(r["apd"][w]),
+                                           "t_act_ref": float(R["ta"][w]), "t_act": float(r["ta"][w])}
+    return e
+
+
+def _timed_window(h, warmup, steps, dist, clk=None):
+    """W untimed steps, then K steps timed on the device (per-kernel events on)."""
+    import torch
+    h.set_profiling(True)
+    h.step(warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    st = h.step(steps)
+    torch.cuda.synchronize()
+    return st, max_over_ranks(st["device_ms"], dist)
 
 
 def run_ours(args, rank, world, local):
@@ -272,122 +472,113 @@ def run_ours(args, rank, world, local):
     if args.workload == "batch_c3":
         return run_batch(args, rank, world, local, dist, prec)
     wl = {"shell_c2": W.shell_c2, "slab_c0": W.slab_c0, "slab_c1": W.slab_c1}[args.workload]()
-    g = wl.create(prec, device=local)
-    if prec == capi.SURROGATE:
-        from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
-        Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(g)
     n = wl.mesh.n
-    # the timed window starts at t_start (advanced untimed), inside the
-    # activation of the wall, so that the window holds wavefronts, plateau
-    # and rest rather than the quiet first milliseconds
-    pre = int(round(args.t_start / wl.dt))
-    if args.launch:
-        g.set_launch_config(**json.loads(args.launch))
-    for k in range(0, pre, 500):
-        g.step(min(500, pre - k))
-    # the project's autotuner picks the launch shape (state is restored)
-    tuned = g.autotune(20) if not args.no_tune else None
-    if args.launch and tuned:
-        g.set_launch_config(**json.loads(args.launch))
-    g.set_profiling(True)
-    g.step(args.warmup)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    K, Wu = args.steps, args.warmup
     clk = Clocks(local)
     clk.start()
-    st = g.step(args.steps)
-    clocks = clk.stop()
-    torch.cuda.synchronize()
-    ms = max_over_ranks(st["device_ms"], dist)
-    if dist:
-        dist.barrier()
-    value = replica_value(n, args.steps, world, ms)
-    # ---- end to end through the public API with host buffers ----
-    states = g.states()
-    V = g.voltage()
-    k_e2e = max(3, args.steps)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    g.set_states(states)
-    g.set_voltage(V)
-    for _ in range(k_e2e):
-        g.step(1)
-        V = g.voltage()
-    e2e_s = time.perf_counter() - t0
+    # ---- the primary form over the common window ----
+    g = _deploy(wl.create(prec, device=local), prec)
+    if args.launch:
+        g.set_launch_config(**json.loads(args.launch))
+    tuned = g.autotune(20) if not args.no_tune else None    # the state is put back afterwards
+    if args.launch and tuned:
+        g.set_launch_config(**json.loads(args.launch))
+    shape = g.launch_config()
+    st, ms = _timed_window(g, Wu, K, dist)
+    value = replica_value(n, K, world, ms)
     rb = 8 if prec == capi.FP64 else 4
-    e2e = {"value": n * k_e2e / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": int((states.nbytes + V.nbytes) / k_e2e),
-           "d2h_bytes_per_step": int(V.nbytes)}
-    # ---- roofline of the dominant kernel ----
+    # roofline of the dominant kernel, from the per-kernel events of the window
     nnz = int(wl.mesh.n + 2 * _edge_count(wl.mesh))
-    cg_per_solve = st["cg_iters"] / max(1, 2 * args.steps)
+    cg_per_solve = st["cg_iters"] / max(1, 2 * K)
     kms = {"cg": st["cg_ms"], "ionic": st["ionic_ms"], "ecg": st["ecg_ms"]}
     ecg_every = max(1, int(round(1.0 / wl.dt)))
-    launches = {"cg": 2 * args.steps, "ionic": args.steps, "ecg": max(1, args.steps // ecg_every)}
+    launches = {"cg": 2 * K, "ionic": K, "ecg": max(1, K // ecg_every)}
     dom = max(kms, key=kms.get)
     per_launch_ms = kms[dom] / max(1, launches[dom])
     nstate = capi.model_nstate(wl.model)
     alg = algorithmic_bytes(dom, n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes),
-                            ecg_every=ecg_every, cg_predict=g.launch_config()["cg_predict"])
+                            ecg_every=ecg_every, cg_predict=shape["cg_predict"])
     peak, peak_kind = _peaks()
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": _traffic(dom, args.form, cg_per_solve, g.launch_config()["cg_predict"]) if wl.name == "shell_c2" else None,
-            "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
-            "kernel_ms": kms}
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": _traffic(dom, args.form, cg_per_solve, shape["cg_predict"]) if wl.name == "shell_c2" else None,
+            "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "kernel_ms": kms}
     b_ns = node_step_bytes(n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes), ecg_every=ecg_every,
-                           cg_predict=g.launch_config()["cg_predict"])
+                           cg_predict=shape["cg_predict"])
     roof["step"] = {"bytes_per_node_step": b_ns, "achieved": b_ns * value / 1e9, "frac": b_ns * value / 1e9 / peak}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else ("bf16+f32" if prec == capi.SURROGATE else "f32"),
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD_TEXT[wl.name].format(n=n, m=wl.mesh.m),
-                       "form": args.form, "dt_ms": wl.dt, "ionic_dt_ms": wl.ionic_dt,
-                       "t_window_ms": [round((pre + args.warmup) * wl.dt, 3),
-                                       round((pre + args.warmup + args.steps) * wl.dt, 3)],
-                       "l2": "inputs > L2 (operators + states ~ 0.5 GB), no flush",
-                       "cg_iters_per_solve": cg_per_solve, "newton_iters": st["newton_iters"],
-                       "launch_config": tuned[0] if tuned else g.launch_config(),
-                       "fallback_fraction": st["fallback_nodes"] / float(n * args.steps),
-                       "parallelism": f"replicas x{world}"},
-            "gpu_launches": int(st["launches"]),
-            "clocks": clocks, "roofline": roof, "e2e": e2e}
-    if prec == capi.SURROGATE and not args.no_compare:
-        # the plain FP32 form over the same simulated window, for the ratio
-        # the metric is about (same handle set-up, same steps)
-        gp = wl.create(capi.FP32, device=local)
-        for k in range(0, pre, 500):
-            gp.step(min(500, pre - k))
-        if not args.no_tune:
-            gp.autotune(20)
-        gp.step(args.warmup)
-        torch.cuda.synchronize()
-        stp = gp.step(args.steps)
-        vp = replica_value(n, args.steps, world, max_over_ranks(stp["device_ms"], dist))
-        line["config"]["plain_fp32"] = {"value": vp, "ms_per_step": stp["device_ms"] / args.steps,
-                                        "launch_config": gp.launch_config(),
-                                        "cg_iters_per_solve": stp["cg_iters"] / max(1, 2 * args.steps)}
-        line["config"]["speedup_vs_plain_fp32"] = value / vp
-        gp.close()
-    if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        h = float(os.environ.get("EP_CPU_SAMPLE_H", "0.12"))
-        ncpu, times, kind = cpu_sample("reference", h, 6, threads)
-        v = ncpu * 5 / sum(times[1:])
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
-                                "sample": f"5 steps (after 1 untimed) of a {ncpu}-node shell "
-                                          f"(h={h} cm) from t=0, same model, dt and stimuli",
-                                "cpu": cpu_model()}
-        # the same path on one host thread (the reference runs one MPI rank
-        # per core; this is one rank's speed), on a coarser sample
-        n1, t1, _ = cpu_sample("reference", 0.2, 3, 1)
-        line["cpu_baseline"]["value_1_thread"] = n1 * 2 / sum(t1[1:])
-        line["cpu_baseline"]["sample_1_thread"] = f"2 steps (after 1 untimed) of a {n1}-node shell (h=0.2 cm)"
+    forms = {args.form: {"value": value, "ms_per_step": ms / K, "cg_iters_per_solve": cg_per_solve,
+                         "newton_iters": st["newton_iters"], "fallback_fraction": st["fallback_nodes"] / float(n * K),
+                         "launch_config": shape}}
+    gpu_launches = int(st["launches"])
     g.close()
+    # ---- the plain FP32 form over the same window (the metric's ratio) ----
+    if prec == capi.SURROGATE and not args.no_compare:
+        gp = wl.create(capi.FP32, device=local)
+        tp = gp.autotune(20) if not args.no_tune else None
+        stp, msp = _timed_window(gp, Wu, K, dist)
+        vp = replica_value(n, K, world, msp)
+        forms["plain_fp32"] = {"value": vp, "ms_per_step": msp / K,
+                               "cg_iters_per_solve": stp["cg_iters"] / max(1, 2 * K),
+                               "newton_iters": stp["newton_iters"], "launch_config": gp.launch_config()}
+        forms["speedup_vs_plain_fp32"] = value / vp
+        gp.close()
+    # ---- end to end through the public API with host buffers, same window ----
+    ge = _deploy(wl.create(prec, device=local), prec)
+    ge.set_launch_config(**shape)
+    ge.step(Wu)
+    S_host, V_host = ge.states(), ge.voltage()      # the window's inputs, in host memory
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ge.set_states(S_host)
+    ge.set_voltage(V_host)
+    for _ in range(K):
+        ge.step(1)
+        V_out = ge.voltage()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
+    e2e = {"value": replica_value(n, K, world, e2e_s * 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int((S_host.nbytes + V_host.nbytes) / K),
+           "d2h_bytes_per_step": int(V_out.nbytes),
+           "copies": "the window's inputs (V and all cell states, FP64 host arrays) uploaded once at the "
+                     "start of the timed region, V read back after every step; wall clock, synchronised"}
+    ge.close()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": Wu, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == capi.FP64 else ("bf16+f32" if prec == capi.SURROGATE else "f32"),
+            "data": "synthetic", "form": args.form,
+            "config": shared_config(wl.name, n, wl.mesh.m, wl.dt, wl.ionic_dt, Wu, K)
+            if wl.name in WORKLOAD_TEXT else {"workload": wl.name},
+            "forms": forms, "parallelism": f"replicas x{world}", "gpu_launches": gpu_launches,
+            "roofline": roof, "e2e": e2e}
+    # ---- the metric's whole run (500 ms), three forms in lockstep ----
+    if world == 1 and not args.no_run and wl.name == "shell_c2" and prec == capi.SURROGATE:
+        shapes = {"surrogate": shape}
+        if "plain_fp32" in forms:
+            shapes["plain_fp32"] = forms["plain_fp32"]["launch_config"]
+        run = whole_run(wl, [("fp64", capi.FP64), ("plain_fp32", capi.FP32), ("surrogate", capi.SURROGATE)],
+                        shapes, local, T=args.run_ms, tune=not args.no_tune)
+        run["speedup_vs_plain_fp32"] = run["surrogate"]["node_steps_per_s"] / run["plain_fp32"]["node_steps_per_s"]
+        run["speedup_vs_fp64"] = run["surrogate"]["node_steps_per_s"] / run["fp64"]["node_steps_per_s"]
+        line["run_500ms" if abs(args.run_ms - 500.0) < 1e-9 else f"run_{args.run_ms:g}ms"] = run
+        line["speedup_vs_plain_fp32"] = run["speedup_vs_plain_fp32"]
+    line["clocks"] = clk.stop()
+    # ---- CPU baseline: the port on the same shell (bounded sample) ----
+    if rank == 0 and world == 1 and not args.no_cpu and wl.name == "shell_c2":
+        from oracle import oracle as O
+        threads = host_threads()
+        O.set_threads(threads)
+        sim, keep = cpu_sim(wl, "port")
+        t = cpu_steps(sim, wl, 0, 2)
+        line["cpu_baseline"] = {"value": n * len(t) / sum(t), "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"steps 0-1 of the same {n}-node shell from t = 0 (the CPU restatement "
+                                          "of the split step with the GPU arm's cell set-up)",
+                                "cpu": cpu_model()}
+        del sim, keep
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(_finite(line)), flush=True)
     if dist:
         dist.destroy_process_group()
 
@@ -436,64 +627,16 @@ def run_accuracy(args, local):
     Tusscher at dt = 0.1 ms, the step the network was trained for) learned
     forms; errors against FP64: activation time, APD90, Vm L-infinity over
     1 ms snapshots, pseudo-ECG relative L2."""
-    import numpy as np
     import torch
     from ucla_cmg_b200 import capi, workloads as W
-    from ucla_cmg_b200.surrogate import Surrogate, DEFAULT_PATH
     torch.cuda.set_device(local)
     wl = {"shell_c2": W.shell_c2, "slab_c0": W.slab_c0, "slab_c1": W.slab_c1}[args.workload]()
-    steps = int(round(args.accuracy / wl.dt))
-    per_ms = max(1, int(round(1.0 / wl.dt)))
     forms = [("fp64", capi.FP64), ("plain_fp32", capi.FP32)]
     if wl.model == capi.TUSSCHER and abs(wl.dt - 0.1) < 1e-12:
         forms.append(("surrogate", capi.SURROGATE))
-    hs = {}
-    tuned = {}
-    for name, prec in forms:
-        hs[name] = wl.create(prec, device=local)
-        if prec == capi.SURROGATE:
-            Surrogate.load(os.environ.get("EP_SURROGATE_PATH", DEFAULT_PATH)).deploy(hs[name])
-        if not args.no_tune:
-            tuned[name] = hs[name].autotune(20)[0]      # the state is put back afterwards
-    res = {name: dict(ms=0.0, fb=0, vinf=0.0) for name, _ in forms}
-    # the three runs advance in lockstep; Vm is compared every 1 ms
-    for k in range(0, steps, per_ms):
-        V = {}
-        for name, _ in forms:
-            st = hs[name].step(min(per_ms, steps - k))
-            res[name]["ms"] += st["device_ms"]
-            res[name]["fb"] += st["fallback_nodes"]
-            V[name] = hs[name].voltage()
-        for name, _ in forms[1:]:
-            res[name]["vinf"] = max(res[name]["vinf"], float(np.abs(V[name] - V["fp64"]).max()))
-    for name, _ in forms:
-        r = res[name]
-        r["ta"], r["apd"] = hs[name].activation()
-        r["ecg"] = hs[name].ecg()[1]
-        r["fb"] /= float(wl.mesh.n * steps)
-        hs[name].close()
-    ref = res["fp64"]
-    out = {"workload": wl.name, "t_ms": args.accuracy, "n_nodes": int(wl.mesh.n), "dt_ms": wl.dt}
-    for name, _ in forms:
-        r = res[name]
-        e = {"node_steps_per_s": wl.mesh.n * steps / (r["ms"] * 1e-3), "fallback_fraction": r["fb"],
-             "launch_config": tuned.get(name)}
-        if name != "fp64":
-            both = (ref["ta"] >= 0) & (r["ta"] >= 0)
-            da = np.abs(r["ta"] - ref["ta"])[both]
-            ab = (ref["apd"] > 0) & (r["apd"] > 0)
-            dp = np.abs(r["apd"] - ref["apd"])[ab]
-            e.update({"activated": float((r["ta"] >= 0).mean()), "activated_fp64": float((ref["ta"] >= 0).mean()),
-                      "act_err_ms": {"mean": float(da.mean()), "p99": float(np.percentile(da, 99)), "max": float(da.max())},
-                      "apd90_err_ms": {"n": int(ab.sum()), "mean": float(dp.mean()) if ab.any() else None,
-                                       "p99": float(np.percentile(dp, 99)) if ab.any() else None,
-                                       "max": float(dp.max()) if ab.any() else None,
-                                       "repolarised": float((r["apd"] > 0).mean()),
-                                       "repolarised_fp64": float((ref["apd"] > 0).mean())},
-                      "vm_linf_mv": r["vinf"],
-                      "ecg_rel_l2": float(np.linalg.norm(r["ecg"] - ref["ecg"]) / np.linalg.norm(ref["ecg"]))})
-        out[name] = e
-    print(json.dumps(out), flush=True)
+    out = whole_run(wl, forms, {}, local, T=args.accuracy, tune=not args.no_tune)
+    out["workload"] = wl.name
+    print(json.dumps(_finite(out)), flush=True)
 
 
 def _edge_count(m):
@@ -507,22 +650,26 @@ def _edge_count(m):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="surrogate", choices=["plain_fp32", "fp64", "surrogate"])
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-run", action="store_true", help="skip the whole 500-ms run of the three forms")
+    ap.add_argument("--run-ms", type=float, default=500.0, help="length of the whole run (ms)")
+    ap.add_argument("--no-ref-objects", action="store_true",
+                    help="reference arm: skip the one-step sample of the reference's own cell objects")
     ap.add_argument("--workload", default="shell_c2", choices=["shell_c2", "batch_c3", "slab_c0", "slab_c1"])
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--launch", default="", help='launch-shape fields set after tuning, JSON ({"cg_predict": 2})')
     ap.add_argument("--no-compare", action="store_true",
                     help="surrogate form: skip the plain FP32 run over the same window")
-    ap.add_argument("--t-start", type=float, default=40.0,
-                    help="simulated ms advanced (untimed) before the warm-up")
     ap.add_argument("--accuracy", type=float, default=0.0,
-                    help="instead of timing: run the shell this many ms in FP64, FP32 and the "
-                         "learned form and print the errors against FP64")
+                    help="instead of timing: run --workload this many ms in FP64, FP32 (and the "
+                         "learned form) and print the errors against FP64")
     args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours" and args.accuracy <= 0:
+        ap.error("--warmup must be >= 3")
     rank, world, local = _env()
     if args.accuracy > 0:
         if rank == 0:

@@ -25,13 +25,15 @@ TT_XI = 2000.0
 MH_XI = 1.55e-4 / 2.58e-8
 
 
-def tt_type_consts():
+def tt_type_consts(epi=None):
     """ten Tusscher 2006 parameter sets: 0 endo, 1 M, 2 epi.
 
     The reference ships the epicardial set only (SetUpIonicConstants.h:88-147);
     the endocardial (G_to 0.073, slow s-gate) and M-cell (G_Ks 0.098) sets are
-    the TT2006 paper's values on top of it."""
-    epi = capi.default_consts(capi.TUSSCHER)
+    the TT2006 paper's values on top of it.  ``epi``: the epicardial set to
+    start from (default: the library's copy of SetUpTusscherParameters; a CPU
+    caller that must not load the GPU library passes its own)."""
+    epi = capi.default_consts(capi.TUSSCHER) if epi is None else np.array(epi, dtype=np.float64)
     endo = epi.copy(); endo[20] = 0.073; endo[53] = 1.0
     mid = epi.copy(); mid[15] = 0.098
     return np.stack([endo, mid, epi])
@@ -91,7 +93,7 @@ def slab_c1(nx=201, ny=201, nz=21):
                     node_type=np.zeros(m.n, np.uint8))
 
 
-def shell_c2(h=0.0365, n_rho=20, seed=0, n_pmj=200):
+def shell_c2(h=0.0365, n_rho=20, seed=0, n_pmj=200, epi=None):
     m = M.shell(h=h, n_rho=n_rho)
     rho, height = m.meta["rho"], m.meta["height"]
     node_type = np.where(rho < 0.4, 0, np.where(rho < 0.7, 1, 2)).astype(np.uint8)
@@ -104,7 +106,7 @@ def shell_c2(h=0.0365, n_rho=20, seed=0, n_pmj=200):
     el = M.fibonacci_sphere(10, 15.0, m.xyz.mean(axis=0))
     return Workload("shell_c2", m, capi.TUSSCHER, 0.1, 0.02, 500.0, M.sigma_to_D(1.2, 0.2), -85.423,
                     ids, on, on + 2.0, np.full(len(ids), 50.0 * TT_XI), el,
-                    node_type=node_type, type_consts=tt_type_consts(), gks_scale=gks)
+                    node_type=node_type, type_consts=tt_type_consts(epi), gks_scale=gks)
 
 
 @dataclass
@@ -134,14 +136,14 @@ class BatchWorkload:
         return b
 
 
-def batch_c3(n_inst=64, seed=0, h=0.02, lo=(21, 21, 6), hi=(101, 101, 11)):
+def batch_c3(n_inst=64, seed=0, h=0.02, lo=(21, 21, 6), hi=(101, 101, 11), epi=None):
     """64 independent ten Tusscher slabs of uneven size (grid uniform in
     21x21x6 .. 101x101x11 nodes, spacing 0.02 cm), each with G_Ks, G_to and
     G_CaL scaled by U(0.5, 1.5) and a 5x5-node full-thickness stimulus block
     at a random one of its four vertical edges (50 uA/cm^2, 1 ms at t = 0);
-    FP32, dt = 0.02 ms, 200 ms."""
+    FP32, dt = 0.02 ms, 200 ms.  ``epi`` as for :func:`tt_type_consts`."""
     rng = np.random.default_rng(seed)
-    epi = capi.default_consts(capi.TUSSCHER)
+    epi = capi.default_consts(capi.TUSSCHER) if epi is None else np.array(epi, dtype=np.float64)
     inst, ids, off = [], [], 0
     for k in range(n_inst):
         nx, ny = (int(v) for v in rng.integers(lo[:2], np.asarray(hi[:2]) + 1))
