@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define EP_ABI_VERSION 2
+#define EP_ABI_VERSION 3
 
 /* ---- status codes ---- */
 #define EP_OK               0
@@ -28,7 +28,8 @@ extern "C" {
 #define EP_ERR_MESH        -4   /* degenerate or inverted element */
 #define EP_ERR_CG          -5   /* a CG solve reached cg_maxit */
 #define EP_ERR_NEWTON      -6   /* a Newton solve reached its cap */
-#define EP_ERR_NAN         -7   /* non-finite voltage detected */
+#define EP_ERR_NAN         -7   /* non-finite voltage after a step (ep_step; the
+                                   step's stats are filled, stats->nonfinite > 0) */
 #define EP_ERR_TIMEOUT     -8   /* an in-kernel wait gave up */
 #define EP_ERR_UNSUPPORTED -9
 #define EP_ERR_IO          -10
@@ -214,9 +215,10 @@ int  ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres);
  * working vectors live in one static device array of this library sized for
  * at most 262144 rows (about 8.2 MB, held by every GPU that loads the
  * library until exit); larger n returns EP_ERR_ARG.  Every call shares that
- * array, so calls that overlap on the GPU race: serialise them.  The first
- * call on a device looks up the array's address on that device; make it
- * before any stream capture. */
+ * array, so calls that overlap on the GPU race: serialise them.  Each call
+ * looks up the array's address on the current device.  The call waits on
+ * `stream` for its results before it returns; on a stream in capture mode
+ * it returns EP_ERR_ARG without touching the stream. */
 int  ep_cn_half_step_noalloc(int32_t precision, int32_t n, int32_t nslices,
                              const int32_t *slice_ptr, const int32_t *col,
                              const void *Aval, const void *Bval, const void *dinv,
@@ -271,6 +273,13 @@ typedef struct ep_cables_desc {
     const int32_t *angle_nodes; /* n_angle node ids */
     const double *angle;        /* 4 * n_angle: direction (3), length */
     int32_t angle_sticky;
+    /* n_bars or NULL: per cable, the index into angle_nodes/angle of the
+     * row that overrides it (-1: none), resolved by the caller over the
+     * whole .ele order.  The reference switches the override on for ANY
+     * element whose first node is listed -- tets included -- and keeps it
+     * on (MixedMesh3D.cc:30-34, 78-87), which a bars-only list cannot show;
+     * given, angle_sticky is not consulted. */
+    const int32_t *bar_angle;
 } ep_cables_desc;
 
 /* The FP64 operators ep_create assembles for the solver's scheme, on the
@@ -294,7 +303,10 @@ int  ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_desc *cable
  * (fewer registers per thread), 0 = the compiler's register choice;
  * cg_batch: SELL columns whose gathers the CG kernel issues together (4 or
  * 8; 8 keeps more loads in flight at a larger register budget; 16: groups of
- * 8 with the next group's index loads issued before the current gathers);
+ * 8 with the next group's index loads issued before the current gathers;
+ * 32: staged -- each warp's next two slices of column indices and values are
+ * brought into shared memory by bulk asynchronous copies while it gathers
+ * the current one, at most 256 threads per CTA, cg_variant 0 only);
  * cg_variant: 0 the CG recurrences of the reference (two reductions per
  * iteration), 1 the Chronopoulos-Gear recurrences (one reduction per
  * iteration; same iterates in exact arithmetic, rounding-level differences;
@@ -310,6 +322,20 @@ typedef struct ep_launch_config {
                              SELL indices and values of the slice it reads that
                              many slices ahead (cg_variant 0; 0 = off) */
 } ep_launch_config;
+/* Bounded in-kernel waits (no reference counterpart: the reference has no
+ * device code; its Newton loop has no cap, Tusscher.cc:150).  Every wait of
+ * the persistent kernels polls a bounded number of times and then gives up:
+ * grid_polls caps one CG grid-barrier wait (polls of ~64 ns sleeps; 0 = the
+ * built-in 2^24, seconds), mbar_polls one tensor-core completion wait of
+ * the learned step (0 = 2^22).  A wait that runs out makes ep_step return
+ * EP_ERR_TIMEOUT (stats->timeouts > 0); the handle's wait state is then
+ * reset so it can step again, but V and the states of that call are not to
+ * be trusted (restore them with ep_set_voltage / ep_set_states). */
+int  ep_set_wait_limits(ep_handle *h, uint32_t grid_polls, uint32_t mbar_polls);
+/* Test hook for the timeout path (no reference counterpart): the CG grid
+ * barrier waits for extra_arrivals more CTAs than the launch has, so every
+ * wait runs out after its poll limit; 0 restores normal operation. */
+int  ep_test_hold_barrier(ep_handle *h, int32_t extra_arrivals);
 int  ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg);
 int  ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg);
 /* Autotuner: times trial_steps steps (after one untimed pass) for the

@@ -54,7 +54,8 @@ def run(input_file, out_dir=None, reference_cells=True, rest_voltage=False, cg_t
     if cab is not None:
         cables = O.Cables(cab["bars"], Dp=cab["Dp"], DpLeft=cab["DpLeft"], radius=cab["radius"],
                           fibers=cab["bar_fibers"], lv=cab["lv"], quad_order=cab["quad_order"],
-                          orient=cab["angle"] or None, n=n)
+                          orient=cab["angle"] or None, n=n,
+                          bar_orient_node=cab["bar_angle_node"] if cab["angle"] else None)
     csr = O.Csr(mesh.xyz, mesh.tets, mesh.fibers, cfg["D"], 1.0, dt, smoothing_alpha=cfg["smoothing"] or 0.0,
                 cables=cables)
     tis_nodes = np.where(is_purk == 0)[0]

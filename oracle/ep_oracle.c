@@ -1127,7 +1127,13 @@ static int bar_triplets(const double *xyz, const epo_cables *cb, double Cm, trip
         for (int k = 0; k < 3; k++) ang[k] = xyz[3 * v[1] + k] - xyz[3 * v[0] + k];
         mag = sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
         for (int k = 0; k < 3; k++) ang[k] /= mag;
-        if (pmj && cb->orient_sticky) {
+        if (cb->bar_orient_node) {
+            const int o = cb->bar_orient_node[e];
+            if (o >= 0) {
+                for (int k = 0; k < 3; k++) ang[k] = cb->orient[4 * (size_t)o + k];
+                mag = cb->orient[4 * (size_t)o + 3];
+            }
+        } else if (pmj && cb->orient_sticky) {
             for (int k = 0; k < 3; k++) ang[k] = pmj_data[k];
             mag = pmj_data[3];
         } else if (cb->orient_has && cb->orient_has[v[0]]) {

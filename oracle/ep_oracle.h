@@ -136,6 +136,12 @@ typedef struct epo_cables {
     const uint8_t *orient_has;   /* n or NULL */
     const double *orient;        /* n * 4: direction, length */
     int orient_sticky;
+    /* nb or NULL: per cable, the node whose .angle row overrides it (-1:
+     * none), resolved by the caller over the whole element order (the
+     * reference also lets a tet whose first node is listed switch the
+     * override on, MixedMesh3D.cc:30-34); when given, orient_has and
+     * orient_sticky are not consulted */
+    const int *bar_orient_node;
 } epo_cables;
 
 /* tets then cables, summed in that element order; tets alone == epo_assemble */

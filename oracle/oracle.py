@@ -47,7 +47,7 @@ class _Cables(C.Structure):
     _fields_ = [("nb", C.c_int), ("bars", ip), ("fibers", dp), ("lv", C.POINTER(C.c_uint8)),
                 ("Dp", C.c_double * 3), ("DpLeft", C.c_double * 3), ("radius", C.c_double),
                 ("quad_order", C.c_int), ("orient_has", C.POINTER(C.c_uint8)), ("orient", dp),
-                ("orient_sticky", C.c_int)]
+                ("orient_sticky", C.c_int), ("bar_orient_node", ip)]
 
 
 class _Cells(C.Structure):
@@ -463,7 +463,10 @@ class Cables:
     Purkinje diffusion, the cable radius and the .angle overrides."""
 
     def __init__(self, bars, Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, fibers=None, lv=None,
-                 quad_order=2, orient=None, sticky=True, n=None):
+                 quad_order=2, orient=None, sticky=True, n=None, bar_orient_node=None):
+        """bar_orient_node: per cable the node whose ``orient`` row overrides
+        it (-1: none), resolved over the whole element order (see
+        :func:`bar_angle_nodes`); given, it replaces the sticky rule."""
         self.bars = np.ascontiguousarray(bars, dtype=np.int32).reshape(-1, 2)
         self.fibers = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
         self.lv = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
@@ -478,7 +481,7 @@ class Cables:
         self.c.radius = radius
         self.c.quad_order = quad_order
         self.c.orient_sticky = int(bool(sticky))
-        self.has = self.orient = None
+        self.has = self.orient = self.bon = None
         if orient:                       # {node (zero-based): (dx, dy, dz, length)}
             self.has = np.zeros(n, np.uint8)
             self.orient = np.zeros((n, 4))
@@ -487,6 +490,31 @@ class Cables:
                 self.orient[k] = v
             self.c.orient_has = _p(self.has, C.POINTER(C.c_uint8))
             self.c.orient = _p(self.orient)
+        if bar_orient_node is not None:
+            self.bon = np.ascontiguousarray(bar_orient_node, dtype=np.int32)
+            if self.orient is None:
+                self.orient = np.zeros((n, 4))
+                self.c.orient = _p(self.orient)
+            self.c.bar_orient_node = _p(self.bon, ip)
+
+
+def bar_angle_nodes(elements, angle, sticky=True):
+    """Per 2-node element of ``elements`` (zero-based node lists in .ele
+    order), the node whose .angle row overrides it, or -1: the rule of
+    MixedMesh3D::Compute (MixedMesh3D.cc:30-34, 78-87), where every element
+    whose first node is listed -- tets included -- switches the override on
+    (sticky: it stays on, with the latest row, for every later cable) and
+    ``sticky=False`` applies a row to the cable that starts at its node only."""
+    out, cur = [], -1
+    for el in elements:
+        if el[0] in angle:
+            cur = el[0]
+        if len(el) == 2:
+            if sticky:
+                out.append(cur)
+            else:
+                out.append(el[0] if el[0] in angle else -1)
+    return np.array(out, dtype=np.int32)
 
 
 class Csr:

@@ -90,11 +90,12 @@ def test_single_reduction_variant_in_tissue(gpu):
 
 @pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
 def test_gather_widths_are_bit_identical(gpu, shell, prec):
-    """The gather width (4, 8, or 8 pipelined) changes which loads are in
-    flight together, not the order of the additions: same bits."""
+    """The gather width (4, 8, 8 pipelined, or the staged kernel with its
+    slices brought into shared memory by bulk copies) changes which loads are
+    in flight together, not the order of the additions: same bits."""
     wl, V, c = shell
     out = []
-    for nb in (4, 8, 16):
+    for nb in (4, 8, 16, 32):
         g = Monodomain(wl.mesh, capi.TUSSCHER, prec, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
         g.set_launch_config(cg_batch=nb, cg_per_sm=4)
         g.set_voltage(V)
@@ -186,3 +187,48 @@ def test_prefetch_changes_no_bits(gpu, shell):
             g.set_launch_config(cg_variant=1, cg_prefetch=2)
         finally:
             g.close()
+
+
+@pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
+def test_staged_cg_in_tissue_is_bit_identical(gpu, prec):
+    """The staged CG over a whole tissue run (predictor on, steps replayed
+    from a CUDA graph): every step's solves give the bits of the gather-width
+    8 kernel, so the fields after 400 steps are equal."""
+    from ucla_cmg_b200 import mesh as M
+    m = M.slab(23, 19, 5, 0.44, 0.36, 0.08)
+    out = []
+    for nb in (8, 32):
+        g = Monodomain(m, capi.TUSSCHER, prec, dt=0.02, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
+                       tt_jacobian=capi.TT_JAC_TRUE)
+        g.set_launch_config(cg_batch=nb, cg_predict=1, graph_steps=20)
+        g.set_voltage(-85.423)
+        g.set_stimulus(M.corner_block(m, 3, 3), 0.0, 1.0, 50.0 * 2000.0)
+        st = g.step(400)
+        assert st["cg_failures"] == 0 and st["timeouts"] == 0
+        out.append((g.voltage(), st["cg_iters"]))
+        g.close()
+    assert np.max(out[0][0]) > 0.0
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_staged_cg_batch_instances(gpu):
+    """Independent instances in one staged launch (each CTA group streams
+    its own instance's slices; the slices two instances share are masked):
+    the same bits as gather width 8."""
+    from ucla_cmg_b200 import mesh as M
+    from ucla_cmg_b200.simulation import Batch
+    insts = [dict(mesh=M.slab(nx, ny, 4, 0.02 * (nx - 1), 0.02 * (ny - 1), 0.06), D=M.sigma_to_D(1.2, 0.2))
+             for nx, ny in ((13, 9), (21, 17), (7, 11))]
+    out = []
+    for nb in (8, 32):
+        b = Batch(insts, capi.TUSSCHER, capi.FP32, dt=0.02, ionic_dt=0.02, tt_jacobian=capi.TT_JAC_TRUE)
+        b.set_launch_config(cg_batch=nb)
+        b.set_voltage(-85.423)
+        ids = np.concatenate([M.corner_block(i["mesh"], 3, 3) + o for i, o in zip(insts, b.offsets[:-1])])
+        b.set_stimulus(ids.astype(np.int32), 0.0, 1.0, 50.0 * 2000.0)
+        st = b.step(200)
+        assert st["cg_failures"] == 0
+        out.append(b.voltage())
+        b.close()
+    assert np.array_equal(out[0], out[1])

@@ -182,3 +182,47 @@ def test_reference_reads_the_files_the_library_writes(tmp_path):
     rb = O.RefFemBody(rm, O.TUSSCHER, (1e-3, 2e-4, 2e-4), 1.0)
     o = O.Csr(m.xyz, m.tets, m.fibers, (1e-3, 2e-4, 2e-4), 1.0, 0.1)
     assert _rel(o.scipy("K"), rb.diffusion(1.0)) <= RTOL
+
+
+@pytest.mark.parametrize("sticky_from", ["tet", "cable"])
+def test_angle_override_switched_on_by_any_element(tmp_path, sticky_from):
+    """MixedMesh3D::Compute tests the first node of EVERY element against the
+    .angle list (MixedMesh3D.cc:30-34): a tet whose first node is listed
+    switches the override on for the cables after it, though no cable starts
+    there.  The library's MIX3D reader resolves the override per cable over
+    the .ele order (voomep_io.read_cables), and the restatement and the host
+    assembly then equal the reference's operators."""
+    from ucla_cmg_b200 import voomep_io as IO
+    slab = M.slab(6, 5, 4, 0.5, 0.4, 0.3)
+    n0 = slab.n
+    extra = slab.xyz[[0]] + np.array([[0.0, 0.0, -0.05], [0.0, 0.0, -0.1], [0.02, 0.0, -0.14]])
+    xyz = np.vstack([slab.xyz, extra])
+    bars = [[n0, n0 + 1], [n0 + 1, n0 + 2]]
+    t0 = int(slab.tets[7][0])
+    listed = t0 if sticky_from == "tet" else n0 + 1
+    elements = [list(t) for t in slab.tets[:20]] + [bars[0]] + [list(t) for t in slab.tets[20:]] + [bars[1]]
+    angle = {listed: (0.0, 0.6, -0.8, 0.07)}
+    purk = np.array([n0, n0 + 1, n0 + 2])
+    node_type = np.zeros(len(xyz), np.int64)
+    node_type[purk] = 11
+    base = _ref(tmp_path, "mixa", xyz, elements, None, purk=purk, cell=node_type, angle=angle)
+    D, Dp, radius, dt = (1e-3,) * 3, (0.0016,) * 3, 0.0275, 0.1
+    rm = O.RefFemMesh(base, mixed=True, radius=radius)
+    rb = O.RefFemBody(rm, O.TUSSCHER, D, 1.0, Dp=Dp, DpLeft=Dp)
+    A = rb.diffusion(dt / 4.0) + rb.capacitance(True)
+    cab = IO.read_cables(base, node_type)
+    expect = [listed, listed] if sticky_from == "tet" else [-1, listed]
+    assert cab["angle_node"].tolist() == expect
+    cb = O.Cables(cab["bars"], Dp=Dp, DpLeft=Dp, radius=radius, lv=cab["lv"], orient=cab["angle"], n=len(xyz),
+                  bar_orient_node=cab["angle_node"])
+    o = O.Csr(xyz, slab.tets, None, D, 1.0, dt, cables=cb)
+    assert _rel(o.scipy("A"), A) <= RTOL
+    mm = M.TetMesh(xyz, slab.tets, None, {})
+    Al, _, _ = S.assemble_operators(mm, D, dt, bars=cab["bars"], lv=cab["lv"], angle=cab["angle"], Dp=Dp,
+                                    DpLeft=Dp, radius=radius, bar_angle_node=cab["angle_node"])
+    assert _rel(Al, A) <= RTOL
+    if sticky_from == "tet":
+        # the bars-only rule (no cable starts at a listed node) misses it
+        Ab, _, _ = S.assemble_operators(mm, D, dt, bars=cab["bars"], lv=cab["lv"], angle=cab["angle"], Dp=Dp,
+                                        DpLeft=Dp, radius=radius)
+        assert _rel(Ab, A) > 1e-6

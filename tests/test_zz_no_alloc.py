@@ -17,36 +17,36 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from ucla_cmg_b200 import capi, workloads as W
+from ucla_cmg_b200 import capi, mesh as M, workloads as W
 from ucla_cmg_b200.simulation import Monodomain
-
-pytestmark = pytest.mark.gpu
 
 
 def _sell(csr, S=32):
-    """SELL-32 packing of the oracle CSR (A and B share the columns)."""
+    """SELL-32 packing of the oracle CSR (A and B share the columns): row r
+    sits in slice r // 32, lane r % 32, its j-th entry at slice_ptr + 32 j +
+    lane; padding entries point at the row itself with value 0."""
     rp, col = csr.arr("rowptr"), csr.arr("col")
     A, B = csr.arr("A"), csr.arr("B")
     n = csr.n
     ns = (n + S - 1) // S
     lens = np.diff(rp)
-    width = np.array([lens[s * S:(s + 1) * S].max() for s in range(ns)])
-    sp = np.concatenate([[0], np.cumsum(width * S)]).astype(np.int32)
-    c = np.zeros(sp[-1], np.int32)
+    lp = np.zeros(ns * S, np.int64)
+    lp[:n] = lens
+    width = lp.reshape(ns, S).max(axis=1)
+    sp = np.concatenate([[0], np.cumsum(width * S)]).astype(np.int64)
+    pos = np.arange(sp[-1])
+    sl = np.repeat(np.arange(ns), width * S)
+    row = sl * S + (pos - sp[sl]) % S
+    c = np.minimum(row, n - 1).astype(np.int32)
     a = np.zeros(sp[-1])
     b = np.zeros(sp[-1])
-    for s in range(ns):
-        for lane in range(S):
-            r = s * S + lane
-            rr = min(r, n - 1)
-            ln = lens[r] if r < n else 0
-            idx = sp[s] + np.arange(width[s]) * S + lane
-            c[idx] = rr
-            c[idx[:ln]] = col[rp[r]:rp[r] + ln]
-            a[idx[:ln]] = A[rp[r]:rp[r] + ln]
-            b[idx[:ln]] = B[rp[r]:rp[r] + ln]
+    r = np.repeat(np.arange(n), lens)
+    k = sp[r // S] + (np.arange(len(col)) - rp[r]) * S + r % S
+    c[k] = col
+    a[k] = A
+    b[k] = B
     dinv = 1.0 / csr.scipy("A").diagonal()
-    return ns, sp, c, a, b, dinv
+    return ns, sp.astype(np.int32), c, a, b, dinv
 
 
 @pytest.fixture(scope="module")
@@ -59,10 +59,42 @@ def case():
     return wl, V, _sell(csr)
 
 
+@pytest.fixture(scope="module")
+def case_max():
+    """A 64 x 64 x 64 slab: 262,144 rows, the entry point's limit, so every
+    FP64 vector, the partial slots and the tail of the array are in use."""
+    m = M.slab(64, 64, 64, 1.26, 1.26, 1.26)
+    D = M.sigma_to_D(1.2, 0.2)
+    assert m.n == 262144
+    rng = np.random.default_rng(12)
+    V = -85.0 + 120.0 * (m.xyz[:, 0] < 0.3) + rng.normal(0, 1.0, m.n)
+    csr = O.Csr(m.xyz, m.tets, m.fibers, D, 1.0, 0.1)
+    wl = W.Workload("slab_max", m, capi.TUSSCHER, 0.1, 0.02, 0.0, D, None, None, None, None, None, None)
+    return wl, V, _sell(csr)
+
+
+def test_sell_packing_reproduces_the_csr_product():
+    """The packer itself, on the CPU: SELL-32 A x equals the CSR A x."""
+    m = M.slab(7, 5, 4, 0.3, 0.2, 0.15)
+    csr = O.Csr(m.xyz, m.tets, m.fibers, (1e-3, 2e-4, 2e-4), 1.0, 0.1)
+    ns, sp, c, a, b, dinv = _sell(csr)
+    x = np.random.default_rng(0).normal(size=m.n)
+    y = np.zeros(ns * 32)
+    for s in range(ns):
+        w = (sp[s + 1] - sp[s]) // 32
+        for j in range(w):
+            idx = sp[s] + 32 * j + np.arange(32)
+            y[s * 32:(s + 1) * 32] += a[idx] * x[c[idx]]
+    assert np.allclose(y[:m.n], csr.scipy("A") @ x, rtol=1e-14, atol=1e-14)
+    assert np.allclose(dinv * csr.scipy("A").diagonal(), 1.0)
+
+
 @pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
-def test_noalloc_matches_handle_path(gpu, case, prec):
+@pytest.mark.parametrize("which", ["shell", "max_rows"])
+@pytest.mark.gpu
+def test_noalloc_matches_handle_path(gpu, case, case_max, which, prec):
     import torch
-    wl, V, (ns, sp, c, a, b, dinv) = case
+    wl, V, (ns, sp, c, a, b, dinv) = case if which == "shell" else case_max
     n = wl.mesh.n
     # the existing entry point on the same mesh
     g = Monodomain(wl.mesh, capi.TUSSCHER, prec, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
@@ -99,6 +131,7 @@ def test_noalloc_matches_handle_path(gpu, case, prec):
     assert np.array_equal(outs[0][0], outs[1][0]) and outs[0][1] == outs[1][1]
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_oversize(gpu):
     L = capi.lib()
     n = 262145
@@ -106,3 +139,27 @@ def test_noalloc_rejects_oversize(gpu):
                                    None, None)
     assert rc == -1
     assert b"262144" in L.ep_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_leaves_a_capture_intact(gpu, case):
+    """Called on a stream that is being captured, the entry point returns
+    EP_ERR_ARG before it touches the stream (it waits for its own results,
+    which a capture cannot do), and the caller's capture stays usable."""
+    import torch
+    wl, V, (ns, sp, c, a, b, dinv) = case
+    dev = torch.device("cuda", 0)
+    bufs = [torch.from_numpy(v).to(dev) for v in (sp, c, a, b, dinv, V)]
+    L = capi.lib()
+    x = torch.arange(8, device=dev, dtype=torch.float64)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        y = x * 2.0
+        rc = L.ep_cn_half_step_noalloc(capi.FP64, wl.mesh.n, ns, *(t.data_ptr() for t in bufs[:5]),
+                                       bufs[5].data_ptr(), 1e-7, 1000,
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream), None, None)
+    assert rc == -1 and b"captured" in L.ep_last_error()
+    x.fill_(3.0)
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.all(y == 6.0)

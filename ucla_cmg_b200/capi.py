@@ -80,7 +80,7 @@ class CablesDesc(C.Structure):
                 ("fibers", dp), ("lv", C.POINTER(C.c_uint8)), ("Dp", C.c_double * 3),
                 ("DpLeft", C.c_double * 3), ("radius", C.c_double), ("quad_order", C.c_int32),
                 ("n_angle", C.c_int32), ("angle_nodes", C.POINTER(C.c_int32)), ("angle", dp),
-                ("angle_sticky", C.c_int32)]
+                ("angle_sticky", C.c_int32), ("bar_angle", C.POINTER(C.c_int32))]
 
 
 class LaunchConfig(C.Structure):
@@ -162,6 +162,8 @@ def lib():
         "ep_get_launch_config": ([H, C.POINTER(LaunchConfig)], C.c_int),
         "ep_set_launch_config": ([H, C.POINTER(LaunchConfig)], C.c_int),
         "ep_autotune": ([H, C.c_int32, C.POINTER(LaunchConfig), dp, dp, ip], C.c_int),
+        "ep_set_wait_limits": ([H, C.c_uint32, C.c_uint32], C.c_int),
+        "ep_test_hold_barrier": ([H, C.c_int32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -72,6 +72,7 @@ struct ep_handle {
     int mh_abs = 0;
     long long step = 0;
     int nslices = 0;
+    int max_slice_w = 0;                 // widest SELL slice (columns)
     // device memory
     DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, zv, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
@@ -110,6 +111,10 @@ struct ep_handle {
     DBuf ecg_slot;                       // next ECG sample slot (device counter)
     void *pin = nullptr;                 // pinned host staging for state transfers
     size_t pin_bytes = 0;
+    // bounded in-kernel waits (ep_set_wait_limits; 0 = the built-in limits)
+    // and the test hook that makes the CG barrier wait for arrivals that
+    // never come (ep_test_hold_barrier)
+    unsigned int wait_grid = 0, wait_mbar = 0, bar_extra = 0;
 };
 
 namespace {
@@ -190,6 +195,9 @@ void fill_ionic_args(ep_handle *h, IonicArgs<R> &a) {
     a.stride_dt = (R)h->ionic_dt;
 }
 
+// columns of one stage of the staged CG's shared-memory ring
+static int stage_width(const ep_handle *h) { return std::max(1, std::min(h->max_slice_w, kStageMaxW)); }
+
 template <typename R>
 void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.n = h->n; a.nslices = h->nslices;
@@ -213,6 +221,8 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
     a.delta = nullptr; a.delta_prev = nullptr; a.vin = nullptr;   // the time step sets the predictor
     a.prefetch = h->cg_prefetch;
+    a.bar_extra = h->bar_extra;
+    a.wstage = stage_width(h);
 }
 
 // start the CG predictor from x0 = V again (after a state upload or when it
@@ -232,6 +242,9 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
     Sell sell;
     pack_sell(csr, {&csr.A, &csr.B}, sell);
     h->nslices = sell.nslices;
+    h->max_slice_w = 0;
+    for (int k = 0; k < sell.nslices; k++)
+        h->max_slice_w = std::max(h->max_slice_w, (sell.slice_ptr[k + 1] - sell.slice_ptr[k]) / kSlice);
     if ((rc = upload_raw(h->slice_ptr, sell.slice_ptr.data(), sell.slice_ptr.size()))) return rc;
     if ((rc = upload_raw(h->col, sell.col.data(), sell.col.size()))) return rc;
     if ((rc = upload<R>(h->Aval, sell.vals[0]))) return rc;
@@ -297,7 +310,7 @@ extern "C" int ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_d
         tl[e] = v;
     }
     HostCables hc;
-    std::vector<int> bl;
+    std::vector<int> bl, bon;
     std::vector<uint8_t> ohas;
     std::vector<double> orient;
     if (cables && cables->n_bars > 0) {
@@ -330,6 +343,15 @@ extern "C" int ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_d
             }
             hc.orient_has = ohas.data();
             hc.orient = orient.data();
+            if (cables->bar_angle) {
+                bon.resize(cables->n_bars);
+                for (int e = 0; e < cables->n_bars; e++) {
+                    const int k = cables->bar_angle[e];
+                    EP_CHECK_ARG(k >= -1 && k < cables->n_angle, "bar_angle entry out of range");
+                    bon[e] = k < 0 ? -1 : cables->angle_nodes[k] - off;
+                }
+                hc.bar_orient_node = bon.data();
+            }
         }
     }
     const double Cm = mesh->Cm > 0.0 ? mesh->Cm : 1.0;
@@ -382,10 +404,21 @@ extern "C" int ep_batch_plan(int32_t ninst, const int32_t *inst_row, int32_t gri
 
 // (re)size the CG launch for the handle's launch shape: grid, CTA groups,
 // partials, barriers and per-instance results
+// every instance's grid barrier back to its initial state (count, generation
+// and error word 0) with the handle's poll limit: at creation, and after a
+// wait gave up (the blocks that left early leave count and err behind)
+static int reset_barriers(ep_handle *h) {
+    std::vector<GridBarrier> b(h->ninst);
+    for (GridBarrier &x : b) x = GridBarrier{0u, 0u, 0u, h->wait_grid};
+    EP_CUDA(cudaMemcpy(h->bar.p, b.data(), sizeof(GridBarrier) * b.size(), cudaMemcpyHostToDevice));
+    return EP_OK;
+}
+
 static int plan_cg(ep_handle *h) {
+    const int ws = stage_width(h);
     int rc = h->precision == EP_FP64
-                 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant)
-                 : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant);
+                 ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant, ws)
+                 : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant, ws);
     if (rc) return rc;
     if (h->cg_variant == 1 && !h->w0.p) {
         const size_t vb = (size_t)h->pitch * h->rsize;
@@ -408,7 +441,7 @@ static int plan_cg(ep_handle *h) {
     if ((rc = h->partial.alloc(sizeof(double) * 12 * (size_t)h->cg_grid))) return rc;
     if (h->bar.bytes != sizeof(GridBarrier) * (size_t)h->ninst) {
         if ((rc = h->bar.alloc(sizeof(GridBarrier) * (size_t)h->ninst))) return rc;
-        EP_CUDA(cudaMemset(h->bar.p, 0, sizeof(GridBarrier) * (size_t)h->ninst));
+        if ((rc = reset_barriers(h))) return rc;
     }
     if (h->cg_last.bytes != 2 * sizeof(double) * (size_t)h->ninst) {
         if ((rc = h->cg_last.alloc(2 * sizeof(double) * (size_t)h->ninst))) return rc;
@@ -458,6 +491,7 @@ static void fill_surrogate_args(ep_handle *h, const IonicArgs<float> &ia, Surrog
     sa.fallback_count = h->sg_count.as<int>();
     sa.status = h->status.as<DevStatus>();
     sa.err = h->sg_err.as<unsigned int>();
+    sa.mbar_polls = h->wait_mbar;
     sa.pred = h->sg_pred.as<float>();
     sa.take = h->sg_take.as<uint8_t>();
 }
@@ -1150,8 +1184,17 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
     if (h->has_surrogate) EP_CUDA(cudaMemcpy(&sg_err, h->sg_err.p, sizeof sg_err, cudaMemcpyDeviceToHost));
     if (stats) stats->timeouts += (int32_t)sg_err;
     if (bar.err || sg_err) {
+        // the kernels left early; put the wait state back so the handle can
+        // step again (the simulation state of this call is not to be trusted)
+        int rc2 = reset_barriers(h);
+        if (rc2) return rc2;
+        if (sg_err) EP_CUDA(cudaMemset(h->sg_err.p, 0, sizeof(unsigned int)));
         set_error(bar.err ? "a grid barrier wait gave up" : "a tensor-core completion wait gave up");
         return EP_ERR_TIMEOUT;
+    }
+    if (st.nonfinite) {
+        set_error("%u node(s) with a non-finite voltage after the step", st.nonfinite);
+        return EP_ERR_NAN;
     }
     return EP_OK;
 }
@@ -1177,7 +1220,12 @@ int ep_diffusion_half_step(ep_handle *h, int32_t *iters, double *relres) {
     EP_CUDA(cudaMemcpy(&bar, h->bar.p, sizeof bar, cudaMemcpyDeviceToHost));
     if (iters) *iters = (int32_t)last[0];
     if (relres) *relres = last[1];
-    if (bar.err) { set_error("a grid barrier wait gave up"); return EP_ERR_TIMEOUT; }
+    if (bar.err) {
+        int rc2 = reset_barriers(h);
+        if (rc2) return rc2;
+        set_error("a grid barrier wait gave up");
+        return EP_ERR_TIMEOUT;
+    }
     return EP_OK;
 }
 
@@ -1326,11 +1374,33 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     return EP_OK;
 }
 
+int ep_set_wait_limits(ep_handle *h, uint32_t grid_polls, uint32_t mbar_polls) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    h->wait_grid = grid_polls;
+    h->wait_mbar = mbar_polls;
+    return reset_barriers(h);
+}
+
+int ep_test_hold_barrier(ep_handle *h, int32_t extra_arrivals) {
+    EP_CHECK_ARG(h, "null handle");
+    EP_CHECK_ARG(extra_arrivals >= 0 && extra_arrivals <= 1024, "extra_arrivals must be 0..1024");
+    EP_CUDA(cudaSetDevice(h->device));
+    EP_CUDA(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    h->bar_extra = (unsigned int)extra_arrivals;
+    return EP_OK;
+}
+
 int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(h && cfg, "null argument");
     EP_CHECK_ARG(cfg->cg_block == 128 || cfg->cg_block == 256 || cfg->cg_block == 512 || cfg->cg_block == 768,
                  "cg_block must be 128, 256, 512 or 768");
-    EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8 || cfg->cg_batch == 16, "cg_batch must be 4, 8 or 16");
+    EP_CHECK_ARG(cfg->cg_batch == 4 || cfg->cg_batch == 8 || cfg->cg_batch == 16 || cfg->cg_batch == kStagedBatch,
+                 "cg_batch must be 4, 8, 16 or 32 (staged)");
+    EP_CHECK_ARG(!(cfg->cg_batch == kStagedBatch && cfg->cg_variant), "cg_batch 32 (staged) needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_variant == 0 || cfg->cg_variant == 1, "cg_variant must be 0 or 1");
     EP_CHECK_ARG(cfg->cg_predict >= 0 && cfg->cg_predict <= 2, "cg_predict must be 0, 1 or 2");
     EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
@@ -1471,11 +1541,11 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     // CG: gather width x CTA size x CTAs per SM (all that fit, or half:
     // fewer CTAs make the grid barrier cheaper)
     const ep_launch_config cg0 = b;
-    for (int nb : {4, 8, 16}) {
+    for (int nb : {4, 8, 16, kStagedBatch}) {
         for (int blk : {128, 256, 512, 768}) {
             int maxper = 0;
-            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant)
-                                         : cg_max_per_sm<float>(blk, &maxper, nb, cg0.cg_variant)))
+            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant, stage_width(h))
+                                         : cg_max_per_sm<float>(blk, &maxper, nb, cg0.cg_variant, stage_width(h))))
                 continue;
             maxper = std::min(maxper, 8);
             for (int per : {maxper, maxper / 2}) {

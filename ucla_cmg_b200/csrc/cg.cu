@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         rb = a.inst_row[inst]; re = a.inst_row[inst + 1];
     }
     GridBarrier *bar = a.bar + inst;
-    const unsigned int nblk = nb;
+    const unsigned int nblk = nb + a.bar_extra;
     const int s_lo = rb / kSlice, s_hi = (re + kSlice - 1) / kSlice;
     const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
     const int nwarps = (nb * (int)blockDim.x) >> 5;
@@ -379,6 +379,10 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         it++;
         rr_last = t[1];
         converged = (t[1] <= stop2);
+        // a non-finite residual (a NaN or inf voltage upstream) cannot
+        // recover: stop now, counted as a failed solve (every block sees the
+        // same total and leaves at the same iteration)
+        if (!isfinite(t[1])) break;
         beta = t[0] / rz;
         rz = t[0];
         R *tmp = pc; pc = pn; pn = tmp;
@@ -442,7 +446,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         rb = a.inst_row[inst]; re = a.inst_row[inst + 1];
     }
     GridBarrier *bar = a.bar + inst;
-    const unsigned int nblk = nb;
+    const unsigned int nblk = nb + a.bar_extra;
     const int s_lo = rb / kSlice, s_hi = (re + kSlice - 1) / kSlice;
     const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
     const int nwarps = (nb * (int)blockDim.x) >> 5;
@@ -543,6 +547,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         it++;
         rr_last = t[2];
         converged = (t[2] <= stop2);
+        if (!isfinite(t[2])) { converged = false; break; }   // as in k_cn_half
         const double gnew = t[0];
         beta = gnew / gamma;
         const double den = t[1] - beta * gnew / alpha;
@@ -563,29 +568,407 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_cn_half_staged: the two-reduction solve of k_cn_half (same recurrences,
+// same order of additions, so the same bits), with the matrix stream of
+// phase A taken off the warps' critical path.  Each warp owns the slices
+// gwarp, gwarp + nwarps, ... of its instance; the bulk-copy engine brings the
+// column indices and A values of the warp's next two slices into a
+// two-stage ring in shared memory (cp.async.bulk, completion counted in
+// bytes on a per-stage mbarrier) while the warp gathers p and z for the
+// current one, so a warp waits on one L2 gather round per slice instead of a
+// chain of index load -> gather load trips.  The stream runs past the end of
+// a sweep into the next iteration's first slices (the matrix does not
+// change), so it overlaps phase B and the barriers too.  The copies carry an
+// L2 evict-first hint: the matrix streams through once per iteration while
+// the vectors it gathers stay in L2.  Slices wider than the ring's stage
+// (wstage columns) are read directly, as in k_cn_half.
+//
+// Every mbarrier wait is bounded (kStagePolls try-waits): a wait that runs
+// out sets the barrier's error word (the grid leaves at the next grid
+// barrier, the host reports EP_ERR_TIMEOUT) and the warp carries on with
+// direct loads.  No exit path leaves a copy in flight: the warp waits
+// (again bounded) for its outstanding stages before it returns.
+constexpr unsigned int kStagePolls = 1u << 22;
+
+__device__ __forceinline__ uint32_t cg_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void stage_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(cg_smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool stage_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}"
+        : "=r"(ok)
+        : "r"(cg_smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// one global -> shared bulk copy completing on bar (16-byte aligned, bytes a
+// multiple of 16: SELL slices start on 128-byte boundaries and span w x 128
+// bytes of indices and w x 32 x sizeof(R) bytes of values)
+__device__ __forceinline__ void stage_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar, uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+        ::"r"(cg_smem_u32(dst)), "l"(src), "r"(bytes), "r"(cg_smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
+// shared-memory bytes of the ring for a CTA of `block` threads
+__host__ __device__ inline size_t stage_bytes_per_warp(int wstage, int rsize) {
+    return (size_t)2 * wstage * kSlice * (4 + rsize);
+}
+__host__ __device__ inline size_t stage_smem_bytes(int block, int wstage, int rsize) {
+    const int nw = block / 32;
+    return (size_t)nw * 2 * sizeof(uint64_t) + 128 + (size_t)nw * stage_bytes_per_warp(wstage, rsize);
+}
+
 template <typename R>
-int cg_max_per_sm(int block, int *per, int batch, int variant) {
-    const void *fn = variant == 1 ? (batch >= 8 ? (const void *)k_cn_half_cg1<R, 8> : (const void *)k_cn_half_cg1<R, 4>)
-                     : batch == 8 ? (const void *)k_cn_half<R, 8>
-                     : batch == 16 ? (const void *)k_cn_half<R, 16>
-                                   : (const void *)k_cn_half<R, 4>;
+struct StageRing {
+    uint64_t *bar;            // 2 mbarriers of this warp
+    int *col0;                // stage k's indices at col0 + k * wstage * 32
+    R *val0;                  // stage k's values at val0 + k * wstage * 32
+    int wstage;
+    int L;                    // slices of this warp per sweep
+    int next;                 // ring position of the next fill
+    uint32_t phase;           // bit k: parity of stage k's next completion
+    uint32_t pend;            // bit k: stage k has a fill in flight (warp-uniform)
+    uint64_t pol;
+};
+
+// fill the stage of ring position pos with its slice, when the slice is
+// narrow enough to be staged (every lane takes the same decision)
+template <typename R>
+__device__ __forceinline__ void stage_fill(StageRing<R> &q, const CGArgs<R> &a, int gwarp, int nwarps, int lane) {
+    if (q.L <= 0) return;
+    const int pos = q.next++;
+    const int k = pos & 1;
+    const int s = gwarp + (pos % q.L) * nwarps;
+    const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+    if (w > q.wstage || w <= 0) return;
+    q.pend |= 1u << k;
+    if (lane == 0) {
+        const uint32_t bc = (uint32_t)w * kSlice * 4u, bv = (uint32_t)w * kSlice * (uint32_t)sizeof(R);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cg_smem_u32(q.bar + k)),
+                     "r"(bc + bv)
+                     : "memory");
+        const int off = k * q.wstage * kSlice;
+        stage_copy(q.col0 + off, a.col + beg, bc, q.bar + k, q.pol);
+        stage_copy(q.val0 + off, a.Aval + beg, bv, q.bar + k, q.pol);
+    }
+}
+
+// wait for stage k's fill (bounded); false when the wait ran out
+template <typename R>
+__device__ __forceinline__ bool stage_wait(StageRing<R> &q, int k) {
+    const uint32_t par = (q.phase >> k) & 1u;
+    bool ok = false;
+    for (unsigned int it = 0; it < kStagePolls; it++)
+        if (stage_try_wait(q.bar + k, par)) { ok = true; break; }
+    ok = __all_sync(0xffffffffu, ok);
+    q.phase ^= 1u << k;
+    q.pend &= ~(1u << k);
+    return ok;
+}
+
+// before the warp leaves: every fill it issued has landed
+template <typename R>
+__device__ __forceinline__ void stage_drain(StageRing<R> &q) {
+    for (int k = 0; k < 2; k++)
+        if (q.pend & (1u << k)) stage_wait(q, k);
+}
+
+// row sums of one staged slice (indices and values in shared memory): NB
+// columns' gathers issued together, the products added in column order (the
+// order of slice_row_sum, so the sums are the same bits)
+template <int NB, typename R, typename F>
+__device__ __forceinline__ R smem_row_sum(const int *col, const R *val, int w, int lane, F gather) {
+    R acc = R(0);
+    for (int k = 0; k < w; k += NB) {
+        int c[NB];
+        R v[NB], g[NB];
+#pragma unroll
+        for (int u = 0; u < NB; u++)
+            if (k + u < w) {
+                c[u] = col[(k + u) * kSlice + lane];
+                v[u] = val[(k + u) * kSlice + lane];
+            }
+#pragma unroll
+        for (int u = 0; u < NB; u++)
+            if (k + u < w) g[u] = gather(c[u]);
+#pragma unroll
+        for (int u = 0; u < NB; u++)
+            if (k + u < w) acc += v[u] * g[u];
+    }
+    return acc;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(const CGArgs<R> a) {
+    extern __shared__ __align__(128) unsigned char cg_sm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int G = gridDim.x;
+    int inst = 0, b0 = 0, nb = G, rb = 0, re = a.n;
+    if (a.ninst > 1) {
+        int lo = 0, hi = a.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.inst_blk[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+        }
+        inst = lo;
+        b0 = a.inst_blk[inst]; nb = a.inst_blk[inst + 1] - b0;
+        rb = a.inst_row[inst]; re = a.inst_row[inst + 1];
+    }
+    GridBarrier *bar = a.bar + inst;
+    const unsigned int nblk = nb + a.bar_extra;
+    const int s_lo = rb / kSlice, s_hi = (re + kSlice - 1) / kSlice;
+    const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
+    const int nwarps = (nb * (int)blockDim.x) >> 5;
+
+    // this warp's ring: mbarriers first, then the stages (128-byte aligned)
+    StageRing<R> q;
+    {
+        const int nw = blockDim.x >> 5;
+        uint64_t *bars = reinterpret_cast<uint64_t *>(cg_sm);
+        unsigned char *base = cg_sm + ((nw * 2 * sizeof(uint64_t) + 127) & ~(size_t)127) +
+                              (size_t)wib * stage_bytes_per_warp(a.wstage, (int)sizeof(R));
+        const size_t cb = (size_t)a.wstage * kSlice * 4, vb = (size_t)a.wstage * kSlice * sizeof(R);
+        q.bar = bars + 2 * wib;
+        q.col0 = reinterpret_cast<int *>(base);
+        q.val0 = reinterpret_cast<R *>(base + 2 * cb);
+        (void)vb;
+        q.wstage = a.wstage;
+        q.L = gwarp < s_hi ? (s_hi - gwarp + nwarps - 1) / nwarps : 0;
+        q.next = 0;
+        q.phase = 0;
+        q.pend = 0;
+        q.pol = l2_evict_first_policy();
+        if (lane == 0) {
+            stage_mbar_init(q.bar);
+            stage_mbar_init(q.bar + 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+    }
+    // the first two slices start streaming under the prologue
+    stage_fill(q, a, gwarp, nwarps, lane);
+    stage_fill(q, a, gwarp, nwarps, lane);
+    int cons = 0;                             // ring position of the next slice to consume
+
+    // ---- prologue: as k_cn_half ----
+    const bool pred = a.delta != nullptr;
+    const bool lin = a.delta_prev != nullptr;
+    {
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+            R ax = R(0), bx = R(0), ad = R(0);
+            slice_ab_sums<4>(a.col, a.Aval, a.Bval, a.x, beg, w, lane, pred, [&](int c) {
+                return lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c];
+            }, ax, bx, ad);
+            if (row >= rb && row < re) {
+                const R rref = bx - ax;
+                const R r = pred ? rref - ad : rref;
+                const R z = __ldg(a.dinv + row) * r;
+                a.r[row] = r;
+                a.z[row] = z;
+                a.p0[row] = R(0);
+                if (pred) a.vin[row] = a.x[row];
+                v[0] += (double)r * (double)z;
+                v[1] += (double)r * (double)r;
+                v[2] += (double)bx * (double)bx;
+                v[3] += (double)rref * (double)rref;
+            }
+        }
+        block_reduce_store<4>(v, a.partial + 6 * G, G);
+    }
+    if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+    double rz, rr_start, bb, rr0;
+    {
+        double t[4];
+        grid_total<4>(a.partial + 6 * G, G, b0, nb, t);
+        rz = t[0]; rr_start = t[1]; bb = t[2]; rr0 = t[3];
+    }
+    const double floor2 = a.floor_rel * a.floor_rel * bb;
+    const double stop2 = fmax(a.tol * a.tol * rr0, floor2);
+    double beta = 0.0;
+    int it = 0;
+    bool converged = (rr_start <= stop2);
+    double rr_last = rr_start;
+    R *pc = a.p0, *pn = a.p1;
+    while (!converged && it < a.maxit) {
+        // ---- phase A: q = A p', p' = z + beta p, from the staged slices ----
+        {
+            double v[1] = {0.0};
+            const R bR = (R)beta;
+            const R *pcc = pc;
+            auto gat = [&](int c) { return pdir_z(ldcg(a.z + c), bR, ldcg(pcc + c)); };
+            for (int s = gwarp; s < s_hi; s += nwarps, cons++) {
+                const int row = s * kSlice + lane;
+                const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
+                const int k = cons & 1;
+                R qv;
+                bool staged = w <= q.wstage && w > 0;
+                if (staged && !stage_wait(q, k)) {
+                    if (lane == 0) atomicExch(&bar->err, 1u);
+                    staged = false;
+                }
+                if (staged) {
+                    const int off = k * q.wstage * kSlice;
+                    qv = smem_row_sum<8>(q.col0 + off, q.val0 + off, w, lane, gat);
+                    __syncwarp();                 // every lane is done with stage k
+                } else {
+                    qv = slice_row_sum<8>(a.col, a.Aval, beg, w, lane, gat);
+                }
+                stage_fill(q, a, gwarp, nwarps, lane);   // refill stage k two slices ahead
+                if (row >= rb && row < re) {
+                    const R pi = pdir_z(a.z[row], bR, ldcg(pc + row));
+                    pn[row] = pi;
+                    a.q[row] = qv;
+                    v[0] += (double)pi * (double)qv;
+                }
+            }
+            block_reduce_store<1>(v, a.partial + 3 * G, G);
+        }
+        if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+        double pq;
+        {
+            double t[1];
+            grid_total<1>(a.partial + 3 * G, G, b0, nb, t);
+            pq = t[0];
+        }
+        const double alpha = rz / pq;
+        // ---- phase B: as k_cn_half ----
+        {
+            double v[2] = {0.0, 0.0};
+            const R aR = (R)alpha;
+            for (int s = gwarp; s < s_hi; s += 2 * nwarps) {
+                const int row = s * kSlice + lane, row2 = row + nwarps * kSlice;
+                const bool on = row >= rb && row < re;
+                const bool on2 = s + nwarps < s_hi && row2 >= rb && row2 < re;
+                R pi = R(0), xi = R(0), ri = R(0), qi = R(0), di = R(0);
+                R pi2 = R(0), xi2 = R(0), ri2 = R(0), qi2 = R(0), di2 = R(0);
+                if (on) { pi = pn[row]; xi = a.x[row]; ri = a.r[row]; qi = a.q[row]; di = __ldg(a.dinv + row); }
+                if (on2) { pi2 = pn[row2]; xi2 = a.x[row2]; ri2 = a.r[row2]; qi2 = a.q[row2]; di2 = __ldg(a.dinv + row2); }
+                if (on) {
+                    a.x[row] = xi + aR * pi;
+                    const R r = ri - aR * qi;
+                    a.r[row] = r;
+                    const R z = di * r;
+                    a.z[row] = z;
+                    v[0] += (double)r * (double)z;
+                    v[1] += (double)r * (double)r;
+                }
+                if (on2) {
+                    a.x[row2] = xi2 + aR * pi2;
+                    const R r = ri2 - aR * qi2;
+                    a.r[row2] = r;
+                    const R z = di2 * r;
+                    a.z[row2] = z;
+                    v[0] += (double)r * (double)z;
+                    v[1] += (double)r * (double)r;
+                }
+            }
+            block_reduce_store<2>(v, a.partial, G);
+        }
+        if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+        double t[2];
+        grid_total<2>(a.partial, G, b0, nb, t);
+        it++;
+        rr_last = t[1];
+        converged = (t[1] <= stop2);
+        if (!isfinite(t[1])) break;
+        beta = t[0] / rz;
+        rz = t[0];
+        R *tmp = pc; pc = pn; pn = tmp;
+    }
+    stage_drain(q);                           // the fills that ran ahead into the next sweep
+    if (pred) {
+        for (int s = gwarp; s < s_hi; s += nwarps) {
+            const int row = s * kSlice + lane;
+            if (row >= rb && row < re) {
+                const R d = a.delta[row];
+                const R xf = a.x[row] + (lin ? R(2) * d - a.delta_prev[row] : d);
+                a.x[row] = xf;
+                if (lin) a.delta_prev[row] = d;
+                a.delta[row] = xf - a.vin[row];
+            }
+        }
+    }
+    if ((int)blockIdx.x == b0 && threadIdx.x == 0) {
+        atomicAdd(a.iters_total, (unsigned long long)it);
+        atomicMax(a.iters_max, (unsigned int)it);
+        if (!converged) atomicAdd(a.fails, 1u);
+        if (a.last) {
+            a.last[2 * inst] = (double)it;
+            a.last[2 * inst + 1] = rr0 > 0.0 ? sqrt(rr_last / rr0) : 0.0;
+        }
+    }
+}
+
+// the kernel of a (gather width, variant) choice and its dynamic shared
+// memory; cg_batch kStagedBatch selects k_cn_half_staged (ring of wstage
+// columns per stage)
+// (set_attr: allow the staged kernel the largest ring any handle can ask
+// for -- 256 threads, kStageMaxW columns -- once, from the planning path,
+// never during a stream capture; the attribute only caps the request)
+template <typename R>
+static int cg_kernel(int block, int batch, int variant, int wstage, const void **fn, size_t *smem,
+                     bool set_attr) {
+    *smem = 0;
+    if (batch == kStagedBatch) {
+        if (variant != 0) { set_error("the staged CG runs the two-reduction recurrences only"); return EP_ERR_ARG; }
+        if (wstage < 1 || wstage > kStageMaxW) { set_error("staged CG: stage width %d out of range", wstage); return EP_ERR_ARG; }
+        *fn = (const void *)k_cn_half_staged<R>;
+        *smem = stage_smem_bytes(block, wstage, (int)sizeof(R));
+        if (set_attr)
+            EP_CUDA(cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)stage_smem_bytes(256, kStageMaxW, (int)sizeof(R))));
+        return EP_OK;
+    }
+    *fn = variant == 1 ? (batch >= 8 ? (const void *)k_cn_half_cg1<R, 8> : (const void *)k_cn_half_cg1<R, 4>)
+          : batch == 8 ? (const void *)k_cn_half<R, 8>
+          : batch == 16 ? (const void *)k_cn_half<R, 16>
+                        : (const void *)k_cn_half<R, 4>;
+    return EP_OK;
+}
+
+template <typename R>
+int cg_max_per_sm(int block, int *per, int batch, int variant, int wstage) {
+    const void *fn = nullptr;
+    size_t smem = 0;
+    int rc = cg_kernel<R>(block, batch, variant, wstage, &fn, &smem, true);
+    if (rc) return rc;
     cudaFuncAttributes fa;
     EP_CUDA(cudaFuncGetAttributes(&fa, fn));
     if (block > fa.maxThreadsPerBlock) {
         set_error("CG gather width %d takes at most %d threads per CTA (asked %d)", batch, fa.maxThreadsPerBlock, block);
         return EP_ERR_ARG;
     }
-    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, fn, block, 0));
+    EP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, fn, block, smem));
     if (*per < 1) { set_error("CG kernel cannot be resident with %d threads per CTA", block); return EP_ERR_CUDA; }
     return EP_OK;
 }
 
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm, int batch, int variant) {
+int cg_grid_size(int block, int *grid, int per_sm, int batch, int variant, int wstage) {
     int dev = 0, nsm = 0, per = 0;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int rc = cg_max_per_sm<R>(block, &per, batch, variant);
+    int rc = cg_max_per_sm<R>(block, &per, batch, variant, wstage);
     if (rc) return rc;
     if (per_sm > 0 && per_sm < per) per = per_sm;
     *grid = nsm * per;
@@ -604,7 +987,14 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (variant == 1) {
+    if (batch == kStagedBatch) {
+        const void *fn = nullptr;
+        size_t smem = 0;
+        int rc = cg_kernel<R>(block, batch, variant, a.wstage, &fn, &smem, false);
+        if (rc) return rc;
+        cfg.dynamicSmemBytes = smem;
+        EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_staged<R>, a));
+    } else if (variant == 1) {
         if (!a.r1 || !a.w0 || !a.w1 || !a.s0 || !a.s1) { set_error("single-reduction CG needs its vectors"); return EP_ERR_ARG; }
         if (batch >= 8) EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 8>, a));
         else EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_cg1<R, 4>, a));
@@ -620,10 +1010,10 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch
 
 template int launch_cg<float>(const CGArgs<float> &, int, int, cudaStream_t, int, int);
 template int launch_cg<double>(const CGArgs<double> &, int, int, cudaStream_t, int, int);
-template int cg_grid_size<float>(int, int *, int, int, int);
-template int cg_grid_size<double>(int, int *, int, int, int);
-template int cg_max_per_sm<float>(int, int *, int, int);
-template int cg_max_per_sm<double>(int, int *, int, int);
+template int cg_grid_size<float>(int, int *, int, int, int, int);
+template int cg_grid_size<double>(int, int *, int, int, int, int);
+template int cg_max_per_sm<float>(int, int *, int, int, int);
+template int cg_max_per_sm<double>(int, int *, int, int, int);
 
 // ---------------------------------------------------------------------------
 // One forward-Euler diffusion sub-step of the explicit scheme

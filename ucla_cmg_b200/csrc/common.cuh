@@ -49,12 +49,15 @@ struct DevStatus {
 
 // Bounded sense-reversing grid barrier for cooperative (co-resident) grids.
 // Returns false when the wait gave up; the caller must then leave the kernel
-// (every block reaches the same conclusion through *err).
+// (every block reaches the same conclusion through *err).  `limit` caps the
+// polls of one wait (0: kGridPolls, a few seconds); a wait that runs out
+// sets err, which the host reads as EP_ERR_TIMEOUT and then clears.
+constexpr unsigned int kGridPolls = 1u << 24;
 struct GridBarrier {
     unsigned int count;
     unsigned int gen;
     unsigned int err;
-    unsigned int pad;
+    unsigned int limit;
 };
 
 __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks) {
@@ -65,6 +68,8 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks) 
         int ok = 1;
         volatile unsigned int *vgen = &b->gen;
         volatile unsigned int *verr = &b->err;
+        const unsigned int lim = *(volatile unsigned int *)&b->limit;
+        const unsigned int max_polls = lim ? lim : kGridPolls;
         const unsigned int g = *vgen;
         __threadfence();
         const unsigned int arrived = atomicAdd(&b->count, 1u);
@@ -73,11 +78,11 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks) 
             __threadfence();
             atomicAdd(&b->gen, 1u);
         } else {
-            // ~ 2^24 polls with a short sleep: seconds, then give up
+            // at most max_polls polls with a short sleep, then give up
             unsigned int polls = 0;
             while (*vgen == g) {
                 if (*verr) { ok = 0; break; }
-                if (++polls > (1u << 24)) { atomicExch(&b->err, 1u); ok = 0; break; }
+                if (++polls > max_polls) { atomicExch(&b->err, 1u); ok = 0; break; }
                 __nanosleep(64);
             }
         }

@@ -141,7 +141,13 @@ int bar_mats(const double *xyz, const HostCables &cb, double Cm, std::vector<Bar
         for (int k = 0; k < 3; k++) ang[k] = xyz[3 * (size_t)v[1] + k] - xyz[3 * (size_t)v[0] + k];
         len = std::sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
         for (int k = 0; k < 3; k++) ang[k] /= len;
-        if (listed || (carried && cb.orient_sticky)) {
+        if (cb.bar_orient_node) {
+            const int o = cb.bar_orient_node[e];
+            if (o >= 0) {
+                for (int k = 0; k < 3; k++) ang[k] = cb.orient[4 * (size_t)o + k];
+                len = cb.orient[4 * (size_t)o + 3];
+            }
+        } else if (listed || (carried && cb.orient_sticky)) {
             for (int k = 0; k < 3; k++) ang[k] = carry[k];
             len = carry[3];
         }

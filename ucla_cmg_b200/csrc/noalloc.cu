@@ -19,10 +19,13 @@
 //   library holds it until the process exits;
 // * every call shares the one array, so calls that overlap on the GPU (two
 //   streams, two host threads) race -- serialise them;
-// * the first call on a device looks up the array's device address there
-//   (cudaGetSymbolAddress); make that first call before any stream capture.
-#include <mutex>
-
+// * each call looks up the array's device address on the current device
+//   (cudaGetSymbolAddress): host code only holds a stand-in for the symbol,
+//   and an address kept from an earlier call would be stale after a
+//   cudaDeviceReset;
+// * the call waits on `stream` for its own results before it returns; on a
+//   stream in capture mode it returns EP_ERR_ARG before touching the stream,
+//   so the caller's capture stays intact.
 #include "kernels.cuh"
 
 namespace ep {
@@ -38,24 +41,20 @@ constexpr size_t kScratchBytes = 5 * kVecBytes                            // r, 
 static __device__ __align__(256) unsigned char g_cg_scratch[kScratchBytes];
 
 namespace {
-std::mutex g_mu;
-void *g_addr[64] = {nullptr};                            // per device
 
+// the device address of g_cg_scratch on the current device, looked up anew
+// on every call (cheap next to a persistent CG launch, and never stale)
 int scratch_address(void **out) {
     int dev = 0;
     EP_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) { set_error("device index %d out of range", dev); return EP_ERR_ARG; }
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_scratch);
-        if (e != cudaSuccess) {
-            set_error("cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(e));
-            return EP_ERR_CUDA;
-        }
-        g_addr[dev] = p;
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_scratch);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(e));
+        return EP_ERR_CUDA;
     }
-    *out = g_addr[dev];
+    *out = p;
     return EP_OK;
 }
 
@@ -120,10 +119,17 @@ extern "C" int ep_cn_half_step_noalloc(int32_t precision, int32_t n, int32_t nsl
     }
     EP_CHECK_ARG(nslices == (n + kSlice - 1) / kSlice, "nslices must be ceil(n / 32)");
     EP_CHECK_ARG(slice_ptr && col && Aval && Bval && dinv && x, "null device pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    EP_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("ep_cn_half_step_noalloc: the stream is being captured; the call waits for its "
+                  "results on the stream and would invalidate the capture");
+        return EP_ERR_ARG;
+    }
     void *base = nullptr;
     int rc = scratch_address(&base);
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
     if (precision == EP_FP64)
         return run<double>((unsigned char *)base, n, nslices, slice_ptr, col, (const double *)Aval,
                            (const double *)Bval, (const double *)dinv, (double *)x, cg_tol, cg_maxit, s,

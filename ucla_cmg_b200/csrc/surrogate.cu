@@ -143,10 +143,13 @@ __device__ __forceinline__ void issue_layer(uint32_t d, uint32_t sA, uint32_t sW
     umma_commit(bar);
 }
 
-// block-uniform bounded wait for the next commit of this CTA
-__device__ __forceinline__ bool wait_commit(uint64_t *bar, uint32_t &phase, unsigned int *err) {
+// block-uniform bounded wait for the next commit of this CTA: at most
+// `polls` try-waits (0: kMbarPolls)
+constexpr unsigned int kMbarPolls = 1u << 22;
+__device__ __forceinline__ bool wait_commit(uint64_t *bar, uint32_t &phase, unsigned int *err, unsigned int polls) {
     bool ok = false;
-    for (int it = 0; it < (1 << 22); it++)
+    const unsigned int lim = polls ? polls : kMbarPolls;
+    for (unsigned int it = 0; it < lim; it++)
         if (mbar_try_wait(bar, phase)) { ok = true; break; }
     phase ^= 1u;
     const int bad = __syncthreads_or(ok ? 0 : 1);
@@ -328,7 +331,7 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
                 tc_fence_after();
                 issue_layer(d_hid, sA, sW[l], l == 0 ? SG_KIN : SG_H, SG_H, bar);
             }
-            ok = wait_commit(bar, phase, a.err);
+            ok = wait_commit(bar, phase, a.err, a.mbar_polls);
             if (ok) hidden_epilogue(d_hid + lane_off, bias[l], A, row, half);
         }
         if (!ok) break;
@@ -340,7 +343,7 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
             tc_fence_after();
             issue_layer(d_out, sA, sW4, SG_H, SG_NOUT, bar);
         }
-        if (!wait_commit(bar, phase, a.err)) break;
+        if (!wait_commit(bar, phase, a.err, a.mbar_polls)) break;
         if (!owner) {
             // the next tile's rows (its layer-1 MMA waits for the barrier at
             // the top of the next iteration)

@@ -63,6 +63,7 @@ struct SurrogateArgs {
     int *fallback_list, *fallback_count;
     DevStatus *status;
     unsigned int *err;                  // set when an in-kernel wait gave up
+    unsigned int mbar_polls;            // polls of one completion wait (0: kMbarPolls)
     // raw mode (tests): X [n x 32] normalised inputs -> Y [n x 32] raw outputs
     const float *rawX;
     float *rawY;

@@ -256,6 +256,7 @@ def cable_setup(cfg, node_type):
     if not len(cab["bars"]):
         return None
     return dict(bars=cab["bars"], bar_fibers=cab["fibers"], lv=cab["lv"], angle=cab["angle"],
+                bar_angle_node=cab["angle_node"],
                 radius=cfg["radius"], Dp=tuple(cfg["Dp"]), DpLeft=tuple(cfg["Dp"]), quad_order=cfg["quad_order"])
 
 

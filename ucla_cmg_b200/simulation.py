@@ -224,10 +224,22 @@ class Monodomain:
 
     # ---- time stepping ----
     def step(self, n_steps=1):
+        """Advance n_steps; returns the step statistics.  On an error status
+        (EP_ERR_NAN, EP_ERR_TIMEOUT, ...) raises EPError, with the call's
+        statistics still in ``last_stats``."""
         st = capi.StepStats()
-        check(capi.lib().ep_step(self._h, int(n_steps), C.byref(st)))
+        rc = capi.lib().ep_step(self._h, int(n_steps), C.byref(st))
         self.last_stats = st.as_dict()
+        check(rc)
         return self.last_stats
+
+    def set_wait_limits(self, grid_polls=0, mbar_polls=0):
+        """Poll limits of the in-kernel waits (0: the built-in ones)."""
+        check(capi.lib().ep_set_wait_limits(self._h, int(grid_polls), int(mbar_polls)))
+
+    def test_hold_barrier(self, extra_arrivals):
+        """Test hook: the CG barrier waits for arrivals that never come."""
+        check(capi.lib().ep_test_hold_barrier(self._h, int(extra_arrivals)))
 
     def diffusion_half_step(self):
         """One CN half diffusion step on the current V; returns (CG
@@ -341,12 +353,15 @@ def batch_plan(inst_row, grid):
 
 def assemble_operators(mesh, D, dt, Cm=1.0, scheme=capi.SCHEME_CN, smoothing_alpha=0.0, bars=None,
                        Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, bar_fibers=None, lv=None, quad_order=2,
-                       angle=None, angle_sticky=True):
+                       angle=None, angle_sticky=True, bar_angle_node=None):
     """The FP64 operators ep_create builds, assembled on the host only
     (ep_assemble_operators; no GPU): scipy CSR matrices A and B and the
     lumped capacitance C_L.  ``bars`` (nb x 2, zero-based) adds 2-node
     Purkinje cables after the tets; ``angle`` maps a zero-based node to
-    (dx, dy, dz, length) as in a .angle file."""
+    (dx, dy, dz, length) as in a .angle file; ``bar_angle_node`` (per cable,
+    the node whose row overrides it or -1, from
+    :func:`ucla_cmg_b200.voomep_io.bar_angle_nodes` over the .ele order)
+    replaces the bars-only sticky rule."""
     import scipy.sparse as sp
     md, _, keep = _instance_descs(mesh, capi.TUSSCHER, D, Cm, None, None, None, None, 0.0, 0, 0, 0, None)
     sd = _solver_desc(dt, dt, 1e-7, 1000, smoothing_alpha, capi.FP64, 0.0, 0, -40.0, scheme)
@@ -373,6 +388,10 @@ def assemble_operators(mesh, D, dt, Cm=1.0, scheme=capi.SCHEME_CN, smoothing_alp
             cd.n_angle = len(keep["an"])
             cd.angle_nodes = ptr(keep["an"], C.POINTER(C.c_int32))
             cd.angle = ptr(keep["ad"])
+            if bar_angle_node is not None:
+                row = {int(v): k for k, v in enumerate(keep["an"])}
+                keep["ba"] = np.array([row[int(v)] if v >= 0 else -1 for v in bar_angle_node], dtype=np.int32)
+                cd.bar_angle = ptr(keep["ba"], C.POINTER(C.c_int32))
     nnz = C.c_int64(0)
     L = capi.lib()
     cdp = C.byref(cd) if cd is not None else None

@@ -59,22 +59,45 @@ def read_ele(path):
     return np.array(tets, dtype=np.int32).reshape(-1, 4), np.array(which, dtype=np.int64), other
 
 
-def read_cables(base, node_type=None):
+def bar_angle_nodes(first_nodes, is_bar, angle, sticky=True):
+    """Per cable, the node whose .angle row overrides its direction and
+    length, or -1 -- MixedMesh3D::Compute's rule over the whole .ele order
+    (MixedMesh3D.cc:30-34, 78-87): every element whose first node is listed,
+    a tet as much as a cable, switches the override on with that node's row,
+    and it stays on for every later cable (``sticky``; False applies a row
+    to the cable that starts at its node only).  ``first_nodes``: each
+    element's first node (zero-based) in .ele order; ``is_bar``: which
+    elements are cables."""
+    out, cur = [], -1
+    for v, b in zip(first_nodes, is_bar):
+        v = int(v)
+        if v in angle:
+            cur = v
+        if b:
+            out.append(cur if sticky else (v if v in angle else -1))
+    return np.array(out, dtype=np.int32)
+
+
+def read_cables(base, node_type=None, angle_sticky=True):
     """The 2-node Purkinje cables of a mixed mesh ``base``: dict with
     ``bars`` [nb x 2] zero-based in .ele order, ``fibers`` [nb x 9] or None
     (from .fibers, in .ele order), ``lv`` [nb] (1 where either node has
     tissue type 11: the left-ventricular Purkinje diffusion,
-    CardiacBody.cc:107-110) and ``angle`` {zero-based node: (dx, dy, dz,
-    length)} from .angle (empty if absent)."""
+    CardiacBody.cc:107-110), ``angle`` {zero-based node: (dx, dy, dz,
+    length)} from .angle (empty if absent) and ``angle_node`` [nb], the node
+    whose .angle row overrides each cable (-1: none) by the reference's
+    element-order rule (:func:`bar_angle_nodes`)."""
     with open(base + ".ele") as f:
         tok = f.read().split()
     ne = int(tok[0])
     pos = 3
-    bars, which = [], []
+    bars, which, first, isbar = [], [], [], []
     for e in range(ne):
         k = int(tok[pos + 1])
         conn = tok[pos + 2:pos + 2 + k]
         pos += 2 + k
+        first.append(int(conn[0]) - 1)
+        isbar.append(k == 2)
         if k == 2:
             bars.append([int(c) - 1 for c in conn])
             which.append(e)
@@ -91,7 +114,8 @@ def read_cables(base, node_type=None):
             a = f.read().split()
         for k in range(len(a) // 5):
             angle[int(a[5 * k]) - 1] = tuple(float(v) for v in a[5 * k + 1:5 * k + 5])
-    return {"bars": bars, "fibers": fib, "lv": lv, "angle": angle}
+    return {"bars": bars, "fibers": fib, "lv": lv, "angle": angle,
+            "angle_node": bar_angle_nodes(first, isbar, angle, angle_sticky)}
 
 
 def read_fibers(path, n_elems):
