@@ -29,7 +29,7 @@ def test_every_header_function_bound():
 
 def test_host_only_entry_points():
     L = capi.lib()
-    assert L.ep_version() == 2
+    assert L.ep_version() == 3
     assert L.ep_model_nstate(capi.TUSSCHER) == 19
     assert L.ep_model_nstate(capi.MAHAJAN) == 26
     assert L.ep_model_nstate(capi.LUORUDY) == 8
