@@ -42,9 +42,9 @@ extern "C" {
 #define EP_MAHAJAN          3
 #define EP_MAHAJAN_FAIL     4
 /* not in CellModelType: the Purkinje cell CardiacBody::New gives every .purk
- * node (Body/CardiacBody.cc:982-1101; IonicModel/Purkinje.cc).  Plugin level
- * (ep_ionic_step, ep_ionic_phase) only: ep_create rejects it until mixed
- * tissues (a tissue model plus Purkinje cells on cable nodes) are built. */
+ * node (Body/CardiacBody.cc:982-1101; IonicModel/Purkinje.cc): at plugin
+ * level (ep_ionic_step, ep_ionic_phase) and on the .purk nodes of mixed
+ * tissues (ep_create_mixed); ep_create rejects it as a tissue model. */
 #define EP_PURKINJE         5
 
 /* ---- arithmetic of the ionic update and the SpMV ---- */
@@ -281,6 +281,23 @@ typedef struct ep_cables_desc {
      * given, angle_sticky is not consulted. */
     const int32_t *bar_angle;
 } ep_cables_desc;
+
+/* Mixed tissues: CardiacBody::New on a MIX3D mesh (Body/CardiacBody.cc:
+ * 982-1101).  The 2-node cables join the tets in the operators
+ * (MixedMesh3D.cc:62-108, CardiacBody.cc:100-187); every node of purk_nodes
+ * (the .purk file; ids as mesh->one_based says) carries the Purkinje cell
+ * (IonicModel/Purkinje.cc, defaults of SetUpPurkinjeParameters) with its own
+ * 21 stored states, constants and Xi, every other node the tissue model of
+ * `tissue`, and the shared V starts from each cell's own voltage.  States
+ * (ep_get/set_states) come in rows of ep_num_states(h) = max(tissue nstate,
+ * 22) values: a Purkinje node's row holds its 22 (V first), a tissue node's
+ * its model's, zero-padded; restart files keep each node's own nVar, as the
+ * reference writes them (EPSolver.cc:155-176).  The pseudo-ECG integrates
+ * over the cables too, as ComputeECG does on a MIX3D mesh (tissue D along
+ * each cable's fibres, radius 0.0275 cm).  FP64 and FP32 only. */
+int  ep_create_mixed(const ep_mesh_desc *mesh, const struct ep_cables_desc *cables, int32_t n_purk,
+                     const int32_t *purk_nodes, const ep_model_desc *tissue, const ep_solver_desc *solver,
+                     int device, ep_handle **out);
 
 /* The FP64 operators ep_create assembles for the solver's scheme, on the
  * host only (no GPU, no device memory): CSR of n_nodes rows, zero-based

@@ -1102,6 +1102,57 @@ static int tet_triplets(const double *xyz, int m, const int *tets, const double 
  * geometry and quadrature, CardiacBody.cc:100-187 for D, K, M and
  * CardiacBody.cc:32-67 for the capacitance): the 4 entries of every bar in
  * element order after the tets' entries. */
+/* Direction (unit) and length of every cable in order, with the .angle
+ * overrides of MixedMesh3D::Compute (MixedMesh3D.cc:30-34, 78-87): per cable
+ * from bar_orient_node when the caller resolved them over the whole element
+ * order, else the cables-only rule (sticky or not).  ang[3 nb], mag[nb]. */
+static void bar_frames(const double *xyz, const epo_cables *cb, double *ang_out, double *mag_out)
+{
+    int pmj = 0;
+    double pmj_data[4] = {0., 0., 0., 0.};
+    for (int e = 0; e < cb->nb; e++) {
+        const int *v = cb->bars + 2 * (size_t)e;
+        if (cb->orient_has && cb->orient_has[v[0]]) {
+            pmj = 1;
+            for (int k = 0; k < 4; k++) pmj_data[k] = cb->orient[4 * (size_t)v[0] + k];
+        }
+        double ang[3], mag;
+        for (int k = 0; k < 3; k++) ang[k] = xyz[3 * v[1] + k] - xyz[3 * v[0] + k];
+        mag = sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
+        for (int k = 0; k < 3; k++) ang[k] /= mag;
+        if (cb->bar_orient_node) {
+            const int o = cb->bar_orient_node[e];
+            if (o >= 0) {
+                for (int k = 0; k < 3; k++) ang[k] = cb->orient[4 * (size_t)o + k];
+                mag = cb->orient[4 * (size_t)o + 3];
+            }
+        } else if (pmj && cb->orient_sticky) {
+            for (int k = 0; k < 3; k++) ang[k] = pmj_data[k];
+            mag = pmj_data[3];
+        } else if (cb->orient_has && cb->orient_has[v[0]]) {
+            for (int k = 0; k < 3; k++) ang[k] = pmj_data[k];
+            mag = pmj_data[3];
+        }
+        for (int k = 0; k < 3; k++) ang_out[3 * (size_t)e + k] = ang[k];
+        mag_out[e] = mag;
+    }
+}
+
+/* LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc); -1 for
+ * an order the reference does not have */
+static int bar_quadrature(int quad_order, double *qx, double *qw)
+{
+    const int qord = 2 * (quad_order > 0 ? quad_order : 2) - 1;
+    if (qord == 1) { qx[0] = 0.0; qw[0] = 2.0; return 1; }
+    if (qord == 3) { qx[0] = -0.577350269189626; qx[1] = 0.577350269189626; qw[0] = qw[1] = 1.0; return 2; }
+    if (qord == 5) {
+        qx[0] = -0.774596669241483; qx[1] = 0.0; qx[2] = 0.774596669241483;
+        qw[0] = qw[2] = 5.0 / 9.0; qw[1] = 8.0 / 9.0;
+        return 3;
+    }
+    return -1;
+}
+
 static int bar_triplets(const double *xyz, const epo_cables *cb, double Cm, trip_t *t, double *CL)
 {
     /* LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc) */
@@ -1439,6 +1490,52 @@ void epo_ecg_weights(int n, const double *xyz, int m, const int *tets,
                 W[(size_t)k * n + v[a]] += dN[a][0] * DG[0] + dN[a][1] * DG[1] + dN[a][2] * DG[2];
         }
     }
+}
+
+/* The cables' share of the per-node ECG weights, added to W: ComputeECG.h's
+ * sums over the 2-node elements of a MIX3D mesh (they are not skipped there,
+ * ComputeECG.h:47-50, 107-110): quadrature points of MixedMesh3D::Compute
+ * placed by the shape functions on the cable's own nodes (ComputeECG.h:
+ * 65-70), grad N = -+ ang / length, weight w_q pi r^2 length, and the tissue
+ * D along the cable's fibre frame, or D[0] I without fibres
+ * (computeDiffusionTensor applies Diff to every element, ComputeECG.h:
+ * 92-136; cables->Dp is not used here).  ComputeECG fixes the radius at
+ * 0.0275 cm (ComputeECG.cc:75); the caller passes it in cables->radius. */
+int epo_ecg_weights_cables(int n, const double *xyz, const epo_cables *cb, const double D[3], int ne,
+                           const double *electrodes, double *W)
+{
+    double qx[3], qw[3];
+    const int nq = bar_quadrature(cb->quad_order, qx, qw);
+    if (nq < 0) return -2;
+    double *ang = (double *)malloc(sizeof(double) * 3 * (size_t)(cb->nb > 0 ? cb->nb : 1));
+    double *mag = (double *)malloc(sizeof(double) * (size_t)(cb->nb > 0 ? cb->nb : 1));
+    bar_frames(xyz, cb, ang, mag);
+    for (int e = 0; e < cb->nb; e++) {
+        const int *v = cb->bars + 2 * (size_t)e;
+        double De[3][3];
+        elem_tensor(cb->fibers ? cb->fibers + 9 * (size_t)e : NULL, D, De);
+        const double *a = ang + 3 * (size_t)e;
+        const double dx[2][3] = {{-a[0] / mag[e], -a[1] / mag[e], -a[2] / mag[e]},
+                                 {a[0] / mag[e], a[1] / mag[e], a[2] / mag[e]}};
+        for (int k = 0; k < ne; k++) {
+            double G[3] = {0, 0, 0};
+            for (int q = 0; q < nq; q++) {
+                const double N0 = 0.5 * (1. - qx[q]), N1 = 0.5 * (1. + qx[q]);
+                double pos[3], g[3];
+                for (int d = 0; d < 3; d++) pos[d] = N0 * xyz[3 * v[0] + d] + N1 * xyz[3 * v[1] + d];
+                grad_one_by_r(pos, electrodes + 3 * k, g);
+                const double w = qw[q] * EPO_PI * (cb->radius * cb->radius) * mag[e];
+                for (int d = 0; d < 3; d++) G[d] += g[d] * w;
+            }
+            double DG[3];
+            for (int r = 0; r < 3; r++) DG[r] = De[r][0] * G[0] + De[r][1] * G[1] + De[r][2] * G[2];
+            for (int b = 0; b < 2; b++)
+                W[(size_t)k * n + v[b]] += dx[b][0] * DG[0] + dx[b][1] * DG[1] + dx[b][2] * DG[2];
+        }
+    }
+    free(ang);
+    free(mag);
+    return 0;
 }
 
 /* ====================================================================== */

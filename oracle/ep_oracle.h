@@ -163,6 +163,10 @@ void epo_ecg_elementwise(int n, const double *xyz, int m, const int *tets,
                          const double *fibers, const double D[3], int ne,
                          const double *electrodes, const double *V, double *ecg);
 /* Per-node weights W (ne * n) with ECG_k = sum_i W[k*n+i] V[i]. */
+/* the 2-node cables' share of the weights, added to W (ComputeECG on a MIX3D
+ * mesh; radius from cables->radius, ComputeECG uses 0.0275) */
+int  epo_ecg_weights_cables(int n, const double *xyz, const epo_cables *cables, const double D[3], int ne,
+                            const double *electrodes, double *W);
 void epo_ecg_weights(int n, const double *xyz, int m, const int *tets,
                      const double *fibers, const double D[3], int ne,
                      const double *electrodes, double *W);

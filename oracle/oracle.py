@@ -100,6 +100,7 @@ def lib():
         L.epo_pcg.argtypes = [C.POINTER(_Csr), dp, dp, dp, C.c_double, C.c_int, C.c_int, dp]
         L.epo_ecg_elementwise.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_int, dp, dp, dp]
         L.epo_ecg_weights.argtypes = [C.c_int, dp, C.c_int, ip, dp, dp, C.c_int, dp, dp]
+        L.epo_ecg_weights_cables.argtypes = [C.c_int, dp, C.POINTER(_Cables), dp, C.c_int, dp, dp]
         L.epo_sim_init.argtypes = [C.POINTER(_Sim), C.POINTER(_Csr), C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
                                    C.c_void_p]
@@ -578,15 +579,22 @@ def ecg_elementwise(xyz, tets, fibers, D, electrodes, V):
     return out
 
 
-def ecg_weights(xyz, tets, fibers, D, electrodes):
+def ecg_weights(xyz, tets, fibers, D, electrodes, cables=None):
+    """Per-node ECG weights W (ECG = W V); ``cables`` (a :class:`Cables`,
+    its radius as ComputeECG sets it, 0.0275) adds the 2-node elements of a
+    MIX3D mesh with the tissue D."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float64)
-    tets = np.ascontiguousarray(tets, dtype=np.int32)
+    tets = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
     fib = None if fibers is None else np.ascontiguousarray(fibers, dtype=np.float64)
     D = np.ascontiguousarray(D, dtype=np.float64)
-    el = np.ascontiguousarray(electrodes, dtype=np.float64)
+    el = np.ascontiguousarray(electrodes, dtype=np.float64).reshape(-1, 3)
     W = np.zeros((len(el), len(xyz)))
     lib().epo_ecg_weights(len(xyz), _p(xyz), len(tets), _p(tets, ip), _p(fib), _p(D),
                           len(el), _p(el), _p(W))
+    if cables is not None:
+        rc = lib().epo_ecg_weights_cables(len(xyz), _p(xyz), C.byref(cables.c), _p(D), len(el), _p(el), _p(W))
+        if rc:
+            raise ValueError("unsupported cable quadrature order")
     return W
 
 

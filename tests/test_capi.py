@@ -77,13 +77,14 @@ def test_batch_plan_host():
         batch_plan(row, 63)
 
 
-def test_purkinje_is_plugin_level_only():
-    """EP_PURKINJE is accepted by the plugin entry (ep_ionic_step) and refused
-    as a tissue model by ep_create, before any device work."""
+def test_purkinje_is_not_a_tissue_model():
+    """EP_PURKINJE is accepted by the plugin entry (ep_ionic_step) and on the
+    .purk nodes of mixed tissues (ep_create_mixed), and refused as a tissue
+    model of its own by ep_create, before any device work."""
     from ucla_cmg_b200 import mesh as M, simulation as S
     m = M.slab(3, 3, 2, 0.2, 0.2, 0.1)
     md, mo, keep = S._instance_descs(m, capi.PURKINJE, (1e-3,) * 3, 1.0, None, None, None, None, 0.0, 0, 0, 0, None)
     sd = S._solver_desc(0.02, 0.02, 1e-7, 1000, 0.0, capi.FP64, 0.0, 0, -40.0)
     h = C.c_void_p()
     rc = capi.lib().ep_create(C.byref(md), C.byref(mo), C.byref(sd), 0, C.byref(h))
-    assert rc == -1 and b"plugin level" in capi.lib().ep_last_error()
+    assert rc == -1 and b"not a tissue model" in capi.lib().ep_last_error()

@@ -226,3 +226,32 @@ def test_angle_override_switched_on_by_any_element(tmp_path, sticky_from):
         Ab, _, _ = S.assemble_operators(mm, D, dt, bars=cab["bars"], lv=cab["lv"], angle=cab["angle"], Dp=Dp,
                                         DpLeft=Dp, radius=radius)
         assert _rel(Ab, A) > 1e-6
+
+
+@pytest.mark.parametrize("with_fibres", [False, True])
+def test_mixed_mesh_ecg_equals_the_reference(tmp_path, with_fibres):
+    """ComputeECG on a MIX3D mesh integrates over the cables too, with the
+    tissue D along each cable's fibre frame (computeDiffusionTensor applies
+    Diff to every element) and the radius ComputeECG fixes at 0.0275 cm; the
+    .angle override sets the cables' derivative and weight.  The
+    restatement's per-node weights (tets + cables) against the reference's
+    chain on a field with a front."""
+    from ucla_cmg_b200 import voomep_io as IO
+    base, xyz, slab, bars, bar_fib, lv, angle = _mixed_case(tmp_path, True)
+    if not with_fibres:
+        os.remove(base + ".fibers")
+    D = (1e-3, 5e-4, 2.5e-4)
+    rm = O.RefFemMesh(base, mixed=True, radius=0.0275, compute=True)
+    rng = np.random.default_rng(6)
+    c = xyz.mean(axis=0)
+    el = np.vstack([M.fibonacci_sphere(5, 12.0, c), xyz[-1] + [0.02, 0.0, -0.03]])
+    V = np.where(xyz[:, 2] < c[2], 15.0, -80.0) + rng.normal(0.0, 2.0, len(xyz))
+    e_ref = rm.ecg(D, el, V)
+    cab = IO.read_cables(base, np.zeros(len(xyz), np.int64))
+    cb = O.Cables(cab["bars"], fibers=cab["fibers"], radius=0.0275, orient=cab["angle"], n=len(xyz),
+                  bar_orient_node=cab["angle_node"])
+    W = O.ecg_weights(xyz, slab.tets, slab.fibers if with_fibres else None, D, el, cables=cb)
+    assert np.max(np.abs(W @ V - e_ref)) <= 1e-12 * np.max(np.abs(e_ref))
+    # without the cables' share the sums differ: the cables carry signal
+    W0 = O.ecg_weights(xyz, slab.tets, slab.fibers if with_fibres else None, D, el)
+    assert np.max(np.abs(W0 @ V - e_ref)) > 1e-9 * np.max(np.abs(e_ref))

@@ -115,6 +115,8 @@ def lib():
         "ep_model_default_consts": ([C.c_int, C.c_int, dp], C.c_int),
         "ep_create": ([C.POINTER(MeshDesc), C.POINTER(ModelDesc), C.POINTER(SolverDesc), C.c_int,
                        C.POINTER(H)], C.c_int),
+        "ep_create_mixed": ([C.POINTER(MeshDesc), C.POINTER(CablesDesc), C.c_int32, C.POINTER(C.c_int32),
+                             C.POINTER(ModelDesc), C.POINTER(SolverDesc), C.c_int, C.POINTER(H)], C.c_int),
         "ep_destroy": ([H], None),
         "ep_num_nodes": ([H], C.c_int),
         "ep_num_states": ([H], C.c_int),

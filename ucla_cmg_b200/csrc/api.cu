@@ -115,7 +115,24 @@ struct ep_handle {
     // and the test hook that makes the CG barrier wait for arrivals that
     // never come (ep_test_hold_barrier)
     unsigned int wait_grid = 0, wait_mbar = 0, bar_extra = 0;
+    // mixed tissues (ep_create_mixed): the Purkinje cell on the .purk nodes
+    // (a second SoA population indexed by node id, 21 states + the shared
+    // V), the tissue model everywhere else
+    int mixed = 0, n_pk = 0, nstate_api = 0;   // nstate_api: row width of ep_get/set_states
+    double pk_Xi = 0.0;
+    DBuf Spk, pk_consts, pk_list, pk_count, is_purk_d;
+    std::vector<uint8_t> is_purk;
+    // the cables, kept for the pseudo-ECG weights (zero-based, per-cable
+    // .angle overrides resolved)
+    std::vector<int> cab_bars, cab_bon;
+    std::vector<uint8_t> cab_ohas;
+    std::vector<double> cab_orient, cab_fib;
+    int cab_quad = 2, cab_sticky = 1;
 };
+
+// the radius ComputeECG gives cables (ComputeECG.cc:75), so an in-run ECG
+// of a mixed tissue is the one the reference's post-processor computes
+constexpr double kEcgCableRadius = 0.0275;
 
 namespace {
 
@@ -294,6 +311,57 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
 // CTA groups of the persistent CG launch: every instance gets at least one
 // CTA, the rest in proportion to its SELL slices (largest remainder).
 // Returns -1 if there are more instances than CTAs.
+// ep_cables_desc -> HostCables (zero-based ids, .angle rows per node, the
+// per-cable overrides), with the arrays kept in cs
+struct CableStore {
+    std::vector<int> bl, bon;
+    std::vector<uint8_t> ohas;
+    std::vector<double> orient;
+};
+static int host_cables(const ep_cables_desc *cables, int n, HostCables &hc, CableStore &cs) {
+    if (!cables || cables->n_bars <= 0) return EP_OK;
+    EP_CHECK_ARG(cables->bars, "null cable list");
+    EP_CHECK_ARG(cables->radius > 0.0, "cable radius must be positive");
+    const int off = cables->one_based ? 1 : 0;
+    cs.bl.resize((size_t)cables->n_bars * 2);
+    for (size_t k = 0; k < cs.bl.size(); k++) {
+        cs.bl[k] = cables->bars[k] - off;
+        EP_CHECK_ARG(cs.bl[k] >= 0 && cs.bl[k] < n, "cable node id out of range");
+    }
+    hc.nb = cables->n_bars;
+    hc.bars = cs.bl.data();
+    hc.fibers = cables->fibers;
+    hc.lv = cables->lv;
+    for (int k = 0; k < 3; k++) { hc.Dp[k] = cables->Dp[k]; hc.DpLeft[k] = cables->DpLeft[k]; }
+    hc.radius = cables->radius;
+    hc.quad_order = cables->quad_order > 0 ? cables->quad_order : 2;
+    EP_CHECK_ARG(hc.quad_order >= 1 && hc.quad_order <= 3, "cable quadrature order must be 1, 2 or 3");
+    hc.orient_sticky = cables->angle_sticky ? 1 : 0;
+    if (cables->n_angle > 0) {
+        EP_CHECK_ARG(cables->angle_nodes && cables->angle, "null .angle data");
+        cs.ohas.assign(n, 0);
+        cs.orient.assign((size_t)n * 4, 0.0);
+        for (int k = 0; k < cables->n_angle; k++) {
+            const int v = cables->angle_nodes[k] - off;
+            EP_CHECK_ARG(v >= 0 && v < n, ".angle node id out of range");
+            cs.ohas[v] = 1;
+            for (int c = 0; c < 4; c++) cs.orient[4 * (size_t)v + c] = cables->angle[4 * (size_t)k + c];
+        }
+        hc.orient_has = cs.ohas.data();
+        hc.orient = cs.orient.data();
+        if (cables->bar_angle) {
+            cs.bon.resize(cables->n_bars);
+            for (int e = 0; e < cables->n_bars; e++) {
+                const int k = cables->bar_angle[e];
+                EP_CHECK_ARG(k >= -1 && k < cables->n_angle, "bar_angle entry out of range");
+                cs.bon[e] = k < 0 ? -1 : cables->angle_nodes[k] - off;
+            }
+            hc.bar_orient_node = cs.bon.data();
+        }
+    }
+    return EP_OK;
+}
+
 // host only: the operators ep_create would build (tests and inspection)
 extern "C" int ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_desc *cables,
                                      const ep_solver_desc *sd, int64_t *nnz, int32_t *rowptr, int32_t *col,
@@ -310,50 +378,9 @@ extern "C" int ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_d
         tl[e] = v;
     }
     HostCables hc;
-    std::vector<int> bl, bon;
-    std::vector<uint8_t> ohas;
-    std::vector<double> orient;
-    if (cables && cables->n_bars > 0) {
-        EP_CHECK_ARG(cables->bars, "null cable list");
-        EP_CHECK_ARG(cables->radius > 0.0, "cable radius must be positive");
-        const int off = cables->one_based ? 1 : 0;
-        bl.resize((size_t)cables->n_bars * 2);
-        for (size_t k = 0; k < bl.size(); k++) {
-            bl[k] = cables->bars[k] - off;
-            EP_CHECK_ARG(bl[k] >= 0 && bl[k] < n, "cable node id out of range");
-        }
-        hc.nb = cables->n_bars;
-        hc.bars = bl.data();
-        hc.fibers = cables->fibers;
-        hc.lv = cables->lv;
-        for (int k = 0; k < 3; k++) { hc.Dp[k] = cables->Dp[k]; hc.DpLeft[k] = cables->DpLeft[k]; }
-        hc.radius = cables->radius;
-        hc.quad_order = cables->quad_order > 0 ? cables->quad_order : 2;
-        EP_CHECK_ARG(hc.quad_order >= 1 && hc.quad_order <= 3, "cable quadrature order must be 1, 2 or 3");
-        hc.orient_sticky = cables->angle_sticky ? 1 : 0;
-        if (cables->n_angle > 0) {
-            EP_CHECK_ARG(cables->angle_nodes && cables->angle, "null .angle data");
-            ohas.assign(n, 0);
-            orient.assign((size_t)n * 4, 0.0);
-            for (int k = 0; k < cables->n_angle; k++) {
-                const int v = cables->angle_nodes[k] - off;
-                EP_CHECK_ARG(v >= 0 && v < n, ".angle node id out of range");
-                ohas[v] = 1;
-                for (int c = 0; c < 4; c++) orient[4 * (size_t)v + c] = cables->angle[4 * (size_t)k + c];
-            }
-            hc.orient_has = ohas.data();
-            hc.orient = orient.data();
-            if (cables->bar_angle) {
-                bon.resize(cables->n_bars);
-                for (int e = 0; e < cables->n_bars; e++) {
-                    const int k = cables->bar_angle[e];
-                    EP_CHECK_ARG(k >= -1 && k < cables->n_angle, "bar_angle entry out of range");
-                    bon[e] = k < 0 ? -1 : cables->angle_nodes[k] - off;
-                }
-                hc.bar_orient_node = bon.data();
-            }
-        }
-    }
+    CableStore cs;
+    int rc0 = host_cables(cables, n, hc, cs);
+    if (rc0) return rc0;
     const double Cm = mesh->Cm > 0.0 ? mesh->Cm : 1.0;
     HostCSR csr;
     const int rc = assemble_cn(n, mesh->xyz, mesh->n_tets, tl.data(), mesh->fibers, mesh->D, Cm, sd->dt,
@@ -547,6 +574,32 @@ static int half_diffusion(ep_handle *h, const CGArgs<R> &ca) {
     return launch_cg<R>(ca, h->cg_grid, h->cg_block, h->stream, h->cg_batch, h->cg_variant);
 }
 
+// The plain ionic phase: the tissue model over every node, and in a mixed
+// tissue the Purkinje cell over the .purk nodes (which the tissue launch
+// skips), each with its own states, constants and Xi (CardiacBody::
+// getIonicCurrent calls each node's own model, Body/CardiacBody.cc:405-435)
+template <typename R>
+static int ionic_phase(ep_handle *h, const IonicArgs<R> &ia) {
+    if (!h->mixed) return launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min);
+    IonicArgs<R> t = ia;
+    t.skip = h->is_purk_d.as<uint8_t>();
+    int rc = launch_ionic<R>(h->model, t, h->stream, h->ionic_block, h->ionic_min);
+    if (rc || h->n_pk == 0) return rc;
+    IonicArgs<R> p = ia;
+    p.n = h->n_pk;                       // grid size; the list holds the nodes
+    p.S = h->Spk.as<R>();
+    p.type = nullptr;
+    p.gks = nullptr;
+    p.consts = h->pk_consts.as<R>();
+    p.nconst = ep_model_nconst(EP_PURKINJE);
+    p.Xi = (R)h->pk_Xi;
+    p.lr_table = nullptr;
+    p.node_list = h->pk_list.as<int>();
+    p.list_count = h->pk_count.as<int>();
+    h->launches += 1;
+    return launch_ionic<R>(EP_PURKINJE, p, h->stream, h->ionic_block, h->ionic_min);
+}
+
 template <typename R>
 static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     IonicArgs<R> ia;
@@ -568,11 +621,11 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
             if (h->precision == EP_SURROGATE) {
                 if ((rc = launch_learned_phase(h, ia))) return rc;
                 h->launches += h->sg_vupdate == 2 ? 3 : 2;
-            } else if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) {
+            } else if ((rc = ionic_phase<R>(h, ia))) {
                 return rc;
             }
         } else {
-            if ((rc = launch_ionic<R>(h->model, ia, h->stream, h->ionic_block, h->ionic_min))) return rc;
+            if ((rc = ionic_phase<R>(h, ia))) return rc;
         }
         if ((rc = mark(h, ne, K_CG))) return rc;
         if ((rc = half_diffusion<R>(h, ca2))) return rc;
@@ -711,16 +764,25 @@ void ep_destroy(ep_handle *h) {
 // One handle over ninst independent meshes (ninst = 1: ep_create).  The
 // instances are concatenated node-wise into one block-diagonal operator;
 // their parameter sets are concatenated into one type table.
+// ninst meshes concatenated (block-diagonal operators); with cables and
+// Purkinje nodes (ninst 1 only) a mixed tissue: the cables join the tets in
+// the operators and the listed nodes carry the Purkinje cell
 static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_desc *models,
-                        const ep_solver_desc *sd, int device, ep_handle **out) {
+                        const ep_solver_desc *sd, int device, ep_handle **out,
+                        const ep_cables_desc *cables = nullptr, int32_t n_purk = 0,
+                        const int32_t *purk_nodes = nullptr) {
     EP_CHECK_ARG(meshes && models && sd && out, "null descriptor");
     *out = nullptr;
     EP_CHECK_ARG(ninst >= 1, "no instances");
+    const bool mixed = n_purk > 0 || (cables && cables->n_bars > 0);
+    EP_CHECK_ARG(!mixed || ninst == 1, "cables and Purkinje nodes belong to a single mesh");
+    EP_CHECK_ARG(n_purk >= 0 && (n_purk == 0 || purk_nodes), "bad Purkinje node list");
+    EP_CHECK_ARG(!mixed || sd->precision != EP_SURROGATE, "the learned ionic step is not built for mixed tissues");
     const ep_model_desc *md = &models[0];
     const int nst = ep_model_nstate(md->model);
     EP_CHECK_ARG(nst > 0, "unknown cell model");
     EP_CHECK_ARG(md->model != EP_PURKINJE,
-                 "the Purkinje cell runs at plugin level (ep_ionic_step) only; tissues of it are not built");
+                 "the Purkinje cell is not a tissue model: list its nodes in ep_create_mixed");
     EP_CHECK_ARG(sd->precision == EP_FP64 || sd->precision == EP_FP32 ||
                      (sd->precision == EP_SURROGATE && md->model == EP_TUSSCHER),
                  "unsupported precision (EP_SURROGATE needs the ten Tusscher model)");
@@ -821,11 +883,27 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
         }
         std::memcpy(&h->xyz[3 * (size_t)noff], mesh->xyz, sizeof(double) * 3 * ni);
         if (all_fib) std::memcpy(&h->fibers[9 * (size_t)eoff], mesh->fibers, sizeof(double) * 9 * mi);
-        // FEM operators of this instance in FP64, appended block-diagonally
+        // FEM operators of this instance in FP64 (with the cables of a mixed
+        // tissue after the tets), appended block-diagonally
         HostCSR ci;
-        if (assemble_cn(ni, mesh->xyz, mi, tl.data(), mesh->fibers, mesh->D, h->Cm, h->dt,
-                        sd->smoothing_alpha, ci, sd->scheme) != 0) {
-            set_error("mesh %d has an element with non-positive volume", k);
+        HostCables hc;
+        CableStore cs;
+        if (mixed) {
+            int rc1 = host_cables(cables, ni, hc, cs);
+            if (rc1) return rc1;
+            h->cab_bars = cs.bl;
+            h->cab_bon = cs.bon;
+            h->cab_ohas = cs.ohas;
+            h->cab_orient = cs.orient;
+            if (hc.fibers) h->cab_fib.assign(hc.fibers, hc.fibers + 9 * (size_t)hc.nb);
+            h->cab_quad = hc.quad_order;
+            h->cab_sticky = hc.orient_sticky;
+        }
+        const int arc = assemble_cn(ni, mesh->xyz, mi, tl.data(), mesh->fibers, mesh->D, h->Cm, h->dt,
+                                    sd->smoothing_alpha, ci, sd->scheme, hc.nb ? &hc : nullptr);
+        if (arc != 0) {
+            set_error(arc == -2 ? "unsupported cable quadrature order"
+                                : "mesh %d has an element with non-positive volume or length", k);
             return EP_ERR_MESH;
         }
         const int base = csr.rowptr.back();
@@ -858,6 +936,36 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
     h->model_V0.assign(n, 0.0);
     if (is_mh(md->model))
         for (int i = 0; i < n; i++) h->model_V0[i] = st[(size_t)i * nst];
+    // mixed tissue: the Purkinje population (CardiacBody::New gives every
+    // .purk node a Purkinje cell, Body/CardiacBody.cc:1025-1040)
+    std::vector<double> pk_st;
+    std::vector<int> pk_list;
+    h->nstate_api = nst;
+    if (mixed) {
+        const int pns = ep_model_nstate(EP_PURKINJE);
+        h->mixed = 1;
+        h->nstate_api = std::max(nst, pns);
+        h->is_purk.assign(n, 0);
+        const int off = meshes[0].one_based ? 1 : 0;
+        for (int k = 0; k < n_purk; k++) {
+            const int v = purk_nodes[k] - off;
+            EP_CHECK_ARG(v >= 0 && v < n, "Purkinje node id out of range");
+            h->is_purk[v] = 1;
+        }
+        pk_st.assign((size_t)n * pns, 0.0);
+        for (int i = 0; i < n; i++) {
+            if (!h->is_purk[i]) continue;
+            pk_list.push_back(i);
+            double *ps = &pk_st[(size_t)i * pns];
+            default_state(EP_PURKINJE, 0, ps);
+            // the shared V starts from the cell's own voltage, which is also
+            // what Purkinje::getVoltage reports (IonicModel.h:42, Purkinje.h:79)
+            st[(size_t)i * nst + (is_lr(md->model) ? 7 : 0)] = ps[0];
+            h->model_V0[i] = ps[0];
+        }
+        h->n_pk = (int)pk_list.size();
+        h->pk_Xi = md->user_xi > 0 ? md->user_xi : model_xi(EP_PURKINJE);
+    }
     int rc = EP_OK;
     EP_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     EP_CUDA(cudaEventCreate(&h->ev0));
@@ -868,6 +976,22 @@ static int create_multi(int ninst, const ep_mesh_desc *meshes, const ep_model_de
     if (h->precision == EP_FP64) rc = create_typed<double>(h.get(), csr, st, consts, gks);
     else rc = create_typed<float>(h.get(), csr, st, consts, gks);
     if (rc) return rc;
+    if (mixed) {
+        const int pns = ep_model_nstate(EP_PURKINJE);     // V + the stored states
+        std::vector<double> S((size_t)(pns - 1) * h->pitch, 0.0);
+        for (int i = 0; i < n; i++)
+            if (h->is_purk[i])
+                for (int k = 0; k < pns - 1; k++) S[(size_t)k * h->pitch + i] = pk_st[(size_t)i * pns + k + 1];
+        std::vector<double> pc(ep_model_nconst(EP_PURKINJE));
+        default_consts(EP_PURKINJE, 0, pc.data());
+        rc = h->precision == EP_FP64 ? upload<double>(h->Spk, S) : upload<float>(h->Spk, S);
+        if (!rc) rc = h->precision == EP_FP64 ? upload<double>(h->pk_consts, pc) : upload<float>(h->pk_consts, pc);
+        if (rc) return rc;
+        if (pk_list.empty()) pk_list.push_back(0);           // never read: the count is 0
+        if ((rc = upload_raw(h->pk_list, pk_list.data(), pk_list.size()))) return rc;
+        if ((rc = upload_raw(h->pk_count, &h->n_pk, 1))) return rc;
+        if ((rc = upload_raw(h->is_purk_d, h->is_purk.data(), h->is_purk.size()))) return rc;
+    }
     if (h->scheme == EP_SCHEME_EXPLICIT) {
         std::vector<double> cl(csr.CL);
         cl.resize(h->pitch, 1.0);
@@ -896,6 +1020,12 @@ extern "C" {
 int ep_create(const ep_mesh_desc *mesh, const ep_model_desc *md, const ep_solver_desc *sd,
               int device, ep_handle **out) {
     return create_multi(1, mesh, md, sd, device, out);
+}
+
+int ep_create_mixed(const ep_mesh_desc *mesh, const ep_cables_desc *cables, int32_t n_purk,
+                    const int32_t *purk_nodes, const ep_model_desc *tissue, const ep_solver_desc *sd,
+                    int device, ep_handle **out) {
+    return create_multi(1, mesh, tissue, sd, device, out, cables, n_purk, purk_nodes);
 }
 
 int ep_batch_create(int32_t n_inst, const ep_mesh_desc *meshes, const ep_model_desc *models,
@@ -928,7 +1058,7 @@ int ep_batch_cg_last(ep_handle *h, int32_t *iters, double *relres) {
 }
 
 int ep_num_nodes(const ep_handle *h) { return h ? h->n : EP_ERR_ARG; }
-int ep_num_states(const ep_handle *h) { return h ? h->nstate : EP_ERR_ARG; }
+int ep_num_states(const ep_handle *h) { return h ? h->nstate_api : EP_ERR_ARG; }
 
 }  // extern "C"
 
@@ -979,19 +1109,27 @@ static int get_voltage(ep_handle *h, double *V) {
 template <typename R>
 static int put_states(ep_handle *h, const double *in) {
     const size_t tot = (size_t)h->ns * h->pitch;
-    R *st = (R *)stage(h, sizeof(R) * tot);
+    const int pns1 = h->mixed ? ep_model_nstate(EP_PURKINJE) - 1 : 0;
+    const size_t ptot = (size_t)pns1 * h->pitch;
+    R *st = (R *)stage(h, sizeof(R) * (tot + ptot));
     if (!st) return EP_ERR_NOMEM;
+    R *sp = st + tot;
     const int off = is_lr(h->model) ? 0 : 1;
+    const int w = h->nstate_api;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < h->pitch; i++) {
-        if (i < h->n) {
-            const double *s = in + (size_t)i * h->nstate;
+        const bool pk = h->mixed && i < h->n && h->is_purk[i];
+        if (i < h->n && !pk) {
+            const double *s = in + (size_t)i * w;
             for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = (R)s[k + off];
         } else {
             for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = R(0);
         }
+        // a Purkinje node's row: V, then its stored states (Purkinje.h)
+        for (int k = 0; k < pns1; k++) sp[(size_t)k * h->pitch + i] = pk ? (R)in[(size_t)i * w + 1 + k] : R(0);
     }
     EP_CUDA(cudaMemcpyAsync(h->S.p, st, sizeof(R) * tot, cudaMemcpyHostToDevice, h->stream));
+    if (ptot) EP_CUDA(cudaMemcpyAsync(h->Spk.p, sp, sizeof(R) * ptot, cudaMemcpyHostToDevice, h->stream));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     return EP_OK;
 }
@@ -999,17 +1137,28 @@ static int put_states(ep_handle *h, const double *in) {
 template <typename R>
 static int get_states(ep_handle *h, double *out) {
     const size_t tot = (size_t)h->ns * h->pitch;
-    R *st = (R *)stage(h, sizeof(R) * (tot + h->pitch));
+    const int pns1 = h->mixed ? ep_model_nstate(EP_PURKINJE) - 1 : 0;
+    const size_t ptot = (size_t)pns1 * h->pitch;
+    R *st = (R *)stage(h, sizeof(R) * (tot + h->pitch + ptot));
     if (!st) return EP_ERR_NOMEM;
     R *sv = st + tot;
+    R *sp = sv + h->pitch;
     EP_CUDA(cudaMemcpyAsync(st, h->S.p, sizeof(R) * tot, cudaMemcpyDeviceToHost, h->stream));
     EP_CUDA(cudaMemcpyAsync(sv, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    if (ptot) EP_CUDA(cudaMemcpyAsync(sp, h->Spk.p, sizeof(R) * ptot, cudaMemcpyDeviceToHost, h->stream));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     const bool lr = is_lr(h->model);
+    const int w = h->nstate_api;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < h->n; i++) {
-        double *o = out + (size_t)i * h->nstate;
-        if (lr) {
+        double *o = out + (size_t)i * w;
+        for (int k = h->nstate; k < w; k++) o[k] = 0.0;
+        if (h->mixed && h->is_purk[i]) {
+            // the Purkinje cell's row (its nVar is ep_model_nstate(EP_PURKINJE))
+            o[0] = (double)sv[i];
+            for (int k = 0; k < pns1; k++) o[k + 1] = (double)sp[(size_t)k * h->pitch + i];
+            for (int k = pns1 + 1; k < w; k++) o[k] = 0.0;
+        } else if (lr) {
             for (int k = 0; k < 7; k++) o[k] = (double)st[(size_t)k * h->pitch + i];
             o[7] = (double)sv[i];
         } else {
@@ -1092,8 +1241,20 @@ int ep_set_electrodes(ep_handle *h, int32_t ne, const double *xyz, const double 
     drop_graph(h);
     const double *D = D_ecg ? D_ecg : h->D;
     std::vector<double> W;
+    HostCables hc;
+    if (!h->cab_bars.empty()) {
+        hc.nb = (int)(h->cab_bars.size() / 2);
+        hc.bars = h->cab_bars.data();
+        hc.fibers = h->cab_fib.empty() ? nullptr : h->cab_fib.data();
+        hc.radius = kEcgCableRadius;
+        hc.quad_order = h->cab_quad;
+        hc.orient_sticky = h->cab_sticky;
+        hc.orient_has = h->cab_ohas.empty() ? nullptr : h->cab_ohas.data();
+        hc.orient = h->cab_orient.empty() ? nullptr : h->cab_orient.data();
+        hc.bar_orient_node = h->cab_bon.empty() ? nullptr : h->cab_bon.data();
+    }
     ecg_weights(h->n, h->xyz.data(), (int)(h->tets.size() / 4), h->tets.data(),
-                h->fibers.empty() ? nullptr : h->fibers.data(), D, ne, xyz, W);
+                h->fibers.empty() ? nullptr : h->fibers.data(), D, ne, xyz, W, hc.nb ? &hc : nullptr);
     // pad each electrode row to the pitch
     std::vector<double> Wp((size_t)ne * h->pitch, 0.0);
     for (int k = 0; k < ne; k++)
@@ -1453,7 +1614,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
 namespace {
 // device state that stepping changes, saved and put back around tuning trials
 struct Snapshot {
-    DBuf V, S, track, d_step, slot, pd0, pd1, pq0, pq1;
+    DBuf V, S, Spk, track, d_step, slot, pd0, pd1, pq0, pq1;
     long long step = 0;
     int ecg_count = 0;
     std::vector<double> ecg_t;
@@ -1477,6 +1638,7 @@ int snapshot(ep_handle *h, Snapshot &sn, bool save) {
     int rc;
     if ((rc = snap_copy(sn.V, h->V, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.S, h->S, h->stream, save))) return rc;
+    if ((rc = snap_copy(sn.Spk, h->Spk, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.track, h->track, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.d_step, h->d_step, h->stream, save))) return rc;
     if ((rc = snap_copy(sn.slot, h->ecg_slot, h->stream, save))) return rc;
@@ -1684,19 +1846,25 @@ int ep_write_output(ep_handle *h, double t, const char *dir) {
     return EP_OK;
 }
 
+// nVar of node i in the restart file: its own model's state count
+static int node_nvar(const ep_handle *h, int i) {
+    return (h->mixed && h->is_purk[i]) ? ep_model_nstate(EP_PURKINJE) : h->nstate;
+}
+
 int ep_write_restart(ep_handle *h, double t, const char *dir) {
     EP_CHECK_ARG(h && dir, "null argument");
-    std::vector<double> s((size_t)h->n * h->nstate);
+    const int w = h->nstate_api;
+    std::vector<double> s((size_t)h->n * w);
     int rc = ep_get_states(h, s.data());
     if (rc) return rc;
     const std::string name = out_name(dir, "InterVariables", t);
     FILE *f = fopen(name.c_str(), "wb");
     if (!f) { set_error("cannot create %s", name.c_str()); return EP_ERR_IO; }
-    const int nv = h->nstate;
     bool ok = true;
     for (int i = 0; i < h->n && ok; i++) {
+        const int nv = node_nvar(h, i);
         ok = fwrite(&nv, sizeof(int), 1, f) == 1 &&
-             fwrite(&s[(size_t)i * nv], sizeof(double), nv, f) == (size_t)nv;
+             fwrite(&s[(size_t)i * w], sizeof(double), nv, f) == (size_t)nv;
     }
     fclose(f);
     if (!ok) { set_error("short write %s", name.c_str()); return EP_ERR_IO; }
@@ -1714,11 +1882,12 @@ int ep_read_restart(ep_handle *h, double t, const char *dir) {
     if (got != (size_t)h->n) { set_error("truncated %s", vn.c_str()); return EP_ERR_IO; }
     FILE *fs = fopen(sn.c_str(), "rb");
     if (!fs) { set_error("cannot open %s", sn.c_str()); return EP_ERR_IO; }
-    std::vector<double> s((size_t)h->n * h->nstate);
+    const int w = h->nstate_api;
+    std::vector<double> s((size_t)h->n * w, 0.0);
     for (int i = 0; i < h->n; i++) {
         int nv = 0;
-        if (fread(&nv, sizeof(int), 1, fs) != 1 || nv != h->nstate ||
-            fread(&s[(size_t)i * nv], sizeof(double), nv, fs) != (size_t)nv) {
+        if (fread(&nv, sizeof(int), 1, fs) != 1 || nv != node_nvar(h, i) ||
+            fread(&s[(size_t)i * w], sizeof(double), nv, fs) != (size_t)nv) {
             fclose(fs);
             set_error("truncated or mismatched %s at node %d", sn.c_str(), i);
             return EP_ERR_IO;

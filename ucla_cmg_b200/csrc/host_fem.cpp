@@ -113,21 +113,27 @@ struct BarMat {
     double CL[3][2] = {{0, 0}, {0, 0}, {0, 0}};   // per quadrature point, for the element-order sums
 };
 
-int bar_mats(const double *xyz, const HostCables &cb, double Cm, std::vector<BarMat> &out) {
-    // LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc), weights summing to 2
-    double qx[3], qw[3];
-    int nq;
-    const int qord = 2 * (cb.quad_order > 0 ? cb.quad_order : 2) - 1;
-    if (qord == 1) { nq = 1; qx[0] = 0.0; qw[0] = 2.0; }
-    else if (qord == 3) { nq = 2; qx[0] = -0.577350269189626; qx[1] = 0.577350269189626; qw[0] = qw[1] = 1.0; }
-    else if (qord == 5) {
-        nq = 3; qx[0] = -0.774596669241483; qx[1] = 0.0; qx[2] = 0.774596669241483;
+// LineQuadrature of order 2 q - 1 on [-1, 1] (LineQuadrature.cc), weights
+// summing to 2; -1 for an order the reference does not have
+int bar_quadrature(int quad_order, double *qx, double *qw) {
+    const int qord = 2 * (quad_order > 0 ? quad_order : 2) - 1;
+    if (qord == 1) { qx[0] = 0.0; qw[0] = 2.0; return 1; }
+    if (qord == 3) { qx[0] = -0.577350269189626; qx[1] = 0.577350269189626; qw[0] = qw[1] = 1.0; return 2; }
+    if (qord == 5) {
+        qx[0] = -0.774596669241483; qx[1] = 0.0; qx[2] = 0.774596669241483;
         qw[0] = qw[2] = 5.0 / 9.0; qw[1] = 8.0 / 9.0;
-    } else {
-        return -2;
+        return 3;
     }
-    out.assign(cb.nb, BarMat());
-    int bad = 0;
+    return -1;
+}
+
+// unit direction and length of every cable in order, with the .angle
+// overrides of MixedMesh3D::Compute (MixedMesh3D.cc:30-34, 78-87): per cable
+// from bar_orient_node when resolved over the whole element order, else the
+// cables-only rule (the override carried on when orient_sticky)
+void bar_frames(const double *xyz, const HostCables &cb, std::vector<double> &ang_out, std::vector<double> &len_out) {
+    ang_out.assign(3 * (size_t)cb.nb, 0.0);
+    len_out.assign(cb.nb, 0.0);
     bool carried = false;
     double carry[4] = {0, 0, 0, 0};
     for (int e = 0; e < cb.nb; e++) {
@@ -151,6 +157,22 @@ int bar_mats(const double *xyz, const HostCables &cb, double Cm, std::vector<Bar
             for (int k = 0; k < 3; k++) ang[k] = carry[k];
             len = carry[3];
         }
+        for (int k = 0; k < 3; k++) ang_out[3 * (size_t)e + k] = ang[k];
+        len_out[e] = len;
+    }
+}
+
+int bar_mats(const double *xyz, const HostCables &cb, double Cm, std::vector<BarMat> &out) {
+    double qx[3], qw[3];
+    const int nq = bar_quadrature(cb.quad_order, qx, qw);
+    if (nq < 0) return -2;
+    out.assign(cb.nb, BarMat());
+    std::vector<double> angs, lens;
+    bar_frames(xyz, cb, angs, lens);
+    int bad = 0;
+    for (int e = 0; e < cb.nb; e++) {
+        const double *ang = &angs[3 * (size_t)e];
+        const double len = lens[e];
         if (!(len > 0.0)) bad = 1;
         const bool lv = cb.lv && cb.lv[e];
         const double *Dc = lv ? cb.DpLeft : cb.Dp;
@@ -317,7 +339,8 @@ int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *
 }
 
 void ecg_weights(int n, const double *xyz, int m, const int *tets, const double *fibers,
-                 const double D[3], int ne, const double *el, std::vector<double> &W) {
+                 const double D[3], int ne, const double *el, std::vector<double> &W,
+                 const HostCables *cables) {
     std::vector<int> eptr, elem;
     incidence(n, m, tets, eptr, elem);
     W.assign((size_t)ne * n, 0.0);
@@ -352,6 +375,55 @@ void ecg_weights(int n, const double *xyz, int m, const int *tets, const double 
                 for (int r = 0; r < 3; r++)
                     acc += g.dN[a][r] * (g.De[r][0] * G[0] + g.De[r][1] * G[1] + g.De[r][2] * G[2]);
                 W[(size_t)kk * n + i] += acc;
+            }
+        }
+    }
+    // the cables of a MIX3D mesh: ComputeECG integrates over them too
+    // (ComputeECG.h:47-50, 107-110) with the tissue D along each cable's
+    // fibre frame (computeDiffusionTensor, ComputeECG.h:92-136), shape
+    // derivatives -+ ang / length and weights w_q pi r^2 length of
+    // MixedMesh3D::Compute; the radius is the caller's (ComputeECG fixes
+    // 0.0275 cm, ComputeECG.cc:75)
+    if (cables && cables->nb > 0) {
+        double qx[3], qw[3];
+        const int nq = bar_quadrature(cables->quad_order, qx, qw);
+        std::vector<double> angs, lens;
+        bar_frames(xyz, *cables, angs, lens);
+        for (int e = 0; e < cables->nb && nq > 0; e++) {
+            const int *v = cables->bars + 2 * (size_t)e;
+            double De[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            if (!cables->fibers) {
+                for (int p = 0; p < 3; p++) De[p][p] = D[0];
+            } else {
+                const double *fib = cables->fibers + 9 * (size_t)e;
+                for (int p = 0; p < 3; p++)
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++) De[a][b] += D[p] * fib[3 * p + a] * fib[3 * p + b];
+            }
+            const double *ang = &angs[3 * (size_t)e];
+            const double len = lens[e];
+            const double dx[2][3] = {{-ang[0] / len, -ang[1] / len, -ang[2] / len},
+                                     {ang[0] / len, ang[1] / len, ang[2] / len}};
+            for (int kk = 0; kk < ne; kk++) {
+                const double *x = el + 3 * kk;
+                double G[3] = {0, 0, 0};
+                for (int q = 0; q < nq; q++) {
+                    const double N0 = 0.5 * (1. - qx[q]), N1 = 0.5 * (1. + qx[q]);
+                    double pos[3], d2 = 0.0;
+                    for (int d = 0; d < 3; d++) {
+                        pos[d] = N0 * xyz[3 * (size_t)v[0] + d] + N1 * xyz[3 * (size_t)v[1] + d];
+                        d2 += (pos[d] - x[d]) * (pos[d] - x[d]);
+                    }
+                    const double dist = std::sqrt(d2);
+                    if (dist < 1e-6) continue;       // ComputeECG.h:77-79
+                    const double d3 = dist * dist * dist;
+                    const double w = qw[q] * M_PI * (cables->radius * cables->radius) * len;
+                    for (int d = 0; d < 3; d++) G[d] += (-(pos[d] - x[d]) / d3) * w;
+                }
+                double DG[3];
+                for (int r = 0; r < 3; r++) DG[r] = De[r][0] * G[0] + De[r][1] * G[1] + De[r][2] * G[2];
+                for (int b = 0; b < 2; b++)
+                    W[(size_t)kk * n + v[b]] += dx[b][0] * DG[0] + dx[b][1] * DG[1] + dx[b][2] * DG[2];
             }
         }
     }

@@ -46,9 +46,11 @@ int assemble_cn(int n, const double *xyz, int m, const int *tets, const double *
                 int scheme = 0, const HostCables *cables = nullptr);
 
 // W[k * n + i] with ECG_k = sum_i W V_i (ComputeECG.h:30-189 with grad V
-// constant on a P1 tet).
+// constant on a P1 tet); the cables of a MIX3D mesh add their share (with
+// the tissue D and cables->radius, which ComputeECG fixes at 0.0275 cm).
 void ecg_weights(int n, const double *xyz, int m, const int *tets, const double *fibers,
-                 const double D[3], int ne, const double *electrodes, std::vector<double> &W);
+                 const double D[3], int ne, const double *electrodes, std::vector<double> &W,
+                 const HostCables *cables = nullptr);
 
 // SELL-32 packing of a CSR pattern: slice_ptr (element offsets, multiples of
 // 32), col, and the values of one or more value arrays.

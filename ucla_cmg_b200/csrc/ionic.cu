@@ -128,8 +128,11 @@ __global__ void __launch_bounds__(128, MINB) k_ionic(const IonicArgs<R> a) {
     // could not take).  One call site, so both modes run the same machine
     // code and a node's result does not depend on which mode advanced it.
     const int cnt = a.node_list ? *a.list_count : a.n;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
-        ionic_node<R, MODEL, NS>(a, a.node_list ? a.node_list[k] : k, my_newton, my_caps, my_bad);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const int node = a.node_list ? a.node_list[k] : k;
+        if (a.skip && a.skip[node]) continue;
+        ionic_node<R, MODEL, NS>(a, node, my_newton, my_caps, my_bad);
+    }
     // block-level status reduction, one atomic per block
     for (int o = 16; o > 0; o >>= 1) {
         my_newton += __shfl_xor_sync(0xffffffffu, my_newton, o);

@@ -73,6 +73,8 @@ template <typename R> struct IonicArgs {
                                  // dV/dt, leave V unchanged (one sub-step)
     const int *node_list;        // non-null: run only these nodes (count on the device)
     const int *list_count;
+    const uint8_t *skip;         // non-null: nodes with skip[i] != 0 are left alone (mixed
+                                 // tissues: the Purkinje nodes in the tissue model's launch)
     // model options
     TTOpts tt;
     int mh_abs;

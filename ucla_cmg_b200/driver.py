@@ -34,13 +34,17 @@ Same as the reference:
   ``int(FREQUENCY/DT)`` steps; restart files every ``long(WRITERESTART/DT)``
   steps; simulated time accumulated as ``simtime += dt``.
 
-The Purkinje keys (TWODRADIUS, PURKINJEDIFFUSION, LVPURKINJEDIFFUSION, with
-the reference's defaults 0.0275 cm and 0.0032 cm^2/ms, EPSimulator.cc:89,
-102-103) are read and the 2-node cables of a MIX3D mesh are read with their
-LV flags and .angle overrides (``voomep_io.read_cables``); as in the
+A MIX3D mesh with 2-node cables runs as a mixed tissue (ep_create_mixed):
+the cables join the tets in the operators, the .purk nodes carry the
+Purkinje cell and the other nodes the tissue model, the PURKINJE block of
+INITIALSTATES goes to the Purkinje nodes, and restart files keep each node's
+own nVar.  The Purkinje keys (TWODRADIUS, PURKINJEDIFFUSION,
+LVPURKINJEDIFFUSION, with the reference's defaults 0.0275 cm and 0.0032
+cm^2/ms, EPSimulator.cc:89, 102-103) are read with the cables' LV flags and
+.angle overrides (``voomep_io.read_cables``, which resolves the overrides
+over the whole .ele order as MixedMesh3D::Compute does); as in the
 reference, the LV cables get PURKINJEDIFFUSION, not LVPURKINJEDIFFUSION
-(``setPurkinjeDiffusionInLV(Dp)``, EPSimulator.cc:420-421).  The cables are
-not yet run on the GPU: the driver reports them and runs the tets.
+(``setPurkinjeDiffusionInLV(Dp)``, EPSimulator.cc:420-421).
 
 Not on this path (accepted and ignored, with a note): the mechanics keys,
 QUADORDER other than 2, CONSISTENCYCHECK.
@@ -261,39 +265,64 @@ def cable_setup(cfg, node_type):
 
 
 def run(input_file, precision=capi.FP64, rest_voltage=False, device=0, surrogate_path=None, verbose=True,
-        tt_jacobian=capi.TT_JAC_TRUE, zonal_fallthrough=True):
+        tt_jacobian=capi.TT_JAC_TRUE, zonal_fallthrough=True, cg_tol=1e-7):
     cfg = parse_input(input_file)
     base_dir = cfg["input_dir"]
     model = CELL_MODELS[cfg["cell_model"].upper()]
     mesh, node_type, purk, other = read_mesh(os.path.join(base_dir, cfg["model"]))
-    if other and verbose:
-        cab = cable_setup(cfg, node_type)
-        nb = 0 if cab is None else len(cab["bars"])
-        print(f"** {other} non-tet elements ({nb} Purkinje cables, radius {cfg['radius']} cm, "
-              f"D_p {cfg['Dp'][0]}) are read but not run on this path yet")
+    # a MIX3D mesh with cables: a mixed tissue, the Purkinje cell on the
+    # .purk nodes (CardiacBody::New, CardiacBody.cc:982-1101)
+    cab = cable_setup(cfg, node_type) if other else None
+    purk0 = None
+    if cab is not None or (purk is not None and other):
+        purk0 = (np.asarray(purk, dtype=np.int64) - 1) if purk is not None else np.zeros(0, np.int64)
+        if verbose:
+            nb = 0 if cab is None else len(cab["bars"])
+            print(f"** mixed tissue: {nb} Purkinje cables (radius {cfg['radius']} cm, D_p {cfg['Dp'][0]}), "
+                  f"{len(purk0)} Purkinje cells")
     nstate = capi.model_nstate(model)
-    init = None
+    init, pk_init = None, None
     if cfg["initial_states"]:
-        cell, _ = read_initial_states(os.path.join(base_dir, cfg["initial_states"]))
+        cell, pkb = read_initial_states(os.path.join(base_dir, cfg["initial_states"]))
         if len(cell) != nstate:
             raise ValueError(f"INITIALSTATES CELL block has {len(cell)} values, the model {nstate}")
         init = np.tile(cell, (mesh.n, 1))
+        if purk0 is not None and len(pkb):
+            if len(pkb) != capi.model_nstate(capi.PURKINJE):
+                raise ValueError(f"INITIALSTATES PURKINJE block has {len(pkb)} values, the cell 22")
+            pk_init = pkb
     n_types = None
     if node_type is not None and model in (capi.MAHAJAN, capi.MAHAJAN_FAIL):
         n_types = 9
+        if purk0 is not None:
+            # Purkinje nodes carry types 11/12; their tissue rows are unused
+            node_type = np.where(node_type > 8, 0, node_type)
     elif model not in (capi.MAHAJAN, capi.MAHAJAN_FAIL):
         node_type = None                        # one parameter set (TT, LR)
     dt = cfg["dt"]
-    g = Monodomain(mesh, model, precision, dt=dt, ionic_dt=cfg["ionic_dt"], D=cfg["D"], cg_tol=1e-7,
+    mixed = {} if purk0 is None else dict(cables=cab, purkinje=purk0)
+    g = Monodomain(mesh, model, precision, dt=dt, ionic_dt=cfg["ionic_dt"], D=cfg["D"], cg_tol=cg_tol,
                    cg_maxit=1000, node_type=node_type, n_types=n_types, initial_states=init,
-                   smoothing_alpha=cfg["smoothing"] or 0.0, tt_jacobian=tt_jacobian, device=device)
+                   smoothing_alpha=cfg["smoothing"] or 0.0, tt_jacobian=tt_jacobian, device=device, **mixed)
     if precision == capi.SURROGATE:
         from .surrogate import Surrogate, DEFAULT_PATH
         Surrogate.load(surrogate_path or DEFAULT_PATH).deploy(g)
+    if pk_init is not None:
+        S = g.states()
+        S[purk0, :len(pk_init)] = pk_init
+        g.set_states(S)
+    lr = model in (capi.LUORUDY, capi.LUORUDYWITHGATE)
     if rest_voltage:
-        g.set_voltage(g.states()[:, 7 if model in (capi.LUORUDY, capi.LUORUDYWITHGATE) else 0])
+        S = g.states()
+        V0 = S[:, 7 if lr else 0].copy()
+        if purk0 is not None:
+            V0[purk0] = S[purk0, 0]             # the Purkinje cell keeps V in slot 0
+        g.set_voltage(V0)
     else:
-        g.set_voltage(g.model_voltage())
+        V0 = g.model_voltage()
+        if pk_init is not None:
+            V0[purk0] = pk_init[0]              # Purkinje::getVoltage: State[0]
+        g.set_voltage(V0)
     out = os.path.join(base_dir, cfg["output_dir"])
     os.makedirs(out, exist_ok=True)
     # the loop's step count and simulated time, accumulated as the reference does

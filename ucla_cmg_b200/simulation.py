@@ -94,11 +94,17 @@ class Monodomain:
                  type_consts=None, n_types=None, gks_scale=None, user_xi=0.0, newton_cap=0,
                  tt_jacobian=capi.TT_JAC_REFERENCE, mh_abs_mode=0, initial_states=None,
                  smoothing_alpha=0.0, newton_tol=0.0, ecg_every=0, act_threshold=-40.0, device=0,
-                 scheme=capi.SCHEME_CN, diffusion_dt=0.0):
+                 scheme=capi.SCHEME_CN, diffusion_dt=0.0, cables=None, purkinje=None):
         """scheme: capi.SCHEME_CN (EP_CrankNicholson, the reference driver's),
         SCHEME_BE (EP_BackwardEuler) or SCHEME_EXPLICIT (EP_ExplicitSolver,
         diffusion sub-step diffusion_dt, 0: 0.05 ms).  cg_tol 0 takes the
-        scheme's own (1e-7 CN, 1e-10 BE)."""
+        scheme's own (1e-7 CN, 1e-10 BE).
+
+        Mixed tissues (ep_create_mixed): ``cables``, a dict of the keywords
+        of :func:`assemble_operators` for 2-node cables (bars, bar_fibers,
+        lv, Dp, DpLeft, radius, quad_order, angle, angle_sticky,
+        bar_angle_node), and ``purkinje``, the zero-based nodes carrying the
+        Purkinje cell; the states then come in rows of max(nstate, 22)."""
         L = capi.lib()
         self.mesh = mesh
         self.model = model
@@ -110,7 +116,14 @@ class Monodomain:
         sd = _solver_desc(dt, ionic_dt, cg_tol, cg_maxit, smoothing_alpha, precision, newton_tol, ecg_every,
                           act_threshold, scheme, diffusion_dt)
         h = C.c_void_p()
-        check(L.ep_create(C.byref(md), C.byref(mo), C.byref(sd), int(device), C.byref(h)))
+        if cables is None and purkinje is None:
+            check(L.ep_create(C.byref(md), C.byref(mo), C.byref(sd), int(device), C.byref(h)))
+        else:
+            cd = _cables_desc(self._keep, **cables) if cables is not None else None
+            self._keep["purk"] = np.ascontiguousarray(purkinje if purkinje is not None else [], dtype=np.int32)
+            check(L.ep_create_mixed(C.byref(md), C.byref(cd) if cd is not None else None, len(self._keep["purk"]),
+                                    ptr(self._keep["purk"], C.POINTER(C.c_int32)), C.byref(mo), C.byref(sd),
+                                    int(device), C.byref(h)))
         self._h = h
         self.nstate = L.ep_num_states(h)
         self.last_stats = None
@@ -351,6 +364,37 @@ def batch_plan(inst_row, grid):
     return out
 
 
+def _cables_desc(keep, bars, Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, bar_fibers=None, lv=None,
+                 quad_order=2, angle=None, angle_sticky=True, bar_angle_node=None):
+    """capi.CablesDesc of 2-node cables (zero-based), the arrays kept in ``keep``."""
+    keep["bars"] = np.ascontiguousarray(bars, dtype=np.int32).reshape(-1, 2)
+    keep["bfib"] = None if bar_fibers is None else np.ascontiguousarray(bar_fibers, dtype=np.float64)
+    keep["lv"] = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
+    cd = capi.CablesDesc()
+    cd.n_bars = len(keep["bars"])
+    cd.bars = ptr(keep["bars"], C.POINTER(C.c_int32))
+    cd.one_based = 0
+    cd.fibers = ptr(keep["bfib"])
+    cd.lv = ptr(keep["lv"], C.POINTER(C.c_uint8))
+    for k in range(3):
+        cd.Dp[k] = float(Dp[k])
+        cd.DpLeft[k] = float((DpLeft if DpLeft is not None else Dp)[k])
+    cd.radius = float(radius)
+    cd.quad_order = int(quad_order)
+    cd.angle_sticky = int(bool(angle_sticky))
+    if angle:
+        keep["an"] = np.array(sorted(angle), dtype=np.int32)
+        keep["ad"] = np.array([angle[k] for k in sorted(angle)], dtype=np.float64).reshape(-1, 4)
+        cd.n_angle = len(keep["an"])
+        cd.angle_nodes = ptr(keep["an"], C.POINTER(C.c_int32))
+        cd.angle = ptr(keep["ad"])
+        if bar_angle_node is not None:
+            row = {int(v): k for k, v in enumerate(keep["an"])}
+            keep["ba"] = np.array([row[int(v)] if v >= 0 else -1 for v in bar_angle_node], dtype=np.int32)
+            cd.bar_angle = ptr(keep["ba"], C.POINTER(C.c_int32))
+    return cd
+
+
 def assemble_operators(mesh, D, dt, Cm=1.0, scheme=capi.SCHEME_CN, smoothing_alpha=0.0, bars=None,
                        Dp=(0.0016,) * 3, DpLeft=None, radius=0.0275, bar_fibers=None, lv=None, quad_order=2,
                        angle=None, angle_sticky=True, bar_angle_node=None):
@@ -367,31 +411,8 @@ def assemble_operators(mesh, D, dt, Cm=1.0, scheme=capi.SCHEME_CN, smoothing_alp
     sd = _solver_desc(dt, dt, 1e-7, 1000, smoothing_alpha, capi.FP64, 0.0, 0, -40.0, scheme)
     cd = None
     if bars is not None:
-        keep["bars"] = np.ascontiguousarray(bars, dtype=np.int32).reshape(-1, 2)
-        keep["bfib"] = None if bar_fibers is None else np.ascontiguousarray(bar_fibers, dtype=np.float64)
-        keep["lv"] = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
-        cd = capi.CablesDesc()
-        cd.n_bars = len(keep["bars"])
-        cd.bars = ptr(keep["bars"], C.POINTER(C.c_int32))
-        cd.one_based = 0
-        cd.fibers = ptr(keep["bfib"])
-        cd.lv = ptr(keep["lv"], C.POINTER(C.c_uint8))
-        for k in range(3):
-            cd.Dp[k] = float(Dp[k])
-            cd.DpLeft[k] = float((DpLeft if DpLeft is not None else Dp)[k])
-        cd.radius = float(radius)
-        cd.quad_order = int(quad_order)
-        cd.angle_sticky = int(bool(angle_sticky))
-        if angle:
-            keep["an"] = np.array(sorted(angle), dtype=np.int32)
-            keep["ad"] = np.array([angle[k] for k in sorted(angle)], dtype=np.float64).reshape(-1, 4)
-            cd.n_angle = len(keep["an"])
-            cd.angle_nodes = ptr(keep["an"], C.POINTER(C.c_int32))
-            cd.angle = ptr(keep["ad"])
-            if bar_angle_node is not None:
-                row = {int(v): k for k, v in enumerate(keep["an"])}
-                keep["ba"] = np.array([row[int(v)] if v >= 0 else -1 for v in bar_angle_node], dtype=np.int32)
-                cd.bar_angle = ptr(keep["ba"], C.POINTER(C.c_int32))
+        cd = _cables_desc(keep, bars, Dp, DpLeft, radius, bar_fibers, lv, quad_order, angle, angle_sticky,
+                          bar_angle_node)
     nnz = C.c_int64(0)
     L = capi.lib()
     cdp = C.byref(cd) if cd is not None else None
