@@ -299,6 +299,22 @@ int  ep_create_mixed(const ep_mesh_desc *mesh, const struct ep_cables_desc *cabl
                      const int32_t *purk_nodes, const ep_model_desc *tissue, const ep_solver_desc *solver,
                      int device, ep_handle **out);
 
+/* Offline pseudo-ECG of stored voltage fields: the post-processor ComputeECG
+ * (Applications/CardiacEP/ComputeECG.cc:26-162 over ComputeECG.h:30-189).
+ * ep_ecg_create builds the per-node weights of the mesh once in FP64 on the
+ * host -- the tets and, for a MIX3D mesh, the 2-node cables with the radius
+ * ComputeECG fixes (0.0275 cm, ComputeECG.cc:75; cables->radius is not
+ * used here) and the tissue D along each cable's fibres -- and keeps them on
+ * the GPU; D_ecg NULL takes ComputeECG's hard-coded {1e-3, 5e-4, 2.5e-4}
+ * (ComputeECG.cc:88).  ep_ecg_eval reduces n_frames voltage fields (host,
+ * frame-major, n_nodes each) to out[f * n_electrodes + k], FP64 sums on the
+ * device.  At most 16 electrodes. */
+typedef struct ep_ecg ep_ecg;
+int  ep_ecg_create(const ep_mesh_desc *mesh, const struct ep_cables_desc *cables, int32_t n_electrodes,
+                   const double *xyz, const double *D_ecg, int device, ep_ecg **out);
+int  ep_ecg_eval(ep_ecg *e, int32_t n_frames, const double *V, double *out);
+void ep_ecg_destroy(ep_ecg *e);
+
 /* The FP64 operators ep_create assembles for the solver's scheme, on the
  * host only (no GPU, no device memory): CSR of n_nodes rows, zero-based
  * sorted columns, A and B (CN: C_m M +- dt/4 K; BE: C_L + dt/2 K and C_L;

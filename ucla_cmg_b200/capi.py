@@ -117,6 +117,10 @@ def lib():
                        C.POINTER(H)], C.c_int),
         "ep_create_mixed": ([C.POINTER(MeshDesc), C.POINTER(CablesDesc), C.c_int32, C.POINTER(C.c_int32),
                              C.POINTER(ModelDesc), C.POINTER(SolverDesc), C.c_int, C.POINTER(H)], C.c_int),
+        "ep_ecg_create": ([C.POINTER(MeshDesc), C.POINTER(CablesDesc), C.c_int32, dp, dp, C.c_int,
+                           C.POINTER(H)], C.c_int),
+        "ep_ecg_eval": ([H, C.c_int32, dp, dp], C.c_int),
+        "ep_ecg_destroy": ([H], None),
         "ep_destroy": ([H], None),
         "ep_num_nodes": ([H], C.c_int),
         "ep_num_states": ([H], C.c_int),
