@@ -354,6 +354,10 @@ typedef struct ep_launch_config {
     int32_t cg_prefetch;  /* 0..4: each warp of the CG launch asks L2 for the
                              SELL indices and values of the slice it reads that
                              many slices ahead (cg_variant 0; 0 = off) */
+    int32_t sg_variant;   /* learned ionic step (EP_SURROGATE): 0 two CTAs per SM,
+                             each one tile of 128 nodes at a time; 1 one CTA per SM
+                             running four tiles at once in four warpgroups (one
+                             copy of the weights); same results */
 } ep_launch_config;
 /* Bounded in-kernel waits (no reference counterpart: the reference has no
  * device code; its Newton loop has no cap, Tusscher.cc:150).  Every wait of

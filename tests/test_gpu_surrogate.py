@@ -115,3 +115,29 @@ def test_ablation_untrained_network(gpu):
     bb = (ref["ta"] >= 0) & (b["ta"] >= 0)
     err_b = np.abs(b["ta"] - ref["ta"])[bb].mean() if bb.any() else np.inf
     assert b["fb"] > 2 * a["fb"] or err_b > 4 * max(err_a, 0.05) or not np.array_equal(ref["ta"] >= 0, b["ta"] >= 0)
+
+
+def test_four_pipeline_kernel_gives_the_same_bits(gpu):
+    """sg_variant 1 (one CTA per SM running four 128-node tiles at once in
+    four warpgroups) issues the same MMA and epilogue instructions per tile
+    as sg_variant 0 (two CTAs per SM): the learned runs are bit-identical,
+    fallbacks included, with a node count that leaves a partial last tile."""
+    m, node_type, gks, blk = _setup()
+    sg = _trained()
+    out = []
+    for var in (0, 1):
+        g = Monodomain(m, capi.TUSSCHER, capi.SURROGATE, dt=0.1, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
+                       node_type=node_type, type_consts=W.tt_type_consts(), gks_scale=gks,
+                       tt_jacobian=capi.TT_JAC_TRUE)
+        sg.deploy(g)
+        g.set_launch_config(sg_variant=var)
+        assert g.launch_config()["sg_variant"] == var
+        g.set_voltage(-85.423)
+        g.set_stimulus(blk, 0.0, 2.0, 50.0 * W.TT_XI)
+        st = g.step(300)
+        assert st["timeouts"] == 0
+        out.append((g.voltage(), g.states(), st["fallback_nodes"]))
+        g.close()
+    assert m.n % 128 != 0 and out[0][2] > 0
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])

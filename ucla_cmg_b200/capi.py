@@ -87,7 +87,7 @@ class LaunchConfig(C.Structure):
     _fields_ = [("cg_block", C.c_int32), ("cg_per_sm", C.c_int32), ("ionic_block", C.c_int32),
                 ("graph_steps", C.c_int32), ("ionic_min_ctas", C.c_int32), ("cg_batch", C.c_int32),
                 ("cg_variant", C.c_int32), ("cg_predict", C.c_int32),
-                ("cg_prefetch", C.c_int32)]
+                ("cg_prefetch", C.c_int32), ("sg_variant", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -103,6 +103,7 @@ struct ep_handle {
     std::vector<int> inst_blk;           // ninst + 1 CTA offsets of the CG groups
     DBuf d_inst_row, d_inst_blk;
     // launch shape (ep_set_launch_config / ep_autotune)
+    int sg_variant = 0;                  // learned step: 0 two CTAs/SM, 1 four pipelines in one CTA/SM
     int cg_per_sm = 0, cg_batch = 4, cg_variant = 0, cg_predict = 0, cg_prefetch = 0, ionic_block = 128,
         ionic_min = 0, graph_steps = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -533,7 +534,7 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     EP_CUDA(cudaMemsetAsync(h->sg_count.p, 0, sizeof(int), h->stream));
     SurrogateArgs sa;
     fill_surrogate_args(h, ia, sa);
-    int rc = launch_surrogate(sa, h->stream);
+    int rc = launch_surrogate(sa, h->stream, h->sg_variant);
     if (rc) return rc;
     if (h->sg_vupdate == 2 && (rc = launch_hybrid(sa, h->stream))) return rc;
     IonicArgs<float> fb = ia;
@@ -1525,6 +1526,7 @@ int ep_get_launch_config(const ep_handle *h, ep_launch_config *cfg) {
     cfg->cg_variant = h->cg_variant;
     cfg->cg_predict = h->cg_predict;
     cfg->cg_prefetch = h->cg_prefetch;
+    cfg->sg_variant = h->sg_variant;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1566,6 +1568,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CHECK_ARG(cfg->cg_predict >= 0 && cfg->cg_predict <= 2, "cg_predict must be 0, 1 or 2");
     EP_CHECK_ARG(!(cfg->cg_predict && cfg->cg_variant), "cg_predict needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_prefetch >= 0 && cfg->cg_prefetch <= 4, "cg_prefetch must be 0..4");
+    EP_CHECK_ARG(cfg->sg_variant == 0 || cfg->sg_variant == 1, "sg_variant must be 0 or 1");
     EP_CHECK_ARG(!(cfg->cg_prefetch && cfg->cg_variant), "cg_prefetch needs cg_variant 0");
     EP_CHECK_ARG(cfg->cg_per_sm >= 0 && cfg->cg_per_sm <= 32, "cg_per_sm out of range");
     EP_CHECK_ARG(cfg->ionic_block == 64 || cfg->ionic_block == 128, "ionic_block must be 64 or 128");
@@ -1605,6 +1608,7 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     }
     h->cg_predict = cfg->cg_predict;
     h->cg_prefetch = cfg->cg_prefetch;
+    h->sg_variant = cfg->sg_variant;
     h->ionic_block = cfg->ionic_block;
     h->ionic_min = cfg->ionic_min_ctas;
     h->graph_steps = cfg->graph_steps;
@@ -1675,6 +1679,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     cur.cg_variant = h->cg_variant;
     cur.cg_predict = h->cg_predict;
     cur.cg_prefetch = h->cg_prefetch;
+    cur.sg_variant = h->sg_variant;
     cur.cg_per_sm = h->cg_grid / std::max(1, nsm);
     cur.ionic_block = h->ionic_block;
     cur.ionic_min_ctas = h->ionic_min;
@@ -1745,6 +1750,12 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
             const double t = trial(c);
             if (t >= 0 && t < t_best) { t_best = t; b = c; }
         }
+    }
+    if (h->has_surrogate) {
+        ep_launch_config c = b;
+        c.sg_variant = 1 - b.sg_variant;
+        const double t = trial(c);
+        if (t >= 0 && t < t_best) { t_best = t; b = c; }
     }
     for (int ib : {64, 128}) {
         if (ib == b.ionic_block) continue;

@@ -266,6 +266,76 @@ __device__ __forceinline__ bool build_row(const SurrogateArgs &a, const Surrogat
     return inside;
 }
 
+// One node's share of the output stage: the network's de-normalised
+// changes applied (or, in the hybrid form, its six concentrations handed to
+// k_hybrid), and the nodes outside the envelope or with an output outside
+// its training range appended to the fallback list.  yv: the node's 32
+// output-layer accumulators (bias not yet added).
+__device__ __forceinline__ void output_node(const SurrogateArgs &a, const SurrogateAux *aux, int i, bool valid,
+                                            bool raw, bool inside, const uint32_t (&yv)[32], double t0,
+                                            unsigned int &my_fb) {
+    if (valid && raw) {
+#pragma unroll
+        for (int j = 0; j < SG_NOUT; j++) a.rawY[(size_t)i * SG_NOUT + j] = __uint_as_float(yv[j]) + aux->b4[j];
+    } else if (valid) {
+        // the six concentrations the hybrid form replaces, loaded before
+        // any store of this node (the stores below could alias them for
+        // the compiler, which would otherwise serialise load and store)
+        const int cslot[6] = {0, 1, 2, 9, 16, 17};
+        float xs[6];
+        if (aux->v_update == 2) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) xs[j] = a.S[(size_t)cslot[j] * a.pitch + i];
+        }
+        // de-normalise; a used output outside the range seen in training
+        // sends the node to the plain model as well
+        float d[SG_NY];
+        bool out_ok = inside;
+#pragma unroll
+        for (int j = 0; j < SG_NY; j++) {
+            const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+            if ((aux->out_mask >> j) & 1u) out_ok = out_ok && (u >= aux->out_lo[j]) && (u <= aux->out_hi[j]);
+            const float sc = aux->out_scale[j];
+            d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
+        }
+        const unsigned int lm = aux->log_mask;
+        if (aux->v_update == 2) a.take[i] = out_ok ? 1 : 0;
+        if (!out_ok) {
+            const int slot = atomicAdd(a.fallback_count, 1);
+            a.fallback_list[slot] = i;
+            my_fb++;
+        } else if (aux->v_update == 2) {
+            // the new concentrations; k_hybrid advances gates and V
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                const int q = cslot[j];
+                a.pred[(size_t)j * a.pitch + i] =
+                    ((lm >> (q + 1)) & 1u) ? xs[j] * __expf(d[q + 1]) : xs[j] + d[q + 1];
+            }
+        } else {
+            // every quantity from the network (all loads before the stores)
+            float xk[18];
+#pragma unroll
+            for (int k = 0; k < 18; k++) xk[k] = a.S[(size_t)k * a.pitch + i];
+#pragma unroll
+            for (int k = 0; k < 18; k++) {
+                // log-scaled states are updated multiplicatively: x' = x exp(d)
+                a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk[k] * __expf(d[k + 1]) : xk[k] + d[k + 1];
+            }
+            const float V0 = a.V[i], V1 = V0 + d[0];
+            a.V[i] = V1;
+            if (a.track) {
+                Track tr = a.track[i];
+                if (tr.t_rep < 0.f) {
+                    bool dirty = false;
+                    track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
+                    if (dirty) a.track[i] = tr;
+                }
+            }
+        }
+    }
+}
+
 // The network over tiles of 128 nodes, 256 threads per CTA.  Threads
 // 0..127 own one node each (features, the output layer, the envelope
 // decision); all eight warps share the hidden-layer epilogues (warp w reads
@@ -360,66 +430,7 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
         uint32_t yv[32];
         tmem_ld32(d_out + lane_off, yv);
         tc_fence_before();
-        if (valid && raw) {
-#pragma unroll
-            for (int j = 0; j < SG_NOUT; j++) a.rawY[(size_t)i * SG_NOUT + j] = __uint_as_float(yv[j]) + aux->b4[j];
-        } else if (valid) {
-            // the six concentrations the hybrid form replaces, loaded before
-            // any store of this node (the stores below could alias them for
-            // the compiler, which would otherwise serialise load and store)
-            const int cslot[6] = {0, 1, 2, 9, 16, 17};
-            float xs[6];
-            if (aux->v_update == 2) {
-#pragma unroll
-                for (int j = 0; j < 6; j++) xs[j] = a.S[(size_t)cslot[j] * a.pitch + i];
-            }
-            // de-normalise; a used output outside the range seen in training
-            // sends the node to the plain model as well
-            float d[SG_NY];
-            bool out_ok = inside;
-#pragma unroll
-            for (int j = 0; j < SG_NY; j++) {
-                const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
-                if ((aux->out_mask >> j) & 1u) out_ok = out_ok && (u >= aux->out_lo[j]) && (u <= aux->out_hi[j]);
-                const float sc = aux->out_scale[j];
-                d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
-            }
-            const unsigned int lm = aux->log_mask;
-            if (aux->v_update == 2) a.take[i] = out_ok ? 1 : 0;
-            if (!out_ok) {
-                const int slot = atomicAdd(a.fallback_count, 1);
-                a.fallback_list[slot] = i;
-                my_fb++;
-            } else if (aux->v_update == 2) {
-                // the new concentrations; k_hybrid advances gates and V
-#pragma unroll
-                for (int j = 0; j < 6; j++) {
-                    const int q = cslot[j];
-                    a.pred[(size_t)j * a.pitch + i] =
-                        ((lm >> (q + 1)) & 1u) ? xs[j] * __expf(d[q + 1]) : xs[j] + d[q + 1];
-                }
-            } else {
-                // every quantity from the network (all loads before the stores)
-                float xk[18];
-#pragma unroll
-                for (int k = 0; k < 18; k++) xk[k] = a.S[(size_t)k * a.pitch + i];
-#pragma unroll
-                for (int k = 0; k < 18; k++) {
-                    // log-scaled states are updated multiplicatively: x' = x exp(d)
-                    a.S[(size_t)k * a.pitch + i] = ((lm >> (k + 1)) & 1u) ? xk[k] * __expf(d[k + 1]) : xk[k] + d[k + 1];
-                }
-                const float V0 = a.V[i], V1 = V0 + d[0];
-                a.V[i] = V1;
-                if (a.track) {
-                    Track tr = a.track[i];
-                    if (tr.t_rep < 0.f) {
-                        bool dirty = false;
-                        track_interval(tr, dirty, V0, V1, t0, (float)a.t_per_step, a.act_thr);
-                        if (dirty) a.track[i] = tr;
-                    }
-                }
-            }
-        }
+        output_node(a, aux, i, valid, raw, inside, yv, t0, my_fb);
     }
     // count fallback node-steps
     for (int o = 16; o > 0; o >>= 1) my_fb += __shfl_xor_sync(0xffffffffu, my_fb, o);
@@ -428,6 +439,126 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_surrogate(const SurrogateArgs
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, SG_TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// The same network with four tile pipelines in one CTA per SM (512 threads =
+// four warpgroups).  Warpgroup g owns slot g: an A buffer of its own, TMEM
+// columns [128 g, 128 g + 128) (the output layer reuses the first 32 once the
+// last hidden epilogue has read them), an mbarrier and a named barrier; it
+// runs its tiles start to end -- row build, four MMA layers, output --
+// while the other three do the same, so four tiles are in flight per SM
+// against two with k_surrogate, with one copy of the weights (80 KB) instead
+// of two.  Each thread owns one node of its slot's tile and its whole row in
+// the hidden epilogues.  Same instructions per tile, same results.
+constexpr int SG4_SLOTS = 4;
+constexpr int SG4_THREADS = SG4_SLOTS * SG_M;
+constexpr int OFF4_A = OFF_W4 + SG_W4 * 2;
+constexpr int OFF4_MISC = OFF4_A + SG4_SLOTS * SG_M * SG_H * 2;
+constexpr int SG4_SMEM = OFF4_MISC + 128;
+constexpr uint32_t SG4_TMEM_COLS = 512;
+
+// named barrier `id` over the 128 threads of one warpgroup
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool wg_any(bool pred, int id) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+// wait_commit for one warpgroup (bounded, warpgroup-uniform)
+__device__ __forceinline__ bool wait_commit_wg(uint64_t *bar, uint32_t &phase, unsigned int *err, unsigned int polls,
+                                               int id) {
+    bool ok = false;
+    const unsigned int lim = polls ? polls : kMbarPolls;
+    for (unsigned int it = 0; it < lim; it++)
+        if (mbar_try_wait(bar, phase)) { ok = true; break; }
+    phase ^= 1u;
+    if (wg_any(!ok, id)) {
+        if ((threadIdx.x & (SG_M - 1)) == 0) atomicExch(err, 1u);
+        return false;
+    }
+    tc_fence_after();
+    return true;
+}
+
+__global__ void __launch_bounds__(SG4_THREADS, 1) k_surrogate4(const SurrogateArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = tid >> 7, row = tid & (SG_M - 1);
+    const int bid = 1 + g;                        // named barrier of this warpgroup
+    uint64_t *bars = (uint64_t *)(smem + OFF4_MISC);
+    uint32_t *holder = (uint32_t *)(smem + OFF4_MISC + 64);
+    unsigned char *A = smem + OFF4_A + (size_t)g * SG_M * SG_H * 2;
+    const SurrogateAux *aux = a.aux;
+    {
+        const uint4 *src = (const uint4 *)a.wimg;
+        uint4 *dst = (uint4 *)smem;
+        for (int k = tid; k < SG_WTOT * 2 / 16; k += blockDim.x) dst[k] = __ldg(src + k);
+    }
+    if (tid == 0)
+        for (int k = 0; k < SG4_SLOTS; k++) mbar_init(bars + k, 1);
+    if (warp == 0) tmem_alloc(holder, SG4_TMEM_COLS);
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *holder;
+    const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t d_acc = tmem + 128u * (uint32_t)g;
+    const uint32_t sW[4] = {smem_u32(smem + OFF_W1), smem_u32(smem + OFF_W2), smem_u32(smem + OFF_W3),
+                            smem_u32(smem + OFF_W4)};
+    const float *bias[3] = {aux->b1, aux->b2, aux->b3};
+    const uint32_t sA = smem_u32(A);
+    uint64_t *bar = bars + g;
+    uint32_t phase = 0;
+    unsigned int my_fb = 0;
+    const bool raw = a.rawX != nullptr;
+    const long long step = raw ? 0 : *a.step_ptr;
+    const double t0 = (double)step * a.t_per_step;
+    const int ntiles = (a.n + SG_M - 1) / SG_M;
+    for (int tile = (int)blockIdx.x * SG4_SLOTS + g; tile < ntiles; tile += (int)gridDim.x * SG4_SLOTS) {
+        const int i = tile * SG_M + row;
+        const bool valid = i < a.n;
+        const bool inside = build_row(a, aux, step, raw, i, valid, row, A);
+        bool ok = true;
+#pragma unroll 1
+        for (int l = 0; l < 4 && ok; l++) {
+            fence_proxy_async();
+            tc_fence_before();
+            wg_sync(bid);
+            if (row == 0) {
+                tc_fence_after();
+                issue_layer(d_acc, sA, sW[l], l == 0 ? SG_KIN : SG_H, l == 3 ? SG_NOUT : SG_H, bar);
+            }
+            ok = wait_commit_wg(bar, phase, a.err, a.mbar_polls, bid);
+            if (ok && l < 3) {
+                hidden_epilogue(d_acc + lane_off, bias[l], A, row, 0);
+                hidden_epilogue(d_acc + lane_off, bias[l], A, row, 1);
+            }
+        }
+        if (!ok) break;
+        uint32_t yv[32];
+        tmem_ld32(d_acc + lane_off, yv);
+        tc_fence_before();
+        output_node(a, aux, i, valid, raw, inside, yv, t0, my_fb);
+        // the next tile's row build overwrites A: every thread of the slot
+        // is past its last read of this tile's TMEM and A above
+        wg_sync(bid);
+    }
+    for (int o = 16; o > 0; o >>= 1) my_fb += __shfl_xor_sync(0xffffffffu, my_fb, o);
+    if ((tid & 31) == 0 && my_fb && a.status) atomicAdd(&a.status->fallback, (unsigned long long)my_fb);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, SG4_TMEM_COLS);
 }
 
 // The hybrid form's physics for the nodes the network took: the reference's
@@ -484,19 +615,26 @@ __global__ void __launch_bounds__(128, 4) k_hybrid(const SurrogateArgs a) {
     }
 }
 
-int launch_surrogate(const SurrogateArgs &a, cudaStream_t s) {
-    static int configured = 0;
-    if (!configured) {
+// variant 0: k_surrogate, two CTAs of one tile pipeline per SM; 1:
+// k_surrogate4, one CTA of four tile pipelines per SM
+int launch_surrogate(const SurrogateArgs &a, cudaStream_t s, int variant) {
+    // the shared-memory limit is per kernel and per device; setting it again
+    // is cheap and keeps a second device right
+    if (variant == 1)
+        EP_CUDA(cudaFuncSetAttribute(k_surrogate4, cudaFuncAttributeMaxDynamicSharedMemorySize, SG4_SMEM));
+    else
         EP_CUDA(cudaFuncSetAttribute(k_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, SG_SMEM));
-        configured = 1;
-    }
     int dev = 0, nsm = 148;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int ntiles = (a.n + SG_M - 1) / SG_M;
-    const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
-    if (grid <= 0) return EP_OK;
-    k_surrogate<<<grid, SG_THREADS, SG_SMEM, s>>>(a);
+    if (ntiles <= 0) return EP_OK;
+    if (variant == 1) {
+        const int want = (ntiles + SG4_SLOTS - 1) / SG4_SLOTS;
+        k_surrogate4<<<want < nsm ? want : nsm, SG4_THREADS, SG4_SMEM, s>>>(a);
+    } else {
+        k_surrogate<<<ntiles < 2 * nsm ? ntiles : 2 * nsm, SG_THREADS, SG_SMEM, s>>>(a);
+    }
     EP_CUDA(cudaGetLastError());
     return EP_OK;
 }

@@ -73,7 +73,7 @@ struct SurrogateArgs {
     uint8_t *take;
 };
 
-int launch_surrogate(const SurrogateArgs &a, cudaStream_t s);
+int launch_surrogate(const SurrogateArgs &a, cudaStream_t s, int variant = 0);
 int launch_hybrid(const SurrogateArgs &a, cudaStream_t s);
 size_t surrogate_smem_bytes();
 

@@ -136,7 +136,7 @@ class Monodomain:
 
     def set_launch_config(self, cg_block=None, cg_per_sm=None, ionic_block=None, graph_steps=None,
                           ionic_min_ctas=None, cg_batch=None, cg_variant=None, cg_predict=None,
-                          cg_prefetch=None):
+                          cg_prefetch=None, sg_variant=None):
         cur = self.launch_config()
         c = capi.LaunchConfig()
         c.cg_block = cur["cg_block"] if cg_block is None else int(cg_block)
@@ -148,6 +148,7 @@ class Monodomain:
         c.cg_variant = cur["cg_variant"] if cg_variant is None else int(cg_variant)
         c.cg_predict = cur["cg_predict"] if cg_predict is None else int(cg_predict)
         c.cg_prefetch = cur["cg_prefetch"] if cg_prefetch is None else int(cg_prefetch)
+        c.sg_variant = cur["sg_variant"] if sg_variant is None else int(sg_variant)
         check(capi.lib().ep_set_launch_config(self._h, C.byref(c)))
 
     def autotune(self, trial_steps=20):
