@@ -366,7 +366,8 @@ typedef struct ep_launch_config {
  * built-in 2^24, seconds), mbar_polls one tensor-core completion wait of
  * the learned step (0 = 2^22).  A wait that runs out makes ep_step return
  * EP_ERR_TIMEOUT (stats->timeouts > 0); the handle's wait state is then
- * reset so it can step again, but V and the states of that call are not to
+ * reset so it can step again and its clock (step count, ECG samples) is put
+ * back to the call's start, but V and the states of that call are not to
  * be trusted (restore them with ep_set_voltage / ep_set_states). */
 int  ep_set_wait_limits(ep_handle *h, uint32_t grid_polls, uint32_t mbar_polls);
 /* Test hook for the timeout path (no reference counterpart): the CG grid

@@ -92,12 +92,15 @@ def test_single_reduction_variant_in_tissue(gpu):
 def test_gather_widths_are_bit_identical(gpu, shell, prec):
     """The gather width (4, 8, 8 pipelined, or the staged kernel with its
     slices brought into shared memory by bulk copies) changes which loads are
-    in flight together, not the order of the additions: same bits."""
+    in flight together, not the order of the additions: same bits on the
+    same grid.  (The grid decides how the FP64 dot products are split over
+    CTAs, so every kernel gets one CTA per SM: the staged kernel's ring can
+    fill most of an SM's shared memory.)"""
     wl, V, c = shell
     out = []
     for nb in (4, 8, 16, 32):
         g = Monodomain(wl.mesh, capi.TUSSCHER, prec, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
-        g.set_launch_config(cg_batch=nb, cg_per_sm=4)
+        g.set_launch_config(cg_batch=nb, cg_per_sm=1)
         g.set_voltage(V)
         it, rr = g.diffusion_half_step()
         out.append((g.voltage(), it))

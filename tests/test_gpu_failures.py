@@ -51,11 +51,15 @@ def test_grid_barrier_timeout(gpu):
     assert e.value.code == -8                              # EP_ERR_TIMEOUT
     assert g.last_stats["timeouts"] > 0
     assert waited < 5.0, waited                            # a short limit gives up promptly
-    # clear the hook, put the state back: the handle steps on as if nothing happened
+    assert g.time()[1] == 20                               # the failed call took no step
+    # clear the hook, put the state back: the handle steps on as if nothing
+    # happened.  A voltage upload restarts the CG start predictor, so the
+    # handle that never failed takes the same upload of its own voltage.
     g.test_hold_barrier(0)
     g.set_wait_limits(0, 0)
     g.set_voltage(V0)
     g.set_states(S0)
+    ref.set_voltage(ref.voltage())
     st = g.step(30)
     ref.step(30)
     assert st["timeouts"] == 0 and st["cg_failures"] == 0

@@ -1286,6 +1286,10 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
     EP_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(DevStatus), h->stream));
     EP_CUDA(cudaMemsetAsync(h->cg_stats.p, 0, 32, h->stream));
     EP_CUDA(cudaEventRecord(h->ev0, h->stream));
+    // the clock at entry: a call whose waits gave up did not take its steps
+    const long long step0 = h->step;
+    const int ecg_count0 = h->ecg_count;
+    const size_t ecg_t0 = h->ecg_t.size();
     size_t ne = 0;
     h->launches = 0;
     int rc = EP_OK;
@@ -1347,10 +1351,21 @@ int ep_step(ep_handle *h, int32_t nsteps, ep_step_stats *stats) {
     if (stats) stats->timeouts += (int32_t)sg_err;
     if (bar.err || sg_err) {
         // the kernels left early; put the wait state back so the handle can
-        // step again (the simulation state of this call is not to be trusted)
+        // step again, and the clock (host and device step counters, ECG
+        // samples) back to the call's start: the voltage and states are not
+        // to be trusted and are put back by the caller (ep_set_voltage,
+        // ep_set_states or ep_read_restart) before stepping on
         int rc2 = reset_barriers(h);
         if (rc2) return rc2;
         if (sg_err) EP_CUDA(cudaMemset(h->sg_err.p, 0, sizeof(unsigned int)));
+        h->step = step0;
+        h->ecg_count = ecg_count0;
+        h->ecg_t.resize(ecg_t0);
+        EP_CUDA(cudaMemcpy(h->d_step.p, &h->step, sizeof(long long), cudaMemcpyHostToDevice));
+        if (h->ecg_slot.p) {
+            const unsigned int slot = (unsigned int)ecg_count0;
+            EP_CUDA(cudaMemcpy(h->ecg_slot.p, &slot, sizeof slot, cudaMemcpyHostToDevice));
+        }
         set_error(bar.err ? "a grid barrier wait gave up" : "a tensor-core completion wait gave up");
         return EP_ERR_TIMEOUT;
     }
