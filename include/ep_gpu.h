@@ -337,9 +337,10 @@ int  ep_assemble_operators(const ep_mesh_desc *mesh, const ep_cables_desc *cable
  * cg_batch: SELL columns whose gathers the CG kernel issues together (4 or
  * 8; 8 keeps more loads in flight at a larger register budget; 16: groups of
  * 8 with the next group's index loads issued before the current gathers;
- * 32: staged -- each warp's next two slices of column indices and values are
- * brought into shared memory by bulk asynchronous copies while it gathers
- * the current one, at most 256 threads per CTA, cg_variant 0 only);
+ * 32: staged -- each warp copies its next units of 8 slice columns (column
+ * indices and values) into a ring of shared memory with asynchronous copies
+ * while it gathers the current one, cg_prefetch units ahead (1..4; 0 = 2),
+ * 256 threads per CTA, cg_variant 0 only);
  * cg_variant: 0 the CG recurrences of the reference (two reductions per
  * iteration), 1 the Chronopoulos-Gear recurrences (one reduction per
  * iteration; same iterates in exact arithmetic, rounding-level differences;
@@ -353,7 +354,9 @@ typedef struct ep_launch_config {
                              to B V - A V */
     int32_t cg_prefetch;  /* 0..4: each warp of the CG launch asks L2 for the
                              SELL indices and values of the slice it reads that
-                             many slices ahead (cg_variant 0; 0 = off) */
+                             many slices ahead (cg_variant 0; 0 = off); with
+                             cg_batch 32 the units the ring holds in flight
+                             (0 = 2) */
     int32_t sg_variant;   /* learned ionic step (EP_SURROGATE): 0 two CTAs per SM,
                              each one tile of 128 nodes at a time; 1 one CTA per SM
                              running four tiles at once in four warpgroups (one

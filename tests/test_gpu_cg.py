@@ -91,16 +91,16 @@ def test_single_reduction_variant_in_tissue(gpu):
 @pytest.mark.parametrize("prec", [capi.FP64, capi.FP32])
 def test_gather_widths_are_bit_identical(gpu, shell, prec):
     """The gather width (4, 8, 8 pipelined, or the staged kernel with its
-    slices brought into shared memory by bulk copies) changes which loads are
-    in flight together, not the order of the additions: same bits on the
-    same grid.  (The grid decides how the FP64 dot products are split over
+    units of slice columns copied asynchronously into shared memory) changes
+    which loads are in flight together, not the order of the additions: same
+    bits on the same grid.  (The grid decides how the FP64 dot products are split over
     CTAs, so every kernel gets one CTA per SM: the staged kernel's ring can
     fill most of an SM's shared memory.)"""
     wl, V, c = shell
     out = []
-    for nb in (4, 8, 16, 32):
+    for nb, pf in ((4, 0), (8, 0), (16, 0), (32, 0), (32, 1), (32, 3), (32, 4)):   # pf: the staged ring's depth
         g = Monodomain(wl.mesh, capi.TUSSCHER, prec, dt=wl.dt, ionic_dt=wl.ionic_dt, D=wl.D, cg_tol=1e-7)
-        g.set_launch_config(cg_batch=nb, cg_per_sm=1)
+        g.set_launch_config(cg_batch=nb, cg_per_sm=1, cg_prefetch=pf)
         g.set_voltage(V)
         it, rr = g.diffusion_half_step()
         out.append((g.voltage(), it))

@@ -72,7 +72,6 @@ struct ep_handle {
     int mh_abs = 0;
     long long step = 0;
     int nslices = 0;
-    int max_slice_w = 0;                 // widest SELL slice (columns)
     // device memory
     DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, zv, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
@@ -213,8 +212,9 @@ void fill_ionic_args(ep_handle *h, IonicArgs<R> &a) {
     a.stride_dt = (R)h->ionic_dt;
 }
 
-// columns of one stage of the staged CG's shared-memory ring
-static int stage_width(const ep_handle *h) { return std::max(1, std::min(h->max_slice_w, kStageMaxW)); }
+// units in flight per warp of the staged CG (cg_batch kStagedBatch): its
+// cg_prefetch, or the default depth
+static int stage_depth(const ep_handle *h) { return h->cg_prefetch > 0 ? h->cg_prefetch : kStageDepthDefault; }
 
 template <typename R>
 void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
@@ -238,9 +238,9 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
     a.delta = nullptr; a.delta_prev = nullptr; a.vin = nullptr;   // the time step sets the predictor
-    a.prefetch = h->cg_prefetch;
+    a.prefetch = h->cg_batch == kStagedBatch ? 0 : h->cg_prefetch;   // the staged kernel's is its ring depth
     a.bar_extra = h->bar_extra;
-    a.wstage = stage_width(h);
+    a.depth = stage_depth(h);
 }
 
 // start the CG predictor from x0 = V again (after a state upload or when it
@@ -260,9 +260,6 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
     Sell sell;
     pack_sell(csr, {&csr.A, &csr.B}, sell);
     h->nslices = sell.nslices;
-    h->max_slice_w = 0;
-    for (int k = 0; k < sell.nslices; k++)
-        h->max_slice_w = std::max(h->max_slice_w, (sell.slice_ptr[k + 1] - sell.slice_ptr[k]) / kSlice);
     if ((rc = upload_raw(h->slice_ptr, sell.slice_ptr.data(), sell.slice_ptr.size()))) return rc;
     if ((rc = upload_raw(h->col, sell.col.data(), sell.col.size()))) return rc;
     if ((rc = upload<R>(h->Aval, sell.vals[0]))) return rc;
@@ -443,7 +440,7 @@ static int reset_barriers(ep_handle *h) {
 }
 
 static int plan_cg(ep_handle *h) {
-    const int ws = stage_width(h);
+    const int ws = stage_depth(h);
     int rc = h->precision == EP_FP64
                  ? cg_grid_size<double>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant, ws)
                  : cg_grid_size<float>(h->cg_block, &h->cg_grid, h->cg_per_sm, h->cg_batch, h->cg_variant, ws);
@@ -1593,14 +1590,15 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
     EP_CUDA(cudaSetDevice(h->device));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     drop_graph(h);
-    const int ob = h->cg_block, op = h->cg_per_sm, obt = h->cg_batch, ov = h->cg_variant;
+    const int ob = h->cg_block, op = h->cg_per_sm, obt = h->cg_batch, ov = h->cg_variant, opf = h->cg_prefetch;
     h->cg_block = cfg->cg_block;
     h->cg_per_sm = cfg->cg_per_sm;
     h->cg_batch = cfg->cg_batch;
     h->cg_variant = cfg->cg_variant;
+    h->cg_prefetch = cfg->cg_prefetch;      // the staged kernel's ring depth sizes its launch
     int rc = plan_cg(h);
     if (rc) {
-        h->cg_block = ob; h->cg_per_sm = op; h->cg_batch = obt; h->cg_variant = ov;
+        h->cg_block = ob; h->cg_per_sm = op; h->cg_batch = obt; h->cg_variant = ov; h->cg_prefetch = opf;
         plan_cg(h);
         return rc;
     }
@@ -1622,7 +1620,6 @@ int ep_set_launch_config(ep_handle *h, const ep_launch_config *cfg) {
         EP_CUDA(cudaStreamSynchronize(h->stream));
     }
     h->cg_predict = cfg->cg_predict;
-    h->cg_prefetch = cfg->cg_prefetch;
     h->sg_variant = cfg->sg_variant;
     h->ionic_block = cfg->ionic_block;
     h->ionic_min = cfg->ionic_min_ctas;
@@ -1723,20 +1720,28 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
     // CG: gather width x CTA size x CTAs per SM (all that fit, or half:
     // fewer CTAs make the grid barrier cheaper)
     const ep_launch_config cg0 = b;
+    // (the staged kernel: 256 threads, ring depths 1..3 in cg_prefetch)
     for (int nb : {4, 8, 16, kStagedBatch}) {
         for (int blk : {128, 256, 512, 768}) {
-            int maxper = 0;
-            if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant, stage_width(h))
-                                         : cg_max_per_sm<float>(blk, &maxper, nb, cg0.cg_variant, stage_width(h))))
-                continue;
-            maxper = std::min(maxper, 8);
-            for (int per : {maxper, maxper / 2}) {
-                if (per < 1 || per * nsm < h->ninst) continue;
-                ep_launch_config c = cg0;
-                c.cg_block = blk; c.cg_per_sm = per; c.cg_batch = nb;
-                if (c.cg_block == cg0.cg_block && c.cg_per_sm == cg0.cg_per_sm && c.cg_batch == cg0.cg_batch) continue;
-                const double t = trial(c);
-                if (t >= 0 && t < t_best) { t_best = t; b = c; }
+            for (int dp : {1, 2, 3}) {
+                if (nb != kStagedBatch && dp > 1) break;
+                if (nb == kStagedBatch && (blk != 256 || cg0.cg_variant != 0)) break;
+                const int pf = nb == kStagedBatch ? dp : cg0.cg_prefetch;
+                int maxper = 0;
+                if ((h->precision == EP_FP64 ? cg_max_per_sm<double>(blk, &maxper, nb, cg0.cg_variant, dp)
+                                             : cg_max_per_sm<float>(blk, &maxper, nb, cg0.cg_variant, dp)))
+                    continue;
+                maxper = std::min(maxper, 8);
+                for (int per : {maxper, maxper / 2}) {
+                    if (per < 1 || per * nsm < h->ninst) continue;
+                    ep_launch_config c = cg0;
+                    c.cg_block = blk; c.cg_per_sm = per; c.cg_batch = nb; c.cg_prefetch = pf;
+                    if (c.cg_block == cg0.cg_block && c.cg_per_sm == cg0.cg_per_sm && c.cg_batch == cg0.cg_batch &&
+                        c.cg_prefetch == cg0.cg_prefetch)
+                        continue;
+                    const double t = trial(c);
+                    if (t >= 0 && t < t_best) { t_best = t; b = c; }
+                }
             }
         }
     }
@@ -1759,7 +1764,7 @@ int ep_autotune(ep_handle *h, int32_t trial_steps, ep_launch_config *best, doubl
         }
         const ep_launch_config b1 = b;
         for (int pf : {0, 2}) {
-            if (pf == b1.cg_prefetch) continue;
+            if (pf == b1.cg_prefetch || b1.cg_batch == kStagedBatch) continue;   // the staged kernel's depth is tuned above
             ep_launch_config c = b1;
             c.cg_prefetch = pf;
             const double t = trial(c);

@@ -570,44 +570,30 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
 
 // ---------------------------------------------------------------------------
 // k_cn_half_staged: the two-reduction solve of k_cn_half (same recurrences,
-// same order of additions, so the same bits), with the matrix stream of
-// phase A taken off the warps' critical path.  Each warp owns the slices
-// gwarp, gwarp + nwarps, ... of its instance; the bulk-copy engine brings the
-// column indices and A values of the warp's next two slices into a
-// two-stage ring in shared memory (cp.async.bulk, completion counted in
-// bytes on a per-stage mbarrier) while the warp gathers p and z for the
-// current one, so a warp waits on one L2 gather round per slice instead of a
-// chain of index load -> gather load trips.  The stream runs past the end of
-// a sweep into the next iteration's first slices (the matrix does not
-// change), so it overlaps phase B and the barriers too.  The copies carry an
-// L2 evict-first hint: the matrix streams through once per iteration while
-// the vectors it gathers stay in L2.  Slices wider than the ring's stage
-// (wstage columns) are read directly, as in k_cn_half.
-//
-// Every mbarrier wait is bounded (kStagePolls try-waits): a wait that runs
-// out sets the barrier's error word (the grid leaves at the next grid
-// barrier, the host reports EP_ERR_TIMEOUT) and the warp carries on with
-// direct loads.  No exit path leaves a copy in flight: the warp waits
-// (again bounded) for its outstanding stages before it returns.
-constexpr unsigned int kStagePolls = 1u << 22;
+// same order of additions, so the same bits on the same grid) with the matrix
+// stream of phase A taken off the warps' critical path.  A warp's slices are
+// cut into units of kUnitCols slice columns: the column indices and A values
+// of one slice's columns k .. k+7 (8 x 128 bytes of indices, 8 x 32 x
+// sizeof(R) bytes of values).  The warp copies the units into a ring of
+// shared memory with per-thread asynchronous copies (cp.async.cg: 16 bytes
+// each, L2 only, evict-first, so the matrix streams through L2 while the
+// gathered vectors stay there), `depth` units ahead of the one it gathers
+// for.  The DRAM latency of the index -> gather chain is then hidden behind
+// the gathers of the units before it, and the loads in flight occupy ring
+// slots instead of registers.  The stream runs on past the end of a sweep
+// into the next iteration's first units (the matrix does not change), under
+// phase B and the grid barriers.  No wait in this kernel spins:
+// cp.async.wait_group is the hardware's wait for the thread's own copies, and
+// every exit path waits for all of them before the CTA leaves.
+constexpr int kUnitCols = 8;
+
+__host__ __device__ inline size_t unit_bytes(int rsize) { return (size_t)kUnitCols * kSlice * (4 + (size_t)rsize); }
+// dynamic shared memory of a CTA of `block` threads, `depth` units in flight per warp
+__host__ __device__ inline size_t stage_smem_bytes(int block, int depth, int rsize) {
+    return (size_t)(block / 32) * (size_t)(depth + 1) * unit_bytes(rsize);
+}
 
 __device__ __forceinline__ uint32_t cg_smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void stage_mbar_init(uint64_t *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(cg_smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool stage_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P;\n\t}"
-        : "=r"(ok)
-        : "r"(cg_smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
 __device__ __forceinline__ uint64_t l2_evict_first_policy() {
     uint64_t pol;
@@ -615,108 +601,80 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy() {
     return pol;
 }
 
-// one global -> shared bulk copy completing on bar (16-byte aligned, bytes a
-// multiple of 16: SELL slices start on 128-byte boundaries and span w x 128
-// bytes of indices and w x 32 x sizeof(R) bytes of values)
-__device__ __forceinline__ void stage_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar, uint64_t pol) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
-        ::"r"(cg_smem_u32(dst)), "l"(src), "r"(bytes), "r"(cg_smem_u32(bar)), "l"(pol)
-        : "memory");
+// one 16-byte global -> shared copy, cached in L2 only (both addresses
+// 16-byte aligned: every unit starts on a 128-byte boundary of the SELL
+// arrays and of the ring)
+__device__ __forceinline__ void cp16(void *dst, const void *src, uint64_t pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(cg_smem_u32(dst)), "l"(src),
+                 "l"(pol)
+                 : "memory");
 }
-
-// shared-memory bytes of the ring for a CTA of `block` threads
-__host__ __device__ inline size_t stage_bytes_per_warp(int wstage, int rsize) {
-    return (size_t)2 * wstage * kSlice * (4 + rsize);
-}
-__host__ __device__ inline size_t stage_smem_bytes(int block, int wstage, int rsize) {
-    const int nw = block / 32;
-    return (size_t)nw * 2 * sizeof(uint64_t) + 128 + (size_t)nw * stage_bytes_per_warp(wstage, rsize);
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// this thread's copies of every unit but the newest depth - 1 have landed
+__device__ __forceinline__ void unit_wait(int depth) {
+    switch (depth) {
+        case 1: cp_wait<0>(); break;
+        case 2: cp_wait<1>(); break;
+        case 3: cp_wait<2>(); break;
+        default: cp_wait<3>(); break;
+    }
 }
 
 template <typename R>
-struct StageRing {
-    uint64_t *bar;            // 2 mbarriers of this warp
-    int *col0;                // stage k's indices at col0 + k * wstage * 32
-    R *val0;                  // stage k's values at val0 + k * wstage * 32
-    int wstage;
-    int L;                    // slices of this warp per sweep
-    int next;                 // ring position of the next fill
-    uint32_t phase;           // bit k: parity of stage k's next completion
-    uint32_t pend;            // bit k: stage k has a fill in flight (warp-uniform)
+struct UnitRing {
+    int *idx;          // slot k's indices at idx + k * kUnitCols * kSlice
+    R *val;            // slot k's values at val + k * kUnitCols * kSlice
+    int slots, depth;  // slots = depth + 1
+    int L;             // this warp's slices per sweep (0: nothing to stage)
+    int j, k, beg, w;  // producer cursor: slice j of the warp, its column k, start, width
+    int issued;        // units issued so far
     uint64_t pol;
 };
 
-// fill the stage of ring position pos with its slice, when the slice is
-// narrow enough to be staged (every lane takes the same decision)
+// issue the unit under the cursor into the ring slot of its position and
+// advance the cursor (the next unit of the slice, or the next slice,
+// wrapping to the warp's first slice: the next sweep).  Every lane commits
+// one copy group per call, empty or not, so the group counts stay uniform.
 template <typename R>
-__device__ __forceinline__ void stage_fill(StageRing<R> &q, const CGArgs<R> &a, int gwarp, int nwarps, int lane) {
-    if (q.L <= 0) return;
-    const int pos = q.next++;
-    const int k = pos & 1;
-    const int s = gwarp + (pos % q.L) * nwarps;
-    const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-    if (w > q.wstage || w <= 0) return;
-    q.pend |= 1u << k;
-    if (lane == 0) {
-        const uint32_t bc = (uint32_t)w * kSlice * 4u, bv = (uint32_t)w * kSlice * (uint32_t)sizeof(R);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cg_smem_u32(q.bar + k)),
-                     "r"(bc + bv)
-                     : "memory");
-        const int off = k * q.wstage * kSlice;
-        stage_copy(q.col0 + off, a.col + beg, bc, q.bar + k, q.pol);
-        stage_copy(q.val0 + off, a.Aval + beg, bv, q.bar + k, q.pol);
+__device__ __forceinline__ void unit_issue(UnitRing<R> &q, const CGArgs<R> &a, int gwarp, int nwarps, int lane) {
+    if (q.L > 0) {
+        const int slot = q.issued % q.slots;
+        const int nc = min(kUnitCols, q.w - q.k);
+        int *di = q.idx + slot * (kUnitCols * kSlice);
+        R *dv = q.val + slot * (kUnitCols * kSlice);
+        const int *si = a.col + q.beg + q.k * kSlice;
+        const R *sv = a.Aval + q.beg + q.k * kSlice;
+        // indices: column u, 16-byte piece p is chunk c = 8 u + p
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const int c = lane + 32 * t;
+            if ((c >> 3) < nc) cp16(di + 4 * c, si + 4 * c, q.pol);
+        }
+        // values: VPC chunks of VE values per column
+        constexpr int VPC = kSlice * (int)sizeof(R) / 16, VE = 16 / (int)sizeof(R);
+#pragma unroll
+        for (int t = 0; t < VPC * kUnitCols / 32; t++) {
+            const int c = lane + 32 * t;
+            if (c / VPC < nc) cp16(dv + VE * c, sv + VE * c, q.pol);
+        }
+        q.k += kUnitCols;
+        while (q.k >= q.w) {               // ends: some slice of the warp has columns (q.L > 0)
+            q.j = q.j + 1 == q.L ? 0 : q.j + 1;
+            const int s = gwarp + q.j * nwarps;
+            q.beg = __ldg(a.slice_ptr + s);
+            q.w = (__ldg(a.slice_ptr + s + 1) - q.beg) / kSlice;
+            q.k = 0;
+        }
     }
-}
-
-// wait for stage k's fill (bounded); false when the wait ran out
-template <typename R>
-__device__ __forceinline__ bool stage_wait(StageRing<R> &q, int k) {
-    const uint32_t par = (q.phase >> k) & 1u;
-    bool ok = false;
-    for (unsigned int it = 0; it < kStagePolls; it++)
-        if (stage_try_wait(q.bar + k, par)) { ok = true; break; }
-    ok = __all_sync(0xffffffffu, ok);
-    q.phase ^= 1u << k;
-    q.pend &= ~(1u << k);
-    return ok;
-}
-
-// before the warp leaves: every fill it issued has landed
-template <typename R>
-__device__ __forceinline__ void stage_drain(StageRing<R> &q) {
-    for (int k = 0; k < 2; k++)
-        if (q.pend & (1u << k)) stage_wait(q, k);
-}
-
-// row sums of one staged slice (indices and values in shared memory): NB
-// columns' gathers issued together, the products added in column order (the
-// order of slice_row_sum, so the sums are the same bits)
-template <int NB, typename R, typename F>
-__device__ __forceinline__ R smem_row_sum(const int *col, const R *val, int w, int lane, F gather) {
-    R acc = R(0);
-    for (int k = 0; k < w; k += NB) {
-        int c[NB];
-        R v[NB], g[NB];
-#pragma unroll
-        for (int u = 0; u < NB; u++)
-            if (k + u < w) {
-                c[u] = col[(k + u) * kSlice + lane];
-                v[u] = val[(k + u) * kSlice + lane];
-            }
-#pragma unroll
-        for (int u = 0; u < NB; u++)
-            if (k + u < w) g[u] = gather(c[u]);
-#pragma unroll
-        for (int u = 0; u < NB; u++)
-            if (k + u < w) acc += v[u] * g[u];
-    }
-    return acc;
+    q.issued++;
+    cp_commit();
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(const CGArgs<R> a) {
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(const CGArgs<R> a) {
     extern __shared__ __align__(128) unsigned char cg_sm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int G = gridDim.x;
@@ -737,35 +695,37 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
     const int gwarp = s_lo + (((int)blockIdx.x - b0) * (int)blockDim.x + (int)threadIdx.x) / 32;
     const int nwarps = (nb * (int)blockDim.x) >> 5;
 
-    // this warp's ring: mbarriers first, then the stages (128-byte aligned)
-    StageRing<R> q;
+    // this warp's ring: slots x unit of indices, then slots x unit of values
+    UnitRing<R> q;
     {
-        const int nw = blockDim.x >> 5;
-        uint64_t *bars = reinterpret_cast<uint64_t *>(cg_sm);
-        unsigned char *base = cg_sm + ((nw * 2 * sizeof(uint64_t) + 127) & ~(size_t)127) +
-                              (size_t)wib * stage_bytes_per_warp(a.wstage, (int)sizeof(R));
-        const size_t cb = (size_t)a.wstage * kSlice * 4, vb = (size_t)a.wstage * kSlice * sizeof(R);
-        q.bar = bars + 2 * wib;
-        q.col0 = reinterpret_cast<int *>(base);
-        q.val0 = reinterpret_cast<R *>(base + 2 * cb);
-        (void)vb;
-        q.wstage = a.wstage;
+        q.depth = a.depth;
+        q.slots = a.depth + 1;
+        unsigned char *base = cg_sm + (size_t)wib * q.slots * unit_bytes((int)sizeof(R));
+        q.idx = reinterpret_cast<int *>(base);
+        q.val = reinterpret_cast<R *>(base + (size_t)q.slots * kUnitCols * kSlice * 4);
         q.L = gwarp < s_hi ? (s_hi - gwarp + nwarps - 1) / nwarps : 0;
-        q.next = 0;
-        q.phase = 0;
-        q.pend = 0;
-        q.pol = l2_evict_first_policy();
-        if (lane == 0) {
-            stage_mbar_init(q.bar);
-            stage_mbar_init(q.bar + 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        int cols = 0;
+        for (int j = 0; j < q.L; j++) {
+            const int s = gwarp + j * nwarps;
+            cols += __ldg(a.slice_ptr + s + 1) - __ldg(a.slice_ptr + s);
         }
-        __syncwarp();
+        if (cols == 0) q.L = 0;
+        q.j = 0;
+        q.k = 0;
+        q.beg = q.L > 0 ? __ldg(a.slice_ptr + gwarp) : 0;
+        q.w = q.L > 0 ? (__ldg(a.slice_ptr + gwarp + 1) - q.beg) / kSlice : 0;
+        while (q.L > 0 && q.w == 0) {      // ends: some slice has columns
+            q.j++;
+            const int s = gwarp + q.j * nwarps;
+            q.beg = __ldg(a.slice_ptr + s);
+            q.w = (__ldg(a.slice_ptr + s + 1) - q.beg) / kSlice;
+        }
+        q.issued = 0;
+        q.pol = l2_evict_first_policy();
     }
-    // the first two slices start streaming under the prologue
-    stage_fill(q, a, gwarp, nwarps, lane);
-    stage_fill(q, a, gwarp, nwarps, lane);
-    int cons = 0;                             // ring position of the next slice to consume
+    // the first units start streaming under the prologue
+    for (int d = 0; d < q.depth; d++) unit_issue(q, a, gwarp, nwarps, lane);
+    int cons = 0;                             // units consumed so far
 
     // ---- prologue: as k_cn_half ----
     const bool pred = a.delta != nullptr;
@@ -795,7 +755,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
         }
         block_reduce_store<4>(v, a.partial + 6 * G, G);
     }
-    if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+    if (!grid_sync(bar, nblk)) { cp_wait_all(); return; }
     double rz, rr_start, bb, rr0;
     {
         double t[4];
@@ -810,30 +770,36 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
     double rr_last = rr_start;
     R *pc = a.p0, *pn = a.p1;
     while (!converged && it < a.maxit) {
-        // ---- phase A: q = A p', p' = z + beta p, from the staged slices ----
+        // ---- phase A: q = A p', p' = z + beta p, the units from the ring ----
         {
             double v[1] = {0.0};
             const R bR = (R)beta;
             const R *pcc = pc;
-            auto gat = [&](int c) { return pdir_z(ldcg(a.z + c), bR, ldcg(pcc + c)); };
-            for (int s = gwarp; s < s_hi; s += nwarps, cons++) {
+            for (int s = gwarp; s < s_hi; s += nwarps) {
                 const int row = s * kSlice + lane;
-                const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-                const int k = cons & 1;
-                R qv;
-                bool staged = w <= q.wstage && w > 0;
-                if (staged && !stage_wait(q, k)) {
-                    if (lane == 0) atomicExch(&bar->err, 1u);
-                    staged = false;
+                const int beg = __ldg(a.slice_ptr + s), w = (__ldg(a.slice_ptr + s + 1) - beg) / kSlice;
+                R qv = R(0);
+                for (int k = 0; k < w; k += kUnitCols, cons++) {
+                    unit_wait(q.depth);
+                    __syncwarp();                 // the unit is visible to every lane, and every
+                                                  // lane is done with the slot refilled next
+                    unit_issue(q, a, gwarp, nwarps, lane);
+                    const int off = (cons % q.slots) * (kUnitCols * kSlice) + lane;
+                    const int *ci = q.idx + off;
+                    const R *cv = q.val + off;
+                    const int nc = min(kUnitCols, w - k);
+                    int c[kUnitCols];
+                    R g[kUnitCols];
+#pragma unroll
+                    for (int u = 0; u < kUnitCols; u++)
+                        if (u < nc) c[u] = ci[u * kSlice];
+#pragma unroll
+                    for (int u = 0; u < kUnitCols; u++)
+                        if (u < nc) g[u] = pdir_z(ldcg(a.z + c[u]), bR, ldcg(pcc + c[u]));
+#pragma unroll
+                    for (int u = 0; u < kUnitCols; u++)
+                        if (u < nc) qv += cv[u * kSlice] * g[u];
                 }
-                if (staged) {
-                    const int off = k * q.wstage * kSlice;
-                    qv = smem_row_sum<8>(q.col0 + off, q.val0 + off, w, lane, gat);
-                    __syncwarp();                 // every lane is done with stage k
-                } else {
-                    qv = slice_row_sum<8>(a.col, a.Aval, beg, w, lane, gat);
-                }
-                stage_fill(q, a, gwarp, nwarps, lane);   // refill stage k two slices ahead
                 if (row >= rb && row < re) {
                     const R pi = pdir_z(a.z[row], bR, ldcg(pc + row));
                     pn[row] = pi;
@@ -843,7 +809,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
             }
             block_reduce_store<1>(v, a.partial + 3 * G, G);
         }
-        if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+        if (!grid_sync(bar, nblk)) { cp_wait_all(); return; }
         double pq;
         {
             double t[1];
@@ -884,7 +850,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
             }
             block_reduce_store<2>(v, a.partial, G);
         }
-        if (!grid_sync(bar, nblk)) { stage_drain(q); return; }
+        if (!grid_sync(bar, nblk)) { cp_wait_all(); return; }
         double t[2];
         grid_total<2>(a.partial, G, b0, nb, t);
         it++;
@@ -895,7 +861,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
         rz = t[0];
         R *tmp = pc; pc = pn; pn = tmp;
     }
-    stage_drain(q);                           // the fills that ran ahead into the next sweep
+    cp_wait_all();                            // the units that ran ahead into the next sweep
     if (pred) {
         for (int s = gwarp; s < s_hi; s += nwarps) {
             const int row = s * kSlice + lane;
@@ -920,23 +886,26 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3) k_cn_half_staged(
 }
 
 // the kernel of a (gather width, variant) choice and its dynamic shared
-// memory; cg_batch kStagedBatch selects k_cn_half_staged (ring of wstage
-// columns per stage)
+// memory; cg_batch kStagedBatch selects k_cn_half_staged with `depth` units
+// in flight per warp (1 .. kStageMaxDepth)
 // (set_attr: allow the staged kernel the largest ring any handle can ask
-// for -- 256 threads, kStageMaxW columns -- once, from the planning path,
+// for -- 256 threads, kStageMaxDepth units -- once, from the planning path,
 // never during a stream capture; the attribute only caps the request)
 template <typename R>
-static int cg_kernel(int block, int batch, int variant, int wstage, const void **fn, size_t *smem,
+static int cg_kernel(int block, int batch, int variant, int depth, const void **fn, size_t *smem,
                      bool set_attr) {
     *smem = 0;
     if (batch == kStagedBatch) {
         if (variant != 0) { set_error("the staged CG runs the two-reduction recurrences only"); return EP_ERR_ARG; }
-        if (wstage < 1 || wstage > kStageMaxW) { set_error("staged CG: stage width %d out of range", wstage); return EP_ERR_ARG; }
+        if (depth < 1 || depth > kStageMaxDepth) {
+            set_error("staged CG: %d units in flight, not 1..%d", depth, kStageMaxDepth);
+            return EP_ERR_ARG;
+        }
         *fn = (const void *)k_cn_half_staged<R>;
-        *smem = stage_smem_bytes(block, wstage, (int)sizeof(R));
+        *smem = stage_smem_bytes(block, depth, (int)sizeof(R));
         if (set_attr)
             EP_CUDA(cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)stage_smem_bytes(256, kStageMaxW, (int)sizeof(R))));
+                                         (int)stage_smem_bytes(256, kStageMaxDepth, (int)sizeof(R))));
         return EP_OK;
     }
     *fn = variant == 1 ? (batch >= 8 ? (const void *)k_cn_half_cg1<R, 8> : (const void *)k_cn_half_cg1<R, 4>)
@@ -947,10 +916,10 @@ static int cg_kernel(int block, int batch, int variant, int wstage, const void *
 }
 
 template <typename R>
-int cg_max_per_sm(int block, int *per, int batch, int variant, int wstage) {
+int cg_max_per_sm(int block, int *per, int batch, int variant, int depth) {
     const void *fn = nullptr;
     size_t smem = 0;
-    int rc = cg_kernel<R>(block, batch, variant, wstage, &fn, &smem, true);
+    int rc = cg_kernel<R>(block, batch, variant, depth, &fn, &smem, true);
     if (rc) return rc;
     cudaFuncAttributes fa;
     EP_CUDA(cudaFuncGetAttributes(&fa, fn));
@@ -964,11 +933,11 @@ int cg_max_per_sm(int block, int *per, int batch, int variant, int wstage) {
 }
 
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm, int batch, int variant, int wstage) {
+int cg_grid_size(int block, int *grid, int per_sm, int batch, int variant, int depth) {
     int dev = 0, nsm = 0, per = 0;
     EP_CUDA(cudaGetDevice(&dev));
     EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int rc = cg_max_per_sm<R>(block, &per, batch, variant, wstage);
+    int rc = cg_max_per_sm<R>(block, &per, batch, variant, depth);
     if (rc) return rc;
     if (per_sm > 0 && per_sm < per) per = per_sm;
     *grid = nsm * per;
@@ -990,7 +959,7 @@ int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch
     if (batch == kStagedBatch) {
         const void *fn = nullptr;
         size_t smem = 0;
-        int rc = cg_kernel<R>(block, batch, variant, a.wstage, &fn, &smem, false);
+        int rc = cg_kernel<R>(block, batch, variant, a.depth, &fn, &smem, false);
         if (rc) return rc;
         cfg.dynamicSmemBytes = smem;
         EP_CUDA(cudaLaunchKernelEx(&cfg, k_cn_half_staged<R>, a));

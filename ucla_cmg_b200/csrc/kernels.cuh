@@ -125,15 +125,17 @@ template <typename R> struct CGArgs {
     // arrivals the grid barrier waits for beyond the CTAs that exist (0;
     // > 0 only from ep_test_hold_barrier, to make the bounded wait run out)
     unsigned int bar_extra;
-    // staged variant (cg_batch kStagedBatch): SELL columns one shared-memory
-    // stage holds; wider slices are read directly
-    int wstage;
+    // staged variant (cg_batch kStagedBatch): units of 8 slice columns each
+    // warp keeps in flight in its shared-memory ring (1 .. kStageMaxDepth)
+    int depth;
 };
 
-// cg_batch value of the staged kernel (bulk copies of each warp's next
-// slices into shared memory) and the widest stage it takes
+// cg_batch value of the staged kernel (asynchronous copies of each warp's
+// next units of SELL columns into shared memory), its deepest ring and the
+// depth it runs at when none is asked for
 constexpr int kStagedBatch = 32;
-constexpr int kStageMaxW = 32;
+constexpr int kStageMaxDepth = 4;
+constexpr int kStageDepthDefault = 2;
 
 // batch: SELL columns gathered per group (4 or 8; two register budgets);
 // variant 0: the two-reduction CG of the reference, 1: Chronopoulos-Gear
@@ -142,9 +144,9 @@ template <typename R>
 int launch_cg(const CGArgs<R> &a, int grid, int block, cudaStream_t s, int batch = 4, int variant = 0);
 // CTAs of the persistent launch: per_sm (0 = as many as fit) x SM count
 template <typename R>
-int cg_grid_size(int block, int *grid, int per_sm = 0, int batch = 4, int variant = 0, int wstage = 0);
+int cg_grid_size(int block, int *grid, int per_sm = 0, int batch = 4, int variant = 0, int depth = 0);
 template <typename R>
-int cg_max_per_sm(int block, int *per, int batch = 4, int variant = 0, int wstage = 0);
+int cg_max_per_sm(int block, int *per, int batch = 4, int variant = 0, int depth = 0);
 
 // ECG_k = sum_i W[k n + i] V[i] (ComputeECG.h:172-189 in per-node form),
 // deterministic two-level reduction, written to out[k].
