@@ -17,11 +17,16 @@ struct Track { float t_act, t_rep, v_peak, v_rest; };
 // the interval's start crossed during the preceding diffusion half step and
 // is stamped t0 (at most dt/2 late).  Activation: upward crossing of thr;
 // repolarisation (APD90): downward crossing of v_peak - 0.9 (v_peak - v_rest)
-// later than 5 ms after activation.
+// later than 5 ms after activation, v_rest = the node's voltage at its first
+// tracked interval (the diastolic level the run starts from).  Not the
+// minimum before activation: ahead of a steep front the consistent-mass
+// Crank-Nicolson step undershoots rest by several mV for a few tenths of a
+// ms, and a level taken from that dip falls into the slow end of
+// repolarisation (< 0.01 mV/ms), where 1 mV moves the crossing by ~100 ms.
 __device__ __forceinline__ void track_interval(Track &tr, bool &dirty, float v0, float v1, double t0, float h,
                                                float thr) {
     if (tr.t_act < 0.f) {
-        if (v0 < tr.v_rest) { tr.v_rest = v0; dirty = true; }
+        if (tr.v_rest > 1e29f) { tr.v_rest = v0; dirty = true; }
         if (v0 >= thr) {
             tr.t_act = (float)t0;
             tr.v_peak = fmaxf(v0, v1);
