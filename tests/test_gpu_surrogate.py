@@ -21,16 +21,16 @@ from ucla_cmg_b200.simulation import Monodomain
 pytestmark = pytest.mark.gpu
 
 
-def _setup():
-    m = M.slab(41, 41, 5, 0.8, 0.8, 0.08)
+def _setup(nx=41, ny=41):
+    m = M.slab(nx, ny, 5, 0.02 * (nx - 1), 0.02 * (ny - 1), 0.08)
     node_type = np.where(m.xyz[:, 0] < 0.32, 0, np.where(m.xyz[:, 0] < 0.56, 1, 2)).astype(np.uint8)
     gks = 0.8 + 0.4 * m.xyz[:, 1] / 0.8
     blk = np.where((m.xyz[:, 0] < 0.07) & (m.xyz[:, 1] < 0.07))[0].astype(np.int32)
     return m, node_type, gks, blk
 
 
-def _run(prec, sg=None, T=60.0, ecg=True):
-    m, node_type, gks, blk = _setup()
+def _run(prec, sg=None, T=60.0, ecg=True, size=(41, 41)):
+    m, node_type, gks, blk = _setup(*size)
     g = Monodomain(m, capi.TUSSCHER, prec, dt=0.1, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
                    node_type=node_type, type_consts=W.tt_type_consts(), gks_scale=gks,
                    tt_jacobian=capi.TT_JAC_TRUE, ecg_every=10 if ecg else 0)
@@ -67,6 +67,22 @@ def test_empty_envelope_is_the_plain_model(gpu):
     a = _run(capi.SURROGATE, s, T=20.0)
     b = _run(capi.FP32, None, T=20.0)
     assert a["fb"] == 1.0
+    assert np.array_equal(a["V"], b["V"])
+    assert np.array_equal(a["ta"], b["ta"])
+
+
+def test_short_fallback_list_runs_by_warps_with_the_same_bits(gpu):
+    """A fallback list of at most 4096 nodes runs one warp per node (the
+    Jacobian's rate evaluations side by side); it reproduces the one-thread-
+    per-node model bit for bit: an empty envelope on a 765-node slab sends
+    every node down that path, and the run equals the EP_FP32 handle's."""
+    s = _trained()
+    s.env_lo = np.full_like(s.env_lo, 1e30)
+    s.env_hi = np.full_like(s.env_hi, -1e30)
+    a = _run(capi.SURROGATE, s, T=20.0, size=(17, 9))
+    b = _run(capi.FP32, None, T=20.0, size=(17, 9))
+    assert a["fb"] == 1.0
+    assert np.max(b["V"]) > 0.0
     assert np.array_equal(a["V"], b["V"])
     assert np.array_equal(a["ta"], b["ta"])
 

@@ -537,6 +537,7 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
+    fb.list_warp_max = kFallbackWarpMax;    // a short list: one warp per node
     return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block, h->ionic_min);
 }
 
@@ -618,7 +619,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
         if constexpr (sizeof(R) == 4) {
             if (h->precision == EP_SURROGATE) {
                 if ((rc = launch_learned_phase(h, ia))) return rc;
-                h->launches += h->sg_vupdate == 2 ? 3 : 2;
+                h->launches += h->sg_vupdate == 2 ? 4 : 3;   // network, [physics,] fallback by warps and by threads
             } else if ((rc = ionic_phase<R>(h, ia))) {
                 return rc;
             }

@@ -30,10 +30,12 @@ __device__ __forceinline__ void track_update(Track &tr, bool &dirty, R v0, R v1,
     track_interval(tr, dirty, (float)v0, (float)v1, t0, (float)h, (float)thr);
 }
 
-// one node's ionic phase (all sub-steps), counters accumulated by the caller
-template <typename R, int MODEL, int NS>
+// one node's ionic phase (all sub-steps), counters accumulated by the caller;
+// WARP: the whole warp advances node i (ten Tusscher; every lane computes the
+// same values, lane 0 counts and stores)
+template <typename R, int MODEL, int NS, bool WARP = false>
 __device__ __forceinline__ void ionic_node(const IonicArgs<R> &a, const int i, unsigned int &my_newton,
-                                           unsigned int &my_caps, unsigned int &my_bad) {
+                                           unsigned int &my_caps, unsigned int &my_bad, int lane = 0) {
     const long long step = *a.step_ptr;
     const double t_start = (double)step * a.t_per_step;
     R V = a.V[i];
@@ -76,9 +78,12 @@ __device__ __forceinline__ void ionic_node(const IonicArgs<R> &a, const int i, u
             const R *__restrict__ c = a.consts + (size_t)ty * a.nconst;
             const R gks = a.gks ? a.gks[i] : R(1);
             int it = 0;
-            dvdt = tt_compute_ion<R>(s + 1, V, -istim / (a.Cm * a.Xi), h, c, gks, a.tt, it);
-            my_newton += it;
-            if (it >= a.tt.newton_cap) my_caps++;
+            if constexpr (WARP) dvdt = tt_compute_ion_warp<R>(s + 1, V, -istim / (a.Cm * a.Xi), h, c, gks, a.tt, it, lane);
+            else dvdt = tt_compute_ion<R>(s + 1, V, -istim / (a.Cm * a.Xi), h, c, gks, a.tt, it);
+            if (!WARP || lane == 0) {
+                my_newton += it;
+                if (it >= a.tt.newton_cap) my_caps++;
+            }
         } else if constexpr (MODEL == EP_MAHAJAN || MODEL == EP_MAHAJAN_FAIL) {
             const R *__restrict__ c = a.consts + (size_t)ty * a.nconst;
             int sub = 0;
@@ -107,6 +112,7 @@ __device__ __forceinline__ void ionic_node(const IonicArgs<R> &a, const int i, u
             }
         }
     }
+    if (WARP && lane != 0) return;
     if (!isfinite((double)V)) my_bad = 1;
     if (a.dvdt_out) a.dvdt_out[i] = last;
     else a.V[i] = V;
@@ -127,7 +133,8 @@ __global__ void __launch_bounds__(128, MINB) k_ionic(const IonicArgs<R> a) {
     // every node or the fallback list of the learned step (the nodes it
     // could not take).  One call site, so both modes run the same machine
     // code and a node's result does not depend on which mode advanced it.
-    const int cnt = a.node_list ? *a.list_count : a.n;
+    int cnt = a.node_list ? *a.list_count : a.n;
+    if (a.node_list && a.list_warp_max > 0 && cnt <= a.list_warp_max) cnt = 0;   // k_ionic_warp takes it
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
         const int node = a.node_list ? a.node_list[k] : k;
         if (a.skip && a.skip[node]) continue;
@@ -140,6 +147,41 @@ __global__ void __launch_bounds__(128, MINB) k_ionic(const IonicArgs<R> a) {
         my_bad += __shfl_xor_sync(0xffffffffu, my_bad, o);
     }
     if ((threadIdx.x & 31) == 0) {
+        if (my_newton) atomicAdd(&s_newton, (unsigned long long)my_newton);
+        if (my_caps) atomicAdd(&s_caps, my_caps);
+        if (my_bad) atomicAdd(&s_bad, my_bad);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_newton) atomicAdd(&a.status->newton_iters, s_newton);
+        if (s_caps) atomicAdd(&a.status->newton_cap_hits, s_caps);
+        if (s_bad) atomicAdd(&a.status->nonfinite, s_bad);
+    }
+}
+
+// A short ten Tusscher node list (at most list_warp_max nodes: the learned
+// step's fallback nodes, mostly upstrokes) one warp per node.  Its cost is the
+// serial chain of one node's Newton iterations, not throughput, and the warp
+// runs the Jacobian's 12 rate evaluations side by side
+// (tt_compute_ion_warp: the same bits as one thread per node).
+template <typename R>
+__global__ void __launch_bounds__(128) k_ionic_warp(const IonicArgs<R> a) {
+    __shared__ unsigned long long s_newton;
+    __shared__ unsigned int s_caps, s_bad;
+    if (threadIdx.x == 0) { s_newton = 0; s_caps = 0; s_bad = 0; }
+    __syncthreads();
+    unsigned int my_newton = 0, my_caps = 0, my_bad = 0;
+    const int cnt = *a.list_count;
+    if (cnt <= a.list_warp_max) {            // else k_ionic takes the list
+        const int lane = threadIdx.x & 31;
+        const int nw = (int)(gridDim.x * blockDim.x) >> 5;
+        for (int k = (int)(blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < cnt; k += nw) {
+            const int node = a.node_list[k];
+            if (a.skip && a.skip[node]) continue;
+            ionic_node<R, EP_TUSSCHER, TT_NS, true>(a, node, my_newton, my_caps, my_bad, lane);
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {           // lane 0 holds each warp's counts
         if (my_newton) atomicAdd(&s_newton, (unsigned long long)my_newton);
         if (my_caps) atomicAdd(&s_caps, my_caps);
         if (my_bad) atomicAdd(&s_bad, my_bad);
@@ -188,6 +230,20 @@ int launch_ionic(int model, const IonicArgs<R> &a, cudaStream_t st, int block, i
         EP_CUDA(cudaGetDevice(&dev));
         EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         grid = std::min(grid, 16 * nsm);   // one node per thread up to ~300K listed nodes
+    }
+    if (a.node_list && a.list_warp_max > 0) {
+        if constexpr (sizeof(R) == 4) {
+            if (model != EP_TUSSCHER) { set_error("one warp per node is built for ten Tusscher lists"); return EP_ERR_ARG; }
+            int dev = 0, nsm = 148;
+            EP_CUDA(cudaGetDevice(&dev));
+            EP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            const int wgrid = std::min(div_up((long long)a.list_warp_max * 32, 128), 8 * nsm);
+            k_ionic_warp<R><<<wgrid, 128, 0, st>>>(a);
+            EP_CUDA(cudaGetLastError());
+        } else {
+            set_error("one warp per node is built for FP32 lists (the learned step's fallback)");
+            return EP_ERR_ARG;
+        }
     }
     if constexpr (sizeof(R) == 8) {
         dispatch_ionic<R, 1>(model, a, grid, block, st);       // FP64: the compiler's register choice

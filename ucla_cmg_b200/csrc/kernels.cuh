@@ -78,6 +78,9 @@ template <typename R> struct IonicArgs {
                                  // dV/dt, leave V unchanged (one sub-step)
     const int *node_list;        // non-null: run only these nodes (count on the device)
     const int *list_count;
+    int list_warp_max;           // > 0 (ten Tusscher lists): a list of at most this many
+                                 // nodes runs one warp per node (k_ionic_warp), a longer
+                                 // one one thread per node
     const uint8_t *skip;         // non-null: nodes with skip[i] != 0 are left alone (mixed
                                  // tissues: the Purkinje nodes in the tissue model's launch)
     // model options
@@ -139,6 +142,10 @@ template <typename R> struct CGArgs {
 // next units of SELL columns into shared memory), its deepest ring and the
 // depth it runs at when none is asked for
 constexpr int kStagedBatch = 32;
+// the learned step's fallback list runs one warp per node up to this many
+// nodes (its time is then one node's serial Newton chain), one thread per
+// node beyond (throughput)
+constexpr int kFallbackWarpMax = 4096;
 constexpr int kStageMaxDepth = 4;
 constexpr int kStageDepthDefault = 2;
 

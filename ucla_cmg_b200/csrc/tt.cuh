@@ -380,4 +380,111 @@ EP_HD R tt_compute_ion(R s[TT_NS], R V, R ist, R dt, const R *__restrict__ c,
     return dvdt;
 }
 
+#ifdef __CUDACC__
+// tt_compute_ion with one node per warp, for short node lists (a single
+// upstroke node's Newton is a long serial chain).  Every lane holds the node's
+// state and runs the gate step, the fixed terms, the LU solve and the update
+// (the same bits on every lane); the 12 perturbed rate evaluations of the
+// finite-difference Jacobian run one per lane (lane 2i: column i plus side,
+// lane 2i + 1: minus side; lanes 12..31 repeat lane 0's) and their residuals
+// are gathered by shuffles.  Each lane rebuilds the state the sequential loop
+// has when it reaches its evaluation -- x_i + eps and (x_i + eps) - 2 eps for
+// column i, and the earlier columns' entries after their round trip
+// ((x_j + eps) - 2 eps) + eps -- and the update continues from those
+// round-tripped entries, as the sequential loop does, so the result is
+// tt_compute_ion's to the bit.
+template <typename R>
+__device__ __forceinline__ R tt_compute_ion_warp(R s[TT_NS], R V, R ist, R dt, const R *__restrict__ c, R gks,
+                                                 const TTOpts &opt, int &iters, int lane) {
+    tt_gate_step(s, V, dt, c);
+    const TTFixed<R> f = tt_fixed<R>(V, s, c, ist, gks);
+    R x[6] = {s[0], s[1], s[2], s[9], s[16], s[17]};
+    R xn[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) xn[i] = x[i];
+    TTRev<R> e;
+    tt_rev_na(e, x[1], c, f);
+    tt_rev_k(e, x[0], c, f);
+    tt_rev_ks(e, x[0], x[1], c, f);
+    tt_rev_ca(e, x[2], c, f);
+    R old[6], dvdt;
+    tt_nr_rates(x, e, f, c, old, dvdt);
+
+    const int col = (lane >> 1) < 6 ? (lane >> 1) : 0;
+    const bool minus = (lane & 1) && (lane >> 1) < 6;
+    const R tol = R(opt.newton_tol);
+    R resid = R(100);
+    int it = 0;
+    while (resid > tol) {
+        if (it >= opt.newton_cap) break;
+        R eps[6], xd[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            eps[i] = R(1e-3) * x[i];
+            const R up = x[i] + eps[i];
+            xd[i] = (up - R(2) * eps[i]) + eps[i];
+        }
+        // this lane's evaluation: column col's entry perturbed, the columns
+        // before it round-tripped, the ones after it as they are
+        R xp[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const R up = x[k] + eps[k];
+            xp[k] = k < col ? xd[k] : k == col ? (minus ? up - R(2) * eps[k] : up) : x[k];
+        }
+        TTRev<R> ep = e;
+        if (col == 0) { tt_rev_k(ep, xp[0], c, f); tt_rev_ks(ep, xp[0], xp[1], c, f); }
+        if (col == 1) { tt_rev_na(ep, xp[1], c, f); tt_rev_ks(ep, xp[0], xp[1], c, f); }
+        if (col == 2) { tt_rev_ca(ep, xp[2], c, f); }
+        R rr[6], dd, F[6];
+        tt_nr_rates(xp, ep, f, c, rr, dd);
+#pragma unroll
+        for (int k = 0; k < 6; k++) F[k] = xp[k] - xn[k] - dt * rr[k];
+        R J[36];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            const R twoeps = R(2) * eps[i];
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                const R fp = __shfl_sync(0xffffffffu, F[k], 2 * i);
+                const R fm = __shfl_sync(0xffffffffu, F[k], 2 * i + 1);
+                const R v = (fp - fm) / twoeps;
+                if (opt.jac_true) J[i * 6 + k] = v;
+                else J[k * 6 + i] = v;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; i++) x[i] = xd[i];
+        R B[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) B[i] = x[i] - xn[i] - dt * old[i];
+        lu6_solve(J, B);
+#pragma unroll
+        for (int i = 0; i < 6; i++) x[i] -= B[i];
+        tt_rev_na(e, x[1], c, f);
+        tt_rev_k(e, x[0], c, f);
+        tt_rev_ks(e, x[0], x[1], c, f);
+        tt_rev_ca(e, x[2], c, f);
+        tt_nr_rates(x, e, f, c, old, dvdt);
+        R acc = R(0);
+        if (opt.fp32_scaled_tol) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                const R sc = fmax(fabs(x[i]), R(1));
+                const R q = B[i] / sc;
+                acc += q * q;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 6; i++) acc += B[i] * B[i];
+        }
+        resid = sqrt(acc);
+        it++;
+    }
+    s[0] = x[0]; s[1] = x[1]; s[2] = x[2]; s[9] = x[3]; s[16] = x[4]; s[17] = x[5];
+    iters = it;
+    return dvdt;
+}
+#endif
+
 }  // namespace ep
