@@ -55,6 +55,7 @@ struct ep_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t io_ev[8] = {};           // chunked host <-> device copies (created on first use)
     int n = 0, pitch = 0, model = 0, precision = 0, nstate = 0, ns = 0, ntypes = 1;
     size_t rsize = 8;                    // bytes per real
     double dt = 0.1, ionic_dt = 0.1, Cm = 1.0, Xi = 0.0;
@@ -752,6 +753,8 @@ void ep_destroy(ep_handle *h) {
     for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    for (cudaEvent_t e : h->io_ev)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->pin) cudaFreeHost(h->pin);
     delete h;
@@ -1079,13 +1082,41 @@ static void *stage(ep_handle *h, size_t bytes) {
     return h->pin;
 }
 
+// Host <-> device transfers of the per-node arrays in chunks, so that the
+// host-side conversion (FP64 node-major <-> the device's R / SoA layout) of
+// one chunk overlaps the copy engine's transfer of the next: the copies of a
+// chunk are issued as soon as it is converted (uploads), or all at once with
+// an event after each chunk and each chunk converted once its event has
+// completed (downloads).  Arrays under 64K nodes go in one piece.
+constexpr int kIoChunks = 8;
+
+static int io_chunks(ep_handle *h, int count) {
+    if (count < (1 << 16)) return 1;
+    for (cudaEvent_t &e : h->io_ev)
+        if (!e) EP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return kIoChunks;
+}
+// chunk k of K over [0, total), boundaries on multiples of 32 elements
+static void io_range(int total, int k, int K, int &b, int &e) {
+    const long long step = ((long long)total + K - 1) / K;
+    const long long st = (step + 31) / 32 * 32;
+    b = (int)std::min<long long>(total, st * k);
+    e = (int)std::min<long long>(total, st * (k + 1));
+}
+
 template <typename R>
 static int put_voltage(ep_handle *h, const double *V) {
     R *st = (R *)stage(h, sizeof(R) * h->n);
     if (!st) return EP_ERR_NOMEM;
+    const int K = h->n >= (1 << 16) ? kIoChunks : 1;
+    for (int k = 0; k < K; k++) {
+        int b, e;
+        io_range(h->n, k, K, b, e);
+        if (e <= b) continue;
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < h->n; i++) st[i] = (R)V[i];
-    EP_CUDA(cudaMemcpyAsync(h->V.p, st, sizeof(R) * h->n, cudaMemcpyHostToDevice, h->stream));
+        for (int i = b; i < e; i++) st[i] = (R)V[i];
+        EP_CUDA(cudaMemcpyAsync(h->V.as<R>() + b, st + b, sizeof(R) * (e - b), cudaMemcpyHostToDevice, h->stream));
+    }
     int rc = reset_predictor(h);
     if (rc) return rc;
     EP_CUDA(cudaStreamSynchronize(h->stream));
@@ -1096,15 +1127,35 @@ template <typename R>
 static int get_voltage(ep_handle *h, double *V) {
     R *st = (R *)stage(h, sizeof(R) * h->n);
     if (!st) return EP_ERR_NOMEM;
-    EP_CUDA(cudaMemcpyAsync(st, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
-    EP_CUDA(cudaStreamSynchronize(h->stream));
+    const int K = io_chunks(h, h->n);
+    if (K < 0) return K;
+    if (K == 1) {
+        EP_CUDA(cudaMemcpyAsync(st, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
+        EP_CUDA(cudaStreamSynchronize(h->stream));
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < h->n; i++) V[i] = (double)st[i];
+        for (int i = 0; i < h->n; i++) V[i] = (double)st[i];
+        return EP_OK;
+    }
+    for (int k = 0; k < K; k++) {
+        int b, e;
+        io_range(h->n, k, K, b, e);
+        if (e > b)
+            EP_CUDA(cudaMemcpyAsync(st + b, h->V.as<R>() + b, sizeof(R) * (e - b), cudaMemcpyDeviceToHost, h->stream));
+        EP_CUDA(cudaEventRecord(h->io_ev[k], h->stream));
+    }
+    for (int k = 0; k < K; k++) {
+        int b, e;
+        io_range(h->n, k, K, b, e);
+        EP_CUDA(cudaEventSynchronize(h->io_ev[k]));
+#pragma omp parallel for schedule(static)
+        for (int i = b; i < e; i++) V[i] = (double)st[i];
+    }
     return EP_OK;
 }
 
 // stored states <-> node-major rows (State[0] = V except LR, which keeps V
-// in slot 7)
+// in slot 7); the staging buffer has the device's SoA layout, so a chunk of
+// nodes is one 2-D copy per population
 template <typename R>
 static int put_states(ep_handle *h, const double *in) {
     const size_t tot = (size_t)h->ns * h->pitch;
@@ -1115,20 +1166,30 @@ static int put_states(ep_handle *h, const double *in) {
     R *sp = st + tot;
     const int off = is_lr(h->model) ? 0 : 1;
     const int w = h->nstate_api;
+    const size_t rp = sizeof(R) * (size_t)h->pitch;
+    const int K = h->pitch >= (1 << 16) ? kIoChunks : 1;
+    for (int c = 0; c < K; c++) {
+        int b, e;
+        io_range(h->pitch, c, K, b, e);
+        if (e <= b) continue;
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < h->pitch; i++) {
-        const bool pk = h->mixed && i < h->n && h->is_purk[i];
-        if (i < h->n && !pk) {
-            const double *s = in + (size_t)i * w;
-            for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = (R)s[k + off];
-        } else {
-            for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = R(0);
+        for (int i = b; i < e; i++) {
+            const bool pk = h->mixed && i < h->n && h->is_purk[i];
+            if (i < h->n && !pk) {
+                const double *s = in + (size_t)i * w;
+                for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = (R)s[k + off];
+            } else {
+                for (int k = 0; k < h->ns; k++) st[(size_t)k * h->pitch + i] = R(0);
+            }
+            // a Purkinje node's row: V, then its stored states (Purkinje.h)
+            for (int k = 0; k < pns1; k++) sp[(size_t)k * h->pitch + i] = pk ? (R)in[(size_t)i * w + 1 + k] : R(0);
         }
-        // a Purkinje node's row: V, then its stored states (Purkinje.h)
-        for (int k = 0; k < pns1; k++) sp[(size_t)k * h->pitch + i] = pk ? (R)in[(size_t)i * w + 1 + k] : R(0);
+        const size_t wb = sizeof(R) * (size_t)(e - b);
+        if (h->ns)
+            EP_CUDA(cudaMemcpy2DAsync(h->S.as<R>() + b, rp, st + b, rp, wb, h->ns, cudaMemcpyHostToDevice, h->stream));
+        if (ptot)
+            EP_CUDA(cudaMemcpy2DAsync(h->Spk.as<R>() + b, rp, sp + b, rp, wb, pns1, cudaMemcpyHostToDevice, h->stream));
     }
-    EP_CUDA(cudaMemcpyAsync(h->S.p, st, sizeof(R) * tot, cudaMemcpyHostToDevice, h->stream));
-    if (ptot) EP_CUDA(cudaMemcpyAsync(h->Spk.p, sp, sizeof(R) * ptot, cudaMemcpyHostToDevice, h->stream));
     EP_CUDA(cudaStreamSynchronize(h->stream));
     return EP_OK;
 }
@@ -1142,27 +1203,45 @@ static int get_states(ep_handle *h, double *out) {
     if (!st) return EP_ERR_NOMEM;
     R *sv = st + tot;
     R *sp = sv + h->pitch;
-    EP_CUDA(cudaMemcpyAsync(st, h->S.p, sizeof(R) * tot, cudaMemcpyDeviceToHost, h->stream));
-    EP_CUDA(cudaMemcpyAsync(sv, h->V.p, sizeof(R) * h->n, cudaMemcpyDeviceToHost, h->stream));
-    if (ptot) EP_CUDA(cudaMemcpyAsync(sp, h->Spk.p, sizeof(R) * ptot, cudaMemcpyDeviceToHost, h->stream));
-    EP_CUDA(cudaStreamSynchronize(h->stream));
+    const size_t rp = sizeof(R) * (size_t)h->pitch;
+    const int K = io_chunks(h, h->n);
+    if (K < 0) return K;
+    for (int c = 0; c < K; c++) {
+        int b, e;
+        io_range(h->n, c, K, b, e);
+        if (e > b) {
+            const size_t wb = sizeof(R) * (size_t)(e - b);
+            if (h->ns)
+                EP_CUDA(cudaMemcpy2DAsync(st + b, rp, h->S.as<R>() + b, rp, wb, h->ns, cudaMemcpyDeviceToHost, h->stream));
+            EP_CUDA(cudaMemcpyAsync(sv + b, h->V.as<R>() + b, wb, cudaMemcpyDeviceToHost, h->stream));
+            if (ptot)
+                EP_CUDA(cudaMemcpy2DAsync(sp + b, rp, h->Spk.as<R>() + b, rp, wb, pns1, cudaMemcpyDeviceToHost, h->stream));
+        }
+        if (K > 1) EP_CUDA(cudaEventRecord(h->io_ev[c], h->stream));
+    }
+    if (K == 1) EP_CUDA(cudaStreamSynchronize(h->stream));
     const bool lr = is_lr(h->model);
     const int w = h->nstate_api;
+    for (int c = 0; c < K; c++) {
+        int b, e;
+        io_range(h->n, c, K, b, e);
+        if (K > 1) EP_CUDA(cudaEventSynchronize(h->io_ev[c]));
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < h->n; i++) {
-        double *o = out + (size_t)i * w;
-        for (int k = h->nstate; k < w; k++) o[k] = 0.0;
-        if (h->mixed && h->is_purk[i]) {
-            // the Purkinje cell's row (its nVar is ep_model_nstate(EP_PURKINJE))
-            o[0] = (double)sv[i];
-            for (int k = 0; k < pns1; k++) o[k + 1] = (double)sp[(size_t)k * h->pitch + i];
-            for (int k = pns1 + 1; k < w; k++) o[k] = 0.0;
-        } else if (lr) {
-            for (int k = 0; k < 7; k++) o[k] = (double)st[(size_t)k * h->pitch + i];
-            o[7] = (double)sv[i];
-        } else {
-            o[0] = (double)sv[i];
-            for (int k = 0; k < h->ns; k++) o[k + 1] = (double)st[(size_t)k * h->pitch + i];
+        for (int i = b; i < e; i++) {
+            double *o = out + (size_t)i * w;
+            for (int k = h->nstate; k < w; k++) o[k] = 0.0;
+            if (h->mixed && h->is_purk[i]) {
+                // the Purkinje cell's row (its nVar is ep_model_nstate(EP_PURKINJE))
+                o[0] = (double)sv[i];
+                for (int k = 0; k < pns1; k++) o[k + 1] = (double)sp[(size_t)k * h->pitch + i];
+                for (int k = pns1 + 1; k < w; k++) o[k] = 0.0;
+            } else if (lr) {
+                for (int k = 0; k < 7; k++) o[k] = (double)st[(size_t)k * h->pitch + i];
+                o[7] = (double)sv[i];
+            } else {
+                o[0] = (double)sv[i];
+                for (int k = 0; k < h->ns; k++) o[k + 1] = (double)st[(size_t)k * h->pitch + i];
+            }
         }
     }
     return EP_OK;
