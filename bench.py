@@ -200,23 +200,31 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic(kernel, form, cg_iters, cg_predict=0):
+def _traffic(kernel, form, cg_iters, cg_predict=0, cg_batch=8):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/traffic.json); the CG launch's bytes grow with its
     iteration count, so they are stored as prologue + per iteration, plus the
-    predictor's own passes when one is on (None if that was not captured)."""
+    predictor's own passes when one is on (None if that was not captured).
+    The staged CG kernel (cg_batch 32) has its own entry: its evict-first
+    matrix stream leaves the vectors in L2."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
     except Exception:
         return None
-    if kernel == "cg" and "cg" in t:
+    key = "cg_staged" if cg_batch == 32 else "cg"
+    if kernel == "cg" and key in t:
+        c = t[key]
+        if "predict2_bytes" in c:               # measured with predictor 2 only
+            if cg_predict != 2:
+                return None
+            return c["predict2_bytes"]["prologue_bytes"] + cg_iters * c["predict2_bytes"]["per_iteration_bytes"]
         extra = 0
         if cg_predict:
-            extra = t["cg"].get("predict_extra_bytes", {}).get(str(cg_predict))
+            extra = c.get("predict_extra_bytes", {}).get(str(cg_predict))
             if extra is None:
                 return None
-        return t["cg"]["prologue_bytes"] + extra + cg_iters * t["cg"]["per_iteration_bytes"]
+        return c["prologue_bytes"] + extra + cg_iters * c["per_iteration_bytes"]
     if kernel == "ionic":
         return t.get("surrogate" if form == "surrogate" else "ionic_plain_fp32" if form == "plain_fp32" else "-")
     return None
@@ -502,7 +510,8 @@ def run_ours(args, rank, world, local):
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind,
-            "traffic": _traffic(dom, args.form, cg_per_solve, shape["cg_predict"]) if wl.name == "shell_c2" else None,
+            "traffic": _traffic(dom, args.form, cg_per_solve, shape["cg_predict"], shape["cg_batch"])
+            if wl.name == "shell_c2" else None,
             "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "kernel_ms": kms}
     b_ns = node_step_bytes(n, nnz, cg_per_solve, rb, nstate=nstate, ne=len(wl.electrodes), ecg_every=ecg_every,
                            cg_predict=shape["cg_predict"])

@@ -130,32 +130,43 @@ __device__ __forceinline__ R slice_tail(const int *__restrict__ col, const R *__
     return acc;
 }
 
+// G columns k .. k+G-1 of a slice as one group: their column and value loads,
+// then their gathers, then the products added in column order
+template <int G, typename R, typename F>
+__device__ __forceinline__ R slice_group(const int *__restrict__ col, const R *__restrict__ val, int beg, int k,
+                                         int lane, F gather, R acc) {
+    int c[G];
+    R v[G], g[G];
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+        const int idx = beg + (k + u) * kSlice + lane;
+        c[u] = __ldg(col + idx);
+        v[u] = __ldg(val + idx);
+    }
+#pragma unroll
+    for (int u = 0; u < G; u++) g[u] = gather(c[u]);
+#pragma unroll
+    for (int u = 0; u < G; u++) acc += v[u] * g[u];
+    return acc;
+}
+
 // Row sums of one SELL slice, NB slice columns at a time: the column and
 // value loads of a group are issued together, then the gathers, so each lane
 // has 3 NB independent loads in flight (at one lane per row the kernel is
 // bound by memory latency, not bandwidth); the w mod NB columns left over
-// form one more, partial group.  The products are still added in column
-// order, so the sums are those of the plain loop whatever NB is.
+// form one more, partial group -- except a single one, which joins the last
+// full group (a 17-wide slice gathers in 2 rounds of 8 + 9, not 3 of
+// 8 + 8 + 1: on the shell's meshes this is what evens out the warps' loads).
+// The products are still added in column order, so the sums are those of
+// the plain loop whatever the grouping.
 template <int NB, typename R, typename F>
 __device__ __forceinline__ R slice_row_sum(const int *__restrict__ col, const R *__restrict__ val, int beg, int w,
                                            int lane, F gather) {
     R acc = R(0);
     int k = 0;
-    for (; k + NB <= w; k += NB) {
-        int c[NB];
-        R v[NB], g[NB];
-#pragma unroll
-        for (int u = 0; u < NB; u++) {
-            const int idx = beg + (k + u) * kSlice + lane;
-            c[u] = __ldg(col + idx);
-            v[u] = __ldg(val + idx);
-        }
-#pragma unroll
-        for (int u = 0; u < NB; u++) g[u] = gather(c[u]);
-#pragma unroll
-        for (int u = 0; u < NB; u++) acc += v[u] * g[u];
-    }
-    if (k < w) acc = slice_tail<NB>(col, val, beg, k, w, lane, gather, acc);
+    for (; k + NB <= w && w - k != NB + 1; k += NB) acc = slice_group<NB>(col, val, beg, k, lane, gather, acc);
+    if (w - k == NB + 1) acc = slice_group<NB + 1>(col, val, beg, k, lane, gather, acc);
+    else if (k < w) acc = slice_tail<NB>(col, val, beg, k, w, lane, gather, acc);
     return acc;
 }
 
