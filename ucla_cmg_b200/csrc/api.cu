@@ -74,7 +74,7 @@ struct ep_handle {
     long long step = 0;
     int nslices = 0;
     // device memory
-    DBuf V, S, Aval, Bval, dinv, r, q, p0, p1, zv, consts, gks, lr_table, type, slice_ptr, col;
+    DBuf V, S, Aval, Bval, dinv, r, q, p0, zv, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
     DBuf pd0, pd1, pvin;                 // CG predictor: x - V of the first / second half step, scratch
     DBuf pq0, pq1;                       // linear CG predictor: the corrections one step older
@@ -222,8 +222,8 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.n = h->n; a.nslices = h->nslices;
     a.slice_ptr = h->slice_ptr.as<int>(); a.col = h->col.as<int>();
     a.Aval = h->Aval.as<R>(); a.Bval = h->Bval.as<R>(); a.dinv = h->dinv.as<R>();
-    a.x = h->V.as<R>(); a.r = h->r.as<R>(); a.q = h->q.as<R>(); a.z = h->zv.as<R>();
-    a.p0 = h->p0.as<R>(); a.p1 = h->p1.as<R>();
+    a.x = h->V.as<R>(); a.r = h->r.as<R>(); a.q = h->q.as<R>(); a.zp = h->zv.as<R>();
+    a.p0 = h->p0.as<R>();
     a.partial = h->partial.as<double>();
     a.bar = h->bar.as<GridBarrier>();
     a.tol = h->cg_tol; a.maxit = h->cg_maxit;
@@ -273,11 +273,10 @@ int create_typed(ep_handle *h, const HostCSR &csr, const std::vector<double> &st
     }
     if ((rc = upload<R>(h->dinv, dinv))) return rc;
     const size_t vb = (size_t)h->pitch * sizeof(R);
-    if ((rc = h->r.alloc(vb)) || (rc = h->q.alloc(vb)) || (rc = h->p0.alloc(vb)) || (rc = h->p1.alloc(vb)) ||
-        (rc = h->zv.alloc(vb)))
+    if ((rc = h->r.alloc(vb)) || (rc = h->q.alloc(vb)) || (rc = h->p0.alloc(vb)) || (rc = h->zv.alloc(2 * vb)))
         return rc;
-    EP_CUDA(cudaMemset(h->r.p, 0, vb)); EP_CUDA(cudaMemset(h->q.p, 0, vb)); EP_CUDA(cudaMemset(h->zv.p, 0, vb));
-    EP_CUDA(cudaMemset(h->p0.p, 0, vb)); EP_CUDA(cudaMemset(h->p1.p, 0, vb));
+    EP_CUDA(cudaMemset(h->r.p, 0, vb)); EP_CUDA(cudaMemset(h->q.p, 0, vb)); EP_CUDA(cudaMemset(h->zv.p, 0, 2 * vb));
+    EP_CUDA(cudaMemset(h->p0.p, 0, vb));
     // cell states (SoA) and voltage
     std::vector<double> V(h->pitch, 0.0), S((size_t)h->ns * h->pitch, 0.0);
     const int off = is_lr(h->model) ? 0 : 1;       // LR keeps V in slot 7

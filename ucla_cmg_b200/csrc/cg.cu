@@ -15,7 +15,9 @@
 //            dinv r), q = A p', partial p'.q          -> barrier
 //   phase B  x += alpha p', r -= alpha q, partial r.z, r.r -> barrier
 // The same thread owns a row in every phase, so x, r, q need no cross-block
-// visibility; z and p are read across blocks.  Phase A gathers them with
+// visibility; z and p are read across blocks, interleaved as (z_i, p_i) pairs
+// so that one load brings a neighbour's both (phase B writes the pair: the
+// new z and the p' it used).  Phase A gathers them with
 // plain (L1-allocating) loads: neither changes during the phase, and the grid
 // barrier before it (a gpu-scope fence after the arrival wait, then the CTA
 // barrier, as a cooperative grid sync) orders every block's writes of the
@@ -40,6 +42,13 @@ __device__ __forceinline__ R pdir(R dinv, R r, R beta, R p) { return fma(beta, p
 // the same with z = dinv r already rounded and stored
 template <typename R>
 __device__ __forceinline__ R pdir_z(R z, R beta, R p) { return fma(beta, p, z); }
+
+// the gathered pair (z_i, p_i) of the two-reduction kernels, interleaved so a
+// neighbour's two values come in one load (zp[2i] = z_i, zp[2i+1] = p_i)
+template <typename R> struct ZP;
+template <> struct ZP<float> { using T = float2; };
+template <> struct ZP<double> { using T = double2; };
+template <typename R> using zp_t = typename ZP<R>::T;
 
 template <int NV>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double *out, int stride) {
@@ -294,8 +303,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                 const R r = pred ? rref - ad : rref;
                 const R z = __ldg(a.dinv + row) * r;
                 a.r[row] = r;
-                a.z[row] = z;
-                a.p0[row] = R(0);
+                reinterpret_cast<zp_t<R> *>(a.zp)[row] = zp_t<R>{z, R(0)};
                 if (pred) a.vin[row] = a.x[row];
                 v[0] += (double)r * (double)z;
                 v[1] += (double)r * (double)r;
@@ -321,7 +329,8 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
     int it = 0;
     bool converged = (rr_start <= stop2);
     double rr_last = rr_start;
-    R *pc = a.p0, *pn = a.p1;
+    zp_t<R> *zp = reinterpret_cast<zp_t<R> *>(a.zp);
+    R *pn = a.p0;                             // p' of the own rows, phase A -> phase B
     while (!converged && it < a.maxit) {
         // ---- phase A: p' = z + beta p; q = A p' ----
         {
@@ -332,13 +341,13 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                     prefetch_slice<R>(a.slice_ptr, a.col, a.Aval, nullptr, s + a.prefetch * nwarps, s_hi, lane);
                 const int row = s * kSlice + lane;
                 const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
-                const R *pcc = pc;
-                auto gat = [&](int c) { return pdir_z(a.z[c], bR, pcc[c]); };
+                auto gat = [&](int c) { const zp_t<R> t = zp[c]; return pdir_z(t.x, bR, t.y); };
                 R q;
                 if constexpr (NB == 16) q = slice_row_sum_pipe<8>(a.col, a.Aval, beg, w, lane, gat);
                 else q = slice_row_sum<NB>(a.col, a.Aval, beg, w, lane, gat);
                 if (row >= rb && row < re) {
-                    const R pi = pdir_z(a.z[row], bR, ldcg(pc + row));
+                    const zp_t<R> t = zp[row];
+                    const R pi = pdir_z(t.x, bR, t.y);
                     pn[row] = pi;
                     a.q[row] = q;
                     v[0] += (double)pi * (double)q;
@@ -374,7 +383,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                     const R r = ri - aR * qi;
                     a.r[row] = r;
                     const R z = di * r;
-                    a.z[row] = z;
+                    zp[row] = zp_t<R>{z, pi};
                     v[0] += (double)r * (double)z;
                     v[1] += (double)r * (double)r;
                 }
@@ -383,7 +392,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
                     const R r = ri2 - aR * qi2;
                     a.r[row2] = r;
                     const R z = di2 * r;
-                    a.z[row2] = z;
+                    zp[row2] = zp_t<R>{z, pi2};
                     v[0] += (double)r * (double)z;
                     v[1] += (double)r * (double)r;
                 }
@@ -402,7 +411,6 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
         if (!isfinite(t[1])) break;
         beta = t[0] / rz;
         rz = t[0];
-        R *tmp = pc; pc = pn; pn = tmp;
     }
     if (pred) {
         // the solution x + delta, and the correction this solve made, for the
@@ -761,8 +769,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
                 const R r = pred ? rref - ad : rref;
                 const R z = __ldg(a.dinv + row) * r;
                 a.r[row] = r;
-                a.z[row] = z;
-                a.p0[row] = R(0);
+                reinterpret_cast<zp_t<R> *>(a.zp)[row] = zp_t<R>{z, R(0)};
                 if (pred) a.vin[row] = a.x[row];
                 v[0] += (double)r * (double)z;
                 v[1] += (double)r * (double)r;
@@ -785,13 +792,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
     int it = 0;
     bool converged = (rr_start <= stop2);
     double rr_last = rr_start;
-    R *pc = a.p0, *pn = a.p1;
+    zp_t<R> *zp = reinterpret_cast<zp_t<R> *>(a.zp);
+    R *pn = a.p0;                             // p' of the own rows, phase A -> phase B
     while (!converged && it < a.maxit) {
         // ---- phase A: q = A p', p' = z + beta p, the units from the ring ----
         {
             double v[1] = {0.0};
             const R bR = (R)beta;
-            const R *pcc = pc;
             for (int s = gwarp; s < s_hi; s += nwarps) {
                 const int row = s * kSlice + lane;
                 const int beg = __ldg(a.slice_ptr + s), w = (__ldg(a.slice_ptr + s + 1) - beg) / kSlice;
@@ -812,13 +819,17 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
                         if (u < nc) c[u] = ci[u * kSlice];
 #pragma unroll
                     for (int u = 0; u < kUnitCols; u++)
-                        if (u < nc) g[u] = pdir_z(a.z[c[u]], bR, pcc[c[u]]);
+                        if (u < nc) {
+                            const zp_t<R> t = zp[c[u]];
+                            g[u] = pdir_z(t.x, bR, t.y);
+                        }
 #pragma unroll
                     for (int u = 0; u < kUnitCols; u++)
                         if (u < nc) qv += cv[u * kSlice] * g[u];
                 }
                 if (row >= rb && row < re) {
-                    const R pi = pdir_z(a.z[row], bR, ldcg(pc + row));
+                    const zp_t<R> t = zp[row];
+                    const R pi = pdir_z(t.x, bR, t.y);
                     pn[row] = pi;
                     a.q[row] = qv;
                     v[0] += (double)pi * (double)qv;
@@ -851,7 +862,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
                     const R r = ri - aR * qi;
                     a.r[row] = r;
                     const R z = di * r;
-                    a.z[row] = z;
+                    zp[row] = zp_t<R>{z, pi};
                     v[0] += (double)r * (double)z;
                     v[1] += (double)r * (double)r;
                 }
@@ -860,7 +871,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
                     const R r = ri2 - aR * qi2;
                     a.r[row2] = r;
                     const R z = di2 * r;
-                    a.z[row2] = z;
+                    zp[row2] = zp_t<R>{z, pi2};
                     v[0] += (double)r * (double)z;
                     v[1] += (double)r * (double)r;
                 }
@@ -876,7 +887,6 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
         if (!isfinite(t[1])) break;
         beta = t[0] / rz;
         rz = t[0];
-        R *tmp = pc; pc = pn; pn = tmp;
     }
     cp_wait_all();                            // the units that ran ahead into the next sweep
     if (pred) {

@@ -104,8 +104,9 @@ template <typename R> struct CGArgs {
     const int *slice_ptr;        // nslices + 1
     const int *col;
     const R *Aval, *Bval, *dinv;
-    R *x, *r, *q, *p0, *p1;
-    R *z;                        // two-reduction variant: z = dinv r of the own rows, gathered by the neighbours
+    R *x, *r, *q, *p0;           // p0: the direction p (two-reduction: p' of the own rows)
+    R *zp;                       // two-reduction variant: 2 * pitch, (z_i, p_i) pairs with
+                                 // z = dinv r, gathered by the neighbours (16-byte aligned)
     double *partial;             // 12 * grid: consecutive phases use disjoint slots
     GridBarrier *bar;
     double tol;

@@ -33,7 +33,7 @@ namespace ep {
 constexpr int kNoAllocMaxRows = 262144;                 // 2^18 rows
 constexpr int kNoAllocMaxGrid = 2048;                   // >= 148 SMs x 8 blocks
 constexpr size_t kVecBytes = sizeof(double) * (size_t)kNoAllocMaxRows;   // one vector, FP64
-constexpr size_t kScratchBytes = 5 * kVecBytes                            // r, q, p0, p1, z
+constexpr size_t kScratchBytes = 5 * kVecBytes                            // r, q, p0, (z, p) pairs (2)
                                + sizeof(double) * 12 * kNoAllocMaxGrid    // reduction partials (12 slots)
                                + 256;                                     // barrier, stats, result
 
@@ -69,8 +69,7 @@ int run(unsigned char *base, int n, int nslices, const int *slice_ptr, const int
     a.r = (R *)(base + 0 * kVecBytes);
     a.q = (R *)(base + 1 * kVecBytes);
     a.p0 = (R *)(base + 2 * kVecBytes);
-    a.p1 = (R *)(base + 3 * kVecBytes);
-    a.z = (R *)(base + 4 * kVecBytes);
+    a.zp = (R *)(base + 3 * kVecBytes);                            // two vectors: (z, p) pairs
     a.partial = (double *)(base + 5 * kVecBytes);
     unsigned char *tail = base + 5 * kVecBytes + sizeof(double) * 12 * kNoAllocMaxGrid;
     a.bar = (GridBarrier *)tail;                                   // 16 B
