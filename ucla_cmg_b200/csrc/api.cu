@@ -56,6 +56,10 @@ struct ep_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t io_ev[8] = {};           // chunked host <-> device copies (created on first use)
+    // learned step: the fallback list runs on a second, higher-priority
+    // stream beside the physics of the nodes the network took
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int n = 0, pitch = 0, model = 0, precision = 0, nstate = 0, ns = 0, ntypes = 1;
     size_t rsize = 8;                    // bytes per real
     double dt = 0.1, ionic_dt = 0.1, Cm = 1.0, Xi = 0.0;
@@ -533,12 +537,21 @@ static int launch_learned_phase(ep_handle *h, const IonicArgs<float> &ia) {
     fill_surrogate_args(h, ia, sa);
     int rc = launch_surrogate(sa, h->stream, h->sg_variant);
     if (rc) return rc;
-    if (h->sg_vupdate == 2 && (rc = launch_hybrid(sa, h->stream))) return rc;
+    // the fallback list (the nodes the network did not take) on the side
+    // stream, submitted first and at higher priority, beside the physics of
+    // the taken nodes: disjoint nodes; a short list's time is one node's
+    // Newton chain, which then hides under k_hybrid
     IonicArgs<float> fb = ia;
     fb.node_list = h->sg_list.as<int>();
     fb.list_count = h->sg_count.as<int>();
     fb.list_warp_max = kFallbackWarpMax;    // a short list: one warp per node
-    return launch_ionic<float>(EP_TUSSCHER, fb, h->stream, h->ionic_block, h->ionic_min);
+    EP_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+    EP_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    if ((rc = launch_ionic<float>(EP_TUSSCHER, fb, h->side, h->ionic_block, h->ionic_min))) return rc;
+    EP_CUDA(cudaEventRecord(h->ev_join, h->side));
+    if (h->sg_vupdate == 2 && (rc = launch_hybrid(sa, h->stream))) return rc;
+    EP_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    return EP_OK;
 }
 
 enum { K_CG = 0, K_IONIC = 1, K_ECG = 2, K_OTHER = 3 };
@@ -754,6 +767,10 @@ void ep_destroy(ep_handle *h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     for (cudaEvent_t e : h->io_ev)
         if (e) cudaEventDestroy(e);
+    if (h->side) cudaStreamSynchronize(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->pin) cudaFreeHost(h->pin);
     delete h;
@@ -1566,6 +1583,13 @@ int ep_set_surrogate(ep_handle *h, const ep_surrogate_desc *d) {
     if (aux.v_update == 2 && !h->sg_pred.p) {
         if ((rc = h->sg_pred.alloc(sizeof(float) * 6 * (size_t)h->pitch))) return rc;
         if ((rc = h->sg_take.alloc((size_t)h->pitch))) return rc;
+    }
+    if (!h->side) {
+        int lo = 0, hi = 0;
+        EP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        EP_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi));
+        EP_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        EP_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     }
     EP_CUDA(cudaMemset(h->sg_err.p, 0, sizeof(unsigned int)));
     h->has_surrogate = 1;
