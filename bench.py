@@ -237,8 +237,9 @@ def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=
       prologue  nnz*(A + B + col) + n*(x + dinv read + r, z, p write)
       iteration nnz*(A + col) + n*(z, p_old read + p_new, q write)         [phase A]
                 + n*(p_new, x, r, q, dinv read + x, r, z write)             [phase B]
-      predictor (cg_predict k = 1, 2): n*(k corrections read + V saved) in the
-                prologue, n*(x, V, k corrections read + x, k corrections
+      predictor (cg_predict k = 1, 2): n*(the start correction read + V saved)
+                in the prologue (k = 2: the extrapolation the previous solve
+                stored), n*(x, V, k corrections read + x, k corrections
                 written) after the iterations
     ionic: the V + stored states read and written once, the activation
       record read (16 B), node type (1 B), G_Ks scale and stimulus head (4 B each).
@@ -247,7 +248,7 @@ def algorithmic_bytes(kernel, n, nnz, cg_iters_per_solve, rbytes, nstate=19, ne=
     if kernel == "cg":
         pro = nnz * (2 * rbytes + 4) + n * 5 * rbytes
         if cg_predict:
-            pro += n * rbytes * ((cg_predict + 1) + (2 + cg_predict + 1 + cg_predict))
+            pro += n * rbytes * (2 + (2 + cg_predict + 1 + cg_predict))
         it = nnz * (rbytes + 4) + n * 4 * rbytes + n * 8 * rbytes
         return pro + cg_iters_per_solve * it
     if kernel == "ionic":

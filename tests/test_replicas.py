@@ -58,6 +58,7 @@ def test_node_step_bytes_is_the_sum_of_the_phases():
     z = nnz / n
     for k, pred in ((4.0, 0), (8.5, 1), (8.5, 2)):
         b = bench.node_step_bytes(n, nnz, k, 4, nstate=19, ne=10, ecg_every=10, cg_predict=pred)
-        extra = 0 if not pred else (3 * pred + 4) * 4      # k gathers + V saved; x, V, k read, x + k written
+        # the start correction gathered + V saved; x, V, k corrections read, x + k written
+        extra = 0 if not pred else (2 + 2 * pred + 3) * 4
         cg = z * 12 + 5 * 4 + extra + k * (z * 8 + 12 * 4)
         assert abs(b - ((2 * 19 * 4 + 16 + 1 + 4 + 4) + 2 * cg + 11 * 4 / 10)) < 1e-9

@@ -81,7 +81,7 @@ struct ep_handle {
     DBuf V, S, Aval, Bval, dinv, r, q, p0, zv, consts, gks, lr_table, type, slice_ptr, col;
     DBuf r1, w0, w1, s0, s1;             // single-reduction CG only (allocated on first use)
     DBuf pd0, pd1, pvin;                 // CG predictor: x - V of the first / second half step, scratch
-    DBuf pq0, pq1;                       // linear CG predictor: the corrections one step older
+    DBuf pq0, pq1;                       // linear CG predictor: each half step's next start, 2 delta - delta_prev
     DBuf partial, bar, status, cg_stats, cg_last, d_step, track;
     DBuf stim_head, stim_next, stim_on, stim_off, stim_amp;
     int nstim = 0;
@@ -242,7 +242,7 @@ void fill_cg_args(ep_handle *h, CGArgs<R> &a) {
     a.inst_blk = h->d_inst_blk.as<int>();
     a.r1 = h->r1.as<R>(); a.w0 = h->w0.as<R>(); a.w1 = h->w1.as<R>();
     a.s0 = h->s0.as<R>(); a.s1 = h->s1.as<R>();
-    a.delta = nullptr; a.delta_prev = nullptr; a.vin = nullptr;   // the time step sets the predictor
+    a.delta = nullptr; a.dext = nullptr; a.vin = nullptr;   // the time step sets the predictor
     a.prefetch = h->cg_batch == kStagedBatch ? 0 : h->cg_prefetch;   // the staged kernel's is its ring depth
     a.bar_extra = h->bar_extra;
     a.depth = stage_depth(h);
@@ -622,7 +622,7 @@ static int step_typed(ep_handle *h, int nsteps, size_t &ne) {
     if (h->cg_predict) {
         ca.delta = h->pd0.as<R>(); ca2.delta = h->pd1.as<R>();
         ca.vin = ca2.vin = h->pvin.as<R>();
-        if (h->cg_predict == 2) { ca.delta_prev = h->pq0.as<R>(); ca2.delta_prev = h->pq1.as<R>(); }
+        if (h->cg_predict == 2) { ca.dext = h->pq0.as<R>(); ca2.dext = h->pq1.as<R>(); }
     }
     int rc;
     for (int s = 0; s < nsteps; s++) {

@@ -281,13 +281,13 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
 
     // ---- prologue: r = B x - A x, z = dinv r, p = 0 ----
     // With a predictor (delta: the previous solve's correction x - V of
-    // this half step; with delta_prev the one before it too, extrapolated
-    // linearly to 2 delta - delta_prev) the iteration starts from x + pred
+    // this half step; with dext its linear extrapolation 2 delta - delta_prev,
+    // stored by the previous solve) the iteration starts from x + pred
     // instead, r = B x - A (x + pred), while the stop test keeps the
     // reference's r0 = B x - A x; x itself is not touched before the barrier
     // (neighbours read it here).
     const bool pred = a.delta != nullptr;
-    const bool lin = a.delta_prev != nullptr;
+    const bool lin = a.dext != nullptr;
     {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = gwarp; s < s_hi; s += nwarps) {
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
             R ax = R(0), bx = R(0), ad = R(0);
             slice_ab_sums<NB == 4 ? 2 : 4>(a.col, a.Aval, a.Bval, a.x, beg, w, lane, pred, [&](int c) {
-                return lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c];
+                return lin ? a.dext[c] : a.delta[c];
             }, ax, bx, ad);
             if (row >= rb && row < re) {
                 const R rref = bx - ax;
@@ -420,10 +420,11 @@ __global__ void __launch_bounds__(NB == 4 ? 768 : 256, NB == 4 ? 2 : 4) k_cn_hal
             const int row = s * kSlice + lane;
             if (row >= rb && row < re) {
                 const R d = a.delta[row];
-                const R xf = a.x[row] + (lin ? R(2) * d - a.delta_prev[row] : d);
+                const R xf = a.x[row] + (lin ? a.dext[row] : d);
                 a.x[row] = xf;
-                if (lin) a.delta_prev[row] = d;
-                a.delta[row] = xf - a.vin[row];
+                const R dn = xf - a.vin[row];
+                a.delta[row] = dn;
+                if (lin) a.dext[row] = R(2) * dn - d;     // the next solve's start: 2 delta - delta_prev
             }
         }
     }
@@ -754,7 +755,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
 
     // ---- prologue: as k_cn_half ----
     const bool pred = a.delta != nullptr;
-    const bool lin = a.delta_prev != nullptr;
+    const bool lin = a.dext != nullptr;
     {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int s = gwarp; s < s_hi; s += nwarps) {
@@ -762,7 +763,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
             const int beg = a.slice_ptr[s], w = (a.slice_ptr[s + 1] - beg) / kSlice;
             R ax = R(0), bx = R(0), ad = R(0);
             slice_ab_sums<4>(a.col, a.Aval, a.Bval, a.x, beg, w, lane, pred, [&](int c) {
-                return lin ? R(2) * a.delta[c] - a.delta_prev[c] : a.delta[c];
+                return lin ? a.dext[c] : a.delta[c];
             }, ax, bx, ad);
             if (row >= rb && row < re) {
                 const R rref = bx - ax;
@@ -894,10 +895,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4) k_cn_half_staged(
             const int row = s * kSlice + lane;
             if (row >= rb && row < re) {
                 const R d = a.delta[row];
-                const R xf = a.x[row] + (lin ? R(2) * d - a.delta_prev[row] : d);
+                const R xf = a.x[row] + (lin ? a.dext[row] : d);
                 a.x[row] = xf;
-                if (lin) a.delta_prev[row] = d;
-                a.delta[row] = xf - a.vin[row];
+                const R dn = xf - a.vin[row];
+                a.delta[row] = dn;
+                if (lin) a.dext[row] = R(2) * dn - d;     // the next solve's start: 2 delta - delta_prev
             }
         }
     }

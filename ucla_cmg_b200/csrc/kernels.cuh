@@ -125,9 +125,11 @@ template <typename R> struct CGArgs {
     // (two buffers each); p lives in p0
     R *r1, *w0, *w1, *s0, *s1;
     // predictor (two-reduction variant only; nullable): delta = the previous
-    // solve's x - V for this half step, updated in place; delta_prev (nullable)
-    // the one before it, for a linear extrapolation; vin scratch of n
-    R *delta, *delta_prev, *vin;
+    // solve's x - V for this half step, updated in place; dext (nullable) the
+    // linear extrapolation 2 delta - delta_prev of the last two, which the
+    // previous solve stores for the next one's start (one vector gathered in
+    // the prologue, not two); vin scratch of n
+    R *delta, *dext, *vin;
     // two-reduction variant: each warp asks L2 for the indices and values of
     // the slice it reads `prefetch` slices ahead (0: no prefetch)
     int prefetch;
