@@ -87,6 +87,33 @@ def test_short_fallback_list_runs_by_warps_with_the_same_bits(gpu):
     assert np.array_equal(a["ta"], b["ta"])
 
 
+def test_graph_replay_with_the_fallback_stream(gpu):
+    """The learned step forks its fallback list onto a second stream and joins
+    it before the next kernel; replayed from CUDA graphs of 20 steps (the fork
+    and join captured) the run equals the directly launched one bit for bit."""
+    out = []
+    for gs in (0, 20):
+        m, node_type, gks, blk = _setup()
+        g = Monodomain(m, capi.TUSSCHER, capi.SURROGATE, dt=0.1, ionic_dt=0.02, D=M.sigma_to_D(1.2, 0.2),
+                       node_type=node_type, type_consts=W.tt_type_consts(), gks_scale=gks,
+                       tt_jacobian=capi.TT_JAC_TRUE)
+        _trained().deploy(g)
+        g.set_launch_config(graph_steps=gs)
+        g.set_voltage(-85.423)
+        g.set_stimulus(blk, 0.0, 2.0, 50.0 * W.TT_XI)
+        fb = 0
+        for k in range(4):
+            st = g.step(100)
+            fb += st["fallback_nodes"]
+            assert st["nonfinite"] == 0 and st["timeouts"] == 0
+        out.append((g.voltage(), g.activation()[0], fb))
+        g.close()
+    assert out[0][2] > 0                         # the fallback list did run
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+
+
 def test_output_range_check_falls_back(gpu):
     s = _trained()
     s.out_lo = np.full(SG.DIMS[-1], 1e30, np.float32)
