@@ -62,7 +62,9 @@ struct GridBarrier {
 
 __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks) {
     __shared__ int s_ok;
-    __threadfence();          // every thread publishes its writes at gpu scope
+    // the CTA barrier orders every thread's writes before thread 0's
+    // gpu-scope fence and arrival (fences are cumulative), as a cooperative
+    // grid sync does: one fence per CTA, not one per thread
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
