@@ -74,9 +74,10 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, unsigned int nblocks) 
         const unsigned int max_polls = lim ? lim : kGridPolls;
         const unsigned int g = *vgen;
         __threadfence();
-        const unsigned int arrived = atomicAdd(&b->count, 1u);
+        // the last arrival wraps the count back to 0 in the same atomic (no
+        // separate reset store for the release fence to wait on)
+        const unsigned int arrived = atomicInc(&b->count, nblocks - 1u);
         if (arrived == nblocks - 1) {
-            b->count = 0;
             __threadfence();
             atomicAdd(&b->gen, 1u);
         } else {
