@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(128, MINB) k_ionic(const IonicArgs<R> a) {
     unsigned int my_newton = 0, my_caps = 0, my_bad = 0;
     // every node or the fallback list of the learned step (the nodes it
     // could not take).  One call site, so both modes run the same machine
-    // code and a node's result does not depend on which mode advanced it.
+    // code and a node's result does not depend on which mode advanced it
+    // (k_ionic_warp, which takes the short lists, reproduces those bits).
     int cnt = a.node_list ? *a.list_count : a.n;
     if (a.node_list && a.list_warp_max > 0 && cnt <= a.list_warp_max) cnt = 0;   // k_ionic_warp takes it
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
