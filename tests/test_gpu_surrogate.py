@@ -5,7 +5,8 @@
   run is bit-identical to an EP_FP32 handle.
 * Accuracy: the committed network (ucla_cmg_b200/data/tt_surrogate.npz) on
   a slab with endo/M/epi bands, a G_Ks gradient and a corner stimulus,
-  judged by the plain FP64 run: activation time and pseudo-ECG.
+  judged by the plain FP64 run against the metric's targets: activation time
+  within 0.5 ms, pseudo-ECG within 2 %.
 * Ablation: the same deployment with the untrained network (the trainer's
   initial weights, same normalisation and envelope) against the trained one;
   the trained network takes most node-steps off the plain model at that
@@ -133,9 +134,11 @@ def test_accuracy_against_fp64(gpu):
     ecg_l2 = np.linalg.norm(sg["ecg"] - ref["ecg"]) / np.linalg.norm(ref["ecg"])
     print(f"act err mean {err.mean():.3f} max {err.max():.3f} ms, ECG rel L2 {ecg_l2:.4f}, "
           f"fallback {sg['fb']:.3f}")
+    # the metric's own targets: activation time within 0.5 ms, pseudo-ECG within 2 %
+    # (this slab, 60 ms: mean 0.05 ms, max 0.10 ms, ECG 1.9 %)
     assert err.mean() <= 0.5
-    assert err.max() <= 2.0
-    assert ecg_l2 <= 0.05
+    assert err.max() <= 0.5
+    assert ecg_l2 <= 0.02
 
 
 def test_ablation_untrained_network(gpu):
