@@ -62,3 +62,20 @@ def test_node_step_bytes_is_the_sum_of_the_phases():
         extra = 0 if not pred else (2 + 2 * pred + 3) * 4
         cg = z * 12 + 5 * 4 + extra + k * (z * 8 + 12 * 4)
         assert abs(b - ((2 * 19 * 4 + 16 + 1 + 4 + 4) + 2 * cg + 11 * 4 / 10)) < 1e-9
+
+
+def test_roofline_traffic_follows_the_cg_kernel():
+    """roofline.traffic: the committed ncu bytes of the CG kernel that ran --
+    the staged kernel's own entry (measured with predictor 2) for cg_batch 32,
+    the gather-width kernels' entry otherwise."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(bench.__file__), "profiles", "traffic.json")) as f:
+        t = json.load(f)
+    st = t["cg_staged"]["predict2_bytes"]
+    assert bench._traffic("cg", "surrogate", 5.0, 2, 32) == st["prologue_bytes"] + 5.0 * st["per_iteration_bytes"]
+    assert bench._traffic("cg", "surrogate", 5.0, 1, 32) is None          # not captured
+    c = t["cg"]
+    assert bench._traffic("cg", "surrogate", 5.0, 2, 8) == (c["prologue_bytes"] + c["predict_extra_bytes"]["2"]
+                                                             + 5.0 * c["per_iteration_bytes"])
+    assert bench._traffic("ionic", "surrogate", 5.0) == t["surrogate"]
