@@ -293,10 +293,16 @@ __device__ __forceinline__ void output_node(const SurrogateArgs &a, const Surrog
         bool out_ok = inside;
 #pragma unroll
         for (int j = 0; j < SG_NY; j++) {
-            const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
-            if ((aux->out_mask >> j) & 1u) out_ok = out_ok && (u >= aux->out_lo[j]) && (u <= aux->out_hi[j]);
-            const float sc = aux->out_scale[j];
-            d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
+            // only the outputs the update reads (out_mask: the six concentrations
+            // in the hybrid form, every output otherwise) are range-checked and
+            // mapped back; the others are never read
+            d[j] = 0.f;
+            if ((aux->out_mask >> j) & 1u) {
+                const float u = (__uint_as_float(yv[j]) + aux->b4[j]) * aux->out_std[j] + aux->out_mean[j];
+                out_ok = out_ok && (u >= aux->out_lo[j]) && (u <= aux->out_hi[j]);
+                const float sc = aux->out_scale[j];
+                d[j] = sc > 0.f ? sc * sinhf(fminf(fmaxf(u, -80.f), 80.f)) : u;
+            }
         }
         const unsigned int lm = aux->log_mask;
         if (aux->v_update == 2) a.take[i] = out_ok ? 1 : 0;
