@@ -55,7 +55,7 @@ struct ep_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t io_ev[8] = {};           // chunked host <-> device copies (created on first use)
+    cudaEvent_t io_ev[16] = {};          // chunked host <-> device copies (created on first use)
     // learned step: the fallback list runs on a second, higher-priority
     // stream beside the physics of the nodes the network took
     cudaStream_t side = nullptr;
@@ -1104,7 +1104,8 @@ static void *stage(ep_handle *h, size_t bytes) {
 // chunk are issued as soon as it is converted (uploads), or all at once with
 // an event after each chunk and each chunk converted once its event has
 // completed (downloads).  Arrays under 64K nodes go in one piece.
-constexpr int kIoChunks = 8;
+constexpr int kIoChunks = 16;
+static_assert(kIoChunks <= (int)(sizeof(((ep_handle *)nullptr)->io_ev) / sizeof(cudaEvent_t)), "io_ev too small");
 
 static int io_chunks(ep_handle *h, int count) {
     if (count < (1 << 16)) return 1;
